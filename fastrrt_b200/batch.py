@@ -1,0 +1,104 @@
+"""Batched planner: many planning requests advance together, one CUDA graph
+launch per loop() over every live slot (fastrrt_batch_* in the C ABI)."""
+import math
+
+import numpy as np
+
+from . import _lib
+
+
+def make_request(cls, class_costs, start, goal, *, perception_m=None, m_per_px=0.135,
+                 max_steering_deg=40.0, vehicle_length_m=5.4, max_curvature=-1.0,
+                 velocity_m_s=2.0, min_dist=(22, 40), max_path_size=40.0, dist_to_goal_tol=20.0,
+                 heading_tol_rad=None, seed=0, smart=False, max_iterations=0,
+                 lower_bound=(-1, -1), upper_bound=(-1, -1)):
+    """A fastrrt_request; the returned object keeps its arrays alive."""
+    cls = np.ascontiguousarray(cls, np.uint8)
+    costs = np.ascontiguousarray(class_costs, np.float32)
+    H, W = cls.shape
+    if perception_m is None:
+        perception_m = (W * m_per_px, H * m_per_px)
+    if heading_tol_rad is None:
+        heading_tol_rad = math.radians(10.0)
+    r = _lib.Request()
+    r.width, r.height = W, H
+    r.class_ids = cls.ctypes.data_as(_lib.C.POINTER(_lib.C.c_uint8))
+    r.class_costs = costs.ctypes.data_as(_lib.C.POINTER(_lib.C.c_float))
+    r.n_classes = len(costs)
+    r.perception_w_m, r.perception_h_m = perception_m
+    r.max_steering_deg = max_steering_deg
+    r.vehicle_length_m = vehicle_length_m
+    r.max_curvature = max_curvature
+    r.lb_x, r.lb_z = lower_bound
+    r.ub_x, r.ub_z = upper_bound
+    r.start_x, r.start_z, r.start_heading = int(start[0]), int(start[1]), float(start[2])
+    r.goal_x, r.goal_z, r.goal_heading = int(goal[0]), int(goal[1]), float(goal[2])
+    r.velocity_m_s = velocity_m_s
+    r.min_dist_x, r.min_dist_z = min_dist
+    r.max_path_size = max_path_size
+    r.dist_to_goal_tol = dist_to_goal_tol
+    r.heading_tol_rad = heading_tol_rad
+    r.seed = int(seed)
+    r.smart = int(bool(smart))
+    r.max_iterations = int(max_iterations)
+    r._keep = (cls, costs)
+    return r
+
+
+class BatchPlanner:
+    def __init__(self, n_slots, max_width, max_height):
+        h = _lib.lib().fastrrt_batch_create(n_slots, max_width, max_height)
+        if not h:
+            raise _lib.FastRRTError("batch_create: " + _lib.last_error())
+        self._h = h
+        self.n_slots = n_slots
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib._lib is not None:
+            _lib.lib().fastrrt_batch_destroy(self._h)
+            self._h = None
+
+    def admit_many(self, requests, timeout_ms=0):
+        arr = (_lib.Request * len(requests))(*requests)
+        self._keep = requests
+        _lib.check(_lib.lib().fastrrt_batch_admit_many(self._h, len(requests), arr, timeout_ms),
+                   "batch_admit_many")
+
+    def admit(self, slot, request, timeout_ms=0):
+        _lib.check(_lib.lib().fastrrt_batch_admit(self._h, slot, _lib.C.byref(request), timeout_ms),
+                   "batch_admit")
+
+    def run(self, max_launches=1000, check_every=1):
+        return _lib.check(_lib.lib().fastrrt_batch_run(self._h, max_launches, check_every),
+                          "batch_run")
+
+    def step(self):
+        _lib.check(_lib.lib().fastrrt_batch_step(self._h), "batch_step")
+
+    def last_ms(self):
+        return float(_lib.lib().fastrrt_batch_last_ms(self._h))
+
+    def status(self):
+        done = np.zeros(self.n_slots, np.int32)
+        goal = np.zeros(self.n_slots, np.int32)
+        loops = np.zeros(self.n_slots, np.int32)
+        _lib.check(_lib.lib().fastrrt_batch_status(self._h, done, goal, loops), "batch_status")
+        return done, goal, loops
+
+    def collect(self, slots):
+        slots = np.ascontiguousarray(slots, np.int32)
+        n = len(slots)
+        valid = np.zeros(n, np.int32)
+        length = np.zeros(n, np.float32)
+        path_n = np.zeros(n, np.int32)
+        _lib.check(_lib.lib().fastrrt_batch_collect(self._h, n, slots, valid, length, path_n),
+                   "batch_collect")
+        return valid, length, path_n
+
+    def path(self, k, cap=1024):
+        buf = np.zeros(3 * cap, np.float32)
+        m = _lib.check(_lib.lib().fastrrt_batch_path(self._h, k, buf, cap), "batch_path")
+        return buf[:3 * m].reshape(m, 3).copy()
+
+    def release(self, slot):
+        _lib.check(_lib.lib().fastrrt_batch_release(self._h, slot), "batch_release")

@@ -1,0 +1,533 @@
+// frrt_device.cuh -- device functions of the B200 FastRRT planner.
+//
+// The per-candidate arithmetic (kinematic integration, footprint probe
+// coordinates, Hermite samples) is written with the same expression shapes
+// and types as the reference so that the CUDA compiler produces the same
+// roundings and fused multiply-adds; the feasibility booleans, cell indices
+// and parent links are therefore bit-identical to the reference kernels.
+// Everything around that arithmetic is organised for the GPU: warp-wide
+// cooperative footprint probes, bit-packed frames, a conservative "clear"
+// shortcut that answers most footprint checks with one bit lookup, and a
+// counter-based RNG.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "frrt_common.cuh"
+
+namespace frrt {
+
+// driveless constants (double precision, as the reference headers use them)
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kHalfPi = kPi / 2.0;
+constexpr double kToDeg = 180.0 / kPi;
+
+// ---------------------------------------------------------------------------
+// RNG: Philox4x32-10 (Salmon et al., "Parallel random numbers: as easy as
+// 1, 2, 3", SC 2011).  Counter (cell, iteration, tag, 0), key = seed.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRngTag = 0x46525254u;
+
+__host__ __device__ inline void philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                           uint32_t k0, uint32_t k1, uint32_t out[4])
+{
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// uniform in (0, 1] with 24 random bits (exact in float)
+__host__ __device__ inline float u01(uint32_t r) { return (float)((r >> 8) + 1u) * (1.0f / 16777216.0f); }
+
+// steering U(-max, max] then length max(5, max_path * U) -- generateRandomNeg /
+// generateRandom (random_number_gen.cu:14-20) as called by the expansion
+// kernels (graph_expansion.cu:174-180)
+__device__ inline void draw_expansion(unsigned long long seed, uint32_t pos, uint32_t iter,
+                                      float max_steer, float max_path, float &steer, float &len)
+{
+    uint32_t r[4];
+    philox4x32(pos, iter, kRngTag, 0u, (uint32_t)seed, (uint32_t)(seed >> 32), r);
+    const float u0 = u01(r[0]);
+    const float u1 = u01(r[1]);
+    steer = (2.0f * u0 - 1.0f) * max_steer;
+    len = fmaxf(5.0f, max_path * u1);
+}
+
+// ---------------------------------------------------------------------------
+// frame access
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool bit_xz(const uint32_t *m, int rw, int x, int z)
+{
+    return (m[(long)z * rw + (x >> 5)] >> (x & 31)) & 1u;
+}
+
+// what a footprint probe needs; the mask pointers may be shared or global memory
+struct Foot {
+    int W, H;
+    int mdx, mdz;
+    int lbx, lbz, ubx, ubz;
+    int rw;
+    const uint32_t *blocked;
+    const uint32_t *clear;
+    const int32_t *trav;
+};
+
+__device__ __forceinline__ Foot foot_of(const Inst &I, const uint32_t *blocked, const uint32_t *clear)
+{
+    Foot f;
+    f.W = I.W; f.H = I.H; f.mdx = I.mdx; f.mdz = I.mdz;
+    f.lbx = I.lbx; f.lbz = I.lbz; f.ubx = I.ubx; f.ubz = I.ubz;
+    f.rw = I.mask_rw;
+    f.blocked = blocked; f.clear = clear; f.trav = I.trav;
+    return f;
+}
+
+__device__ __forceinline__ unsigned full_probes(const Foot &f)
+{
+    return (unsigned)((2 * f.mdx + 1) * (2 * f.mdz + 1));
+}
+
+// 1: feasible without probing (isAllAngleFeasible quirk or clear shortcut),
+// 0: the footprint has to be probed.  `probes` gets the reference's count.
+__device__ __forceinline__ int quick_feasible(const Foot &f, int x, int z, unsigned long long &probes)
+{
+    const long pos = (long)z * f.W + x;
+    // isAllAngleFeasible (path_feasible.cu:13-16): `TO_INT(z) & 256 > 0` == bit 0
+    if (f.trav && (f.trav[pos] & 1))
+        return 1;
+    // no obstacle within the Chebyshev radius that bounds every probe
+    if (bit_xz(f.clear, f.rw, x, z)) {
+        probes += full_probes(f);
+        return 1;
+    }
+    return 0;
+}
+
+// the probe loop of __computeFeasibleForAngle (path_feasible.cu:18-78), one
+// lane, reference order
+__device__ inline bool probe_scalar(const Foot &f, int x, int z, float angle, unsigned long long &probes)
+{
+    const float c = cosf(angle);
+    const float s = sinf(angle);
+    for (int i = -f.mdz; i <= f.mdz; i++)
+        for (int j = -f.mdx; j <= f.mdx; j++) {
+            probes++;
+            const int xl = (int)(j * c - i * s + x);
+            const int zl = (int)(j * s + i * c + z);
+            if (xl < 0 || xl >= f.W)
+                continue;
+            if (zl < 0 || zl >= f.H)
+                continue;
+            if (xl >= f.lbx && xl <= f.ubx && zl >= f.ubz && zl <= f.lbz)
+                continue;
+            if (bit_xz(f.blocked, f.rw, xl, zl))
+                return false;
+        }
+    return true;
+}
+
+__device__ inline bool feasible_scalar(const Foot &f, int x, int z, float angle, unsigned long long &probes)
+{
+    if (quick_feasible(f, x, z, probes))
+        return true;
+    return probe_scalar(f, x, z, angle, probes);
+}
+
+// The same probe loop, all 32 lanes of a warp on one (x, z, angle): lane k
+// of batch b evaluates probe b*32+k in the reference's i-major order, and the
+// first blocked probe of the first batch that has one is the reference's
+// early exit, so the returned count is the reference's probe count.
+__device__ inline bool probe_warp(const Foot &f, int x, int z, float angle, int lane, unsigned &count)
+{
+    const float c = cosf(angle);
+    const float s = sinf(angle);
+    const int wdt = 2 * f.mdx + 1;
+    const int total = wdt * (2 * f.mdz + 1);
+    const int q = 32 / wdt, r = 32 % wdt;
+    int ii = lane / wdt, jj = lane % wdt;
+    for (int base = 0; base < total; base += 32) {
+        bool hit = false;
+        if (base + lane < total) {
+            const int i = ii - f.mdz;
+            const int j = jj - f.mdx;
+            const int xl = (int)(j * c - i * s + x);
+            const int zl = (int)(j * s + i * c + z);
+            if (xl >= 0 && xl < f.W && zl >= 0 && zl < f.H &&
+                !(xl >= f.lbx && xl <= f.ubx && zl >= f.ubz && zl <= f.lbz))
+                hit = bit_xz(f.blocked, f.rw, xl, zl);
+        }
+        const unsigned m = __ballot_sync(kFull, hit);
+        if (m) {
+            count = (unsigned)(base + __ffs(m));
+            return false;
+        }
+        ii += q;
+        jj += r;
+        if (jj >= wdt) {
+            jj -= wdt;
+            ii++;
+        }
+    }
+    count = (unsigned)total;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// resumable per-lane tasks: advance() runs until a footprint needs a full
+// probe (returns 1) or the task ends (returns 0); resolve() consumes the
+// probe result.  run_warp() drives 32 tasks and answers their probes with
+// probe_warp, so lanes never probe 943 cells serially.
+// ---------------------------------------------------------------------------
+
+// check_kinematic_new_path (kinematics.cu:123-231)
+struct KinTask {
+    float x, y, heading, beta, ds, hif, nodeCost, velocity;
+    int maxSize, loop_max, loop_count, size, last_x, last_z, pend_x, pend_z;
+    int ok;                     // 1 = feasible end cell, 0 = rejected
+    float og_x, og_z;
+    int W, H;
+    const float *intrinsic;
+
+    __device__ void init(const Inst &I, int sx, int sz, float steeringAngle, float pathSize,
+                         float velocity_m_s, float start_heading, float start_cost)
+    {
+        const double maxSteering = I.max_steer;
+        const double lr = I.lr;
+        W = I.W;
+        H = I.H;
+        og_x = I.og_x;
+        og_z = I.og_z;
+        intrinsic = I.intrinsic;
+        // convert_waypoint_to_map_pose (kinematics.cu:54-59)
+        x = og_z - sz;
+        y = sx - og_x;
+        if (steeringAngle > maxSteering)
+            steeringAngle = maxSteering;
+        else if (steeringAngle < -maxSteering)
+            steeringAngle = -maxSteering;
+        const float steer = tanf(steeringAngle);
+        const float dt = 0.1;
+        velocity = velocity_m_s;
+        ds = velocity_m_s * dt;
+        beta = atanf(steer / 2);
+        hif = ds * cosf(beta) * steer / (2 * lr);
+        maxSize = (int)(pathSize) + 1;
+        size = 0;
+        last_x = sx;
+        last_z = sz;
+        heading = start_heading;
+        nodeCost = start_cost;
+        loop_count = 0;
+        loop_max = (100 * maxSize) / dt;
+        ok = 0;
+    }
+
+    __device__ int advance(const Foot &f, unsigned long long &probes)
+    {
+        while (size < maxSize) {
+            if (loop_count++ > loop_max)
+                break;
+            x += ds * cosf(heading + beta);
+            y += ds * sinf(heading + beta);
+            heading += hif;
+            // convert_map_pose_to_waypoint (kinematics.cu:25-46)
+            const double2 coord = {x, y};
+            const int lpx = (int)(og_x + coord.y);
+            const int lpz = (int)(og_z - coord.x);
+            if (lpx == last_x && lpz == last_z)
+                continue;
+            if (lpx < 0 || lpx >= W)
+                break;
+            if (lpz < 0 || lpz >= H)
+                break;
+            size += 1;
+            nodeCost += (intrinsic ? intrinsic[(long)lpz * W + lpx] : 0.0f) + 1;
+            if (quick_feasible(f, lpx, lpz, probes)) {
+                last_x = lpx;
+                last_z = lpz;
+                continue;
+            }
+            pend_x = lpx;
+            pend_z = lpz;
+            return 1;
+        }
+        ok = size >= 1;
+        return 0;
+    }
+    // returns false when the task ended (infeasible footprint)
+    __device__ bool resolve(bool feasible)
+    {
+        if (!feasible) {
+            ok = 0;
+            return false;
+        }
+        last_x = pend_x;
+        last_z = pend_z;
+        return true;
+    }
+    __device__ float probe_angle() const { return heading; }
+};
+
+// checkDirectConnectionToGoal (graph_direct_goal_connection.cu:16-167) with
+// isDistanceToGoalProcessed = false
+struct HermTask {
+    int x, z, goal_x, goal_z, numPoints, i, last_x, last_z, W, H, trav;
+    float distance, t1x, t1y, t2x, t2y, nodeCost, max_curvature, pend_heading;
+    int safe, ok;
+    const float *intrinsic;
+
+    __device__ void init(const Inst &I, const Foot &f, float max_curv, int x_, int z_,
+                         float local_heading, int gx, int gz, float goal_heading, int safe_zone,
+                         float start_cost)
+    {
+        W = f.W;
+        H = f.H;
+        x = x_;
+        z = z_;
+        goal_x = gx;
+        goal_z = gz;
+        max_curvature = max_curv;
+        intrinsic = I.intrinsic;
+        const long pos = (long)z * W + x;
+        const int dx = goal_x - x;
+        const int dz = goal_z - z;
+        distance = sqrtf(dx * dx + dz * dz);
+        numPoints = (int)(distance);
+        const float a1 = local_heading - kHalfPi;
+        const float a2 = goal_heading - kHalfPi;
+        t1x = distance * cosf(a1);
+        t1y = distance * sinf(a1);
+        t2x = distance * cosf(a2);
+        t2y = distance * sinf(a2);
+        last_x = -1;
+        last_z = -1;
+        nodeCost = start_cost;
+        trav = f.trav ? f.trav[pos] : 0;
+        safe = safe_zone;
+        i = 0;
+        ok = 0;
+    }
+
+    __device__ int advance(const Foot &f, unsigned long long &probes)
+    {
+        for (; i < numPoints; ++i) {
+            const double t = ((double)0.0 + i) / (numPoints - 1);
+            const double t2 = t * t;
+            const double t3 = t2 * t;
+            const double h00 = 2 * t3 - 3 * t2 + 1;
+            const double h10 = t3 - 2 * t2 + t;
+            const double h01 = -2 * t3 + 3 * t2;
+            const double h11 = t3 - t2;
+            const double px = h00 * x + h10 * t1x + h01 * goal_x + h11 * t2x;
+            const double pz = h00 * z + h10 * t1y + h01 * goal_z + h11 * t2y;
+            if (px < 0 || px >= W)
+                continue;
+            if (pz < 0 || pz >= H)
+                continue;
+            const int cx = (int)(px);
+            const int cz = (int)(pz);
+            if (cx == last_x && cz == last_z)
+                continue;
+            if (cx < 0 || cx >= W)
+                continue;
+            if (cz < 0 || cz >= H)
+                continue;
+            nodeCost += (intrinsic ? intrinsic[(long)cz * W + cx] : 0.0f) + 1;
+            const double t00 = 6 * t2 - 6 * t;
+            const double t10 = 3 * t2 - 4 * t + 1;
+            const double t01 = -6 * t2 + 6 * t;
+            const double t11 = 3 * t2 - 2 * t;
+            const double ddx = t00 * x + t10 * t1x + t01 * goal_x + t11 * t2x;
+            const double ddz = t00 * z + t10 * t1y + t01 * goal_z + t11 * t2y;
+            const float heading = atan2f(ddz, ddx) + kHalfPi;
+            const double d00 = 12 * t - 6;
+            const double d10 = 6 * t - 4;
+            const double d01 = -12 * t + 6;
+            const double d11 = 6 * t - 2;
+            const double dd2x = d00 * x + d10 * t1x + d01 * goal_x + d11 * t2x;
+            const double dd2z = d00 * z + d10 * t1y + d01 * goal_z + d11 * t2y;
+            if (max_curvature > 0) {
+                const double num = fabs(ddx * dd2z - ddz * dd2x);
+                const double s2 = ddx * ddx + ddz * ddz;
+                // s2 * sqrt(s2) is within a few ulp of pow(s2, 1.5); pow only
+                // decides cases inside a 1e-6 guard band around the limit
+                const double kf = num / (s2 * sqrt(s2));
+                bool over;
+                if (kf > (double)max_curvature * (1.0 + 1e-6))
+                    over = true;
+                else if (kf < (double)max_curvature * (1.0 - 1e-6))
+                    over = false;
+                else {
+                    const float k = num / pow(s2, 1.5);
+                    over = k > max_curvature;
+                }
+                if (over) {
+                    ok = 0;
+                    i = numPoints;
+                    return 0;
+                }
+            }
+            last_x = cx;
+            last_z = cz;
+            if (safe && (trav & 0x100))
+                continue;
+            if (quick_feasible(f, last_x, last_z, probes))
+                continue;
+            pend_heading = heading;
+            ++i;
+            return 1;
+        }
+        if (numPoints <= 0 || (last_x != goal_x && last_z != goal_z))
+            ok = 0;
+        else
+            ok = 1;
+        return 0;
+    }
+    __device__ bool resolve(bool feasible)
+    {
+        if (!feasible) {
+            ok = 0;
+            i = numPoints;
+            numPoints = -1;  // keep ok == 0 if advance() is called again
+            return false;
+        }
+        return true;
+    }
+    __device__ float probe_angle() const { return pend_heading; }
+    __device__ int probe_x() const { return last_x; }
+    __device__ int probe_z() const { return last_z; }
+    __device__ float result() const { return ok ? nodeCost : -1.0f; }
+};
+
+// Drives one task per lane.  `has` says whether the lane holds a task.
+// Probes needing a full footprint scan are answered cooperatively.
+template <class Task, class PX, class PZ>
+__device__ void run_warp(Task &t, bool has, const Foot &f, unsigned long long &probes, PX px, PZ pz)
+{
+    const int lane = threadIdx.x & 31;
+    bool active = has;
+    while (__any_sync(kFull, active)) {
+        bool need = false;
+        if (active) {
+            if (t.advance(f, probes))
+                need = true;
+            else
+                active = false;
+        }
+        unsigned m = __ballot_sync(kFull, need);
+        bool mine = true;
+        while (m) {
+            const int leader = __ffs(m) - 1;
+            m &= m - 1;
+            const int bx = __shfl_sync(kFull, px(t), leader);
+            const int bz = __shfl_sync(kFull, pz(t), leader);
+            const float ba = __shfl_sync(kFull, t.probe_angle(), leader);
+            unsigned cnt = 0;
+            const bool ok = probe_warp(f, bx, bz, ba, lane, cnt);
+            if (lane == leader) {
+                mine = ok;
+                probes += cnt;
+            }
+        }
+        if (need && !t.resolve(mine))
+            active = false;
+    }
+}
+
+// computeHeading (graph.cu:219-234)
+__device__ inline double compute_heading(int x1, int z1, int x2, int z2)
+{
+    double dz = z2 - z1;
+    double dx = x2 - x1;
+    if (dx == 0 && dz == 0)
+        return 0;
+    double v1 = 0;
+    if (dz != 0)
+        v1 = atan2f(-dz, dx);
+    else
+        v1 = atan2f(0, dx);
+    return kHalfPi - v1;
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory staging of the frame masks with the Blackwell bulk copy
+// engine (cp.async.bulk, completion on an mbarrier, bounded waits)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+constexpr long kWaitLimit = 1L << 22;  // try_wait rounds before giving up
+
+// Loads `words` 32-bit words of the two masks into shared memory.  Called by
+// the whole block; returns false (and the caller falls back to the global
+// copies) if the copy did not complete within the wait limit.
+__device__ inline bool stage_masks(uint32_t *s_blk, uint32_t *s_clr, const uint32_t *g_blk,
+                                   const uint32_t *g_clr, int words, uint64_t *bar, unsigned &phase)
+{
+    __syncthreads();  // every warp finished reading the previous masks
+    if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        const unsigned bytes = (unsigned)words * 4u;
+        mbar_expect_tx(bar, 2u * bytes);
+        bulk_g2s(s_blk, g_blk, bytes, bar);
+        bulk_g2s(s_clr, g_clr, bytes, bar);
+    }
+    bool done = false;
+    for (long k = 0; k < kWaitLimit; k++)
+        if (mbar_try_wait(bar, phase)) {
+            done = true;
+            break;
+        }
+    phase ^= 1u;
+    return __syncthreads_and(done) != 0;
+}
+
+}  // namespace frrt

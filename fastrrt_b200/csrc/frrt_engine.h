@@ -1,0 +1,191 @@
+// frrt_engine.h -- host runtime of the B200 FastRRT planner.
+//
+// An Engine owns a device arena of `n_slots` planning slots, each with the
+// node grid, frame masks and scratch of one instance of up to max_w x max_h
+// cells, plus the scheduling tables and a captured CUDA graph of one
+// planning iteration over all slots.  The drop-in FastRRT planner is an
+// Engine with one slot; the batched and served planners use many.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "frrt_common.cuh"
+#include "frrt_kernels.cuh"
+
+namespace frrt {
+
+void set_error(const std::string &msg);
+const char *last_error();
+
+// A BEV frame in device memory: class ids, class costs, optional
+// traversability bits (the reference SearchFrame's three channels, minus the
+// unused distance channel).
+struct Frame {
+    int W = 0, H = 0;
+    uint8_t *d_cls = nullptr;
+    float *d_costs = nullptr;
+    int n_classes = 0;
+    int32_t *d_trav = nullptr;
+    std::vector<float> h_costs;
+    ~Frame();
+};
+
+Frame *frame_create(int W, int H, const uint8_t *cls, const float *costs, int n_classes,
+                    const int32_t *trav);
+// from the reference SearchFrame's float3 layout (class, distance, bits)
+Frame *frame_create_f3(int W, int H, const float *xyz, const float *costs, int n_classes);
+
+struct PlanRequest {
+    int start_x, start_z;
+    float start_heading;
+    int goal_x, goal_z;
+    float goal_heading;
+    float velocity;
+    int min_dist_x, min_dist_z;
+    float max_path;
+    float dist_tol;
+    float heading_tol;
+    unsigned long long seed;
+    int smart;
+    int max_iter;
+    int stop_on_goal;
+};
+
+struct Physical {
+    float pw_m, ph_m;
+    double max_steer_rad;
+    float vehicle_len;
+    float max_curvature;  // < 0: derived from steering and length
+    int lbx, lbz, ubx, ubz;
+};
+
+class Engine {
+public:
+    Engine(int n_slots, int max_w, int max_h, int device = -1);
+    ~Engine();
+    bool ok() const { return ok_; }
+
+    int n_slots() const { return n_slots_; }
+    int max_cells() const { return max_cells_; }
+    cudaStream_t stream() const { return stream_; }
+    const Launch &launch() const { return L_; }
+
+    // slot configuration (host side; uploaded by commit())
+    void set_physical(int slot, const Physical &p);
+    // frame owned by the caller (must outlive its use) or copied into the slot
+    bool bind_frame(int slot, const Frame *f);
+    // copies class ids (host or device memory) into the slot's own buffer
+    bool copy_frame(int slot, int W, int H, const uint8_t *cls, const float *costs_host,
+                    int n_classes, bool cls_on_device = false);
+    void set_request(int slot, const PlanRequest &r);
+    void set_deadline(int slot, long long deadline_ns);
+    // intrinsic costs: nullptr keeps them zero (the planner's default)
+    bool set_intrinsic(int slot, const float *host_costs);
+    bool commit();  // upload Inst table + scheduling tables
+
+    // set_plan_data for listed slots: masks + goal direct-connection precompute
+    bool prepare(const std::vector<int> &slots, float direct_max_curvature = 0.8f);
+    // search_init for listed slots
+    bool search_init(const std::vector<int> &slots, bool reset_regions);
+    // one loop() over every live slot (graph launch); no host sync
+    bool iterate();
+    bool sync();
+    // copy the small head of the state of every slot to host memory
+    bool fetch_states(bool synchronous = true);
+    const State &state(int slot) const { return h_state_[slot]; }
+    bool deactivate(int slot);
+
+    // per-slot operations (drop-in API)
+    bool goal_check(int slot);
+    int extract_path(int slot, std::vector<float> &xyh);
+    bool optimize(int slot, int &changed);
+    int count(int slot, int type);
+    bool grid_download(int slot, std::vector<int8_t> &type, std::vector<int32_t> &parent,
+                       std::vector<int32_t> &child, std::vector<float> &heading,
+                       std::vector<float> &cost, std::vector<float> &intrinsic,
+                       std::vector<float> &direct);
+    bool grid_upload(int slot, const std::vector<int8_t> &type, const std::vector<int32_t> &parent,
+                     const std::vector<int32_t> &child, const std::vector<float> &heading,
+                     const std::vector<float> &cost, const std::vector<float> &intrinsic,
+                     const std::vector<float> &direct);
+    bool gd_download(int slot, std::vector<uint8_t> &flag, std::vector<float> &heading,
+                     std::vector<float> &cost);
+    bool regions_upload(int slot, const std::vector<unsigned> &counts);
+    bool set_state_field_last_expanded(int slot, int v);
+    bool clear_goal_flag(int slot);
+
+    // batched extraction + validation of listed slots
+    bool extract_and_validate(const std::vector<int> &slots, int cap);
+    const std::vector<int> &paths_n() const { return h_path_n_; }
+    const std::vector<int> &valid() const { return h_valid_; }
+    const std::vector<float> &lengths() const { return h_length_; }
+    const std::vector<float> &paths() const { return h_paths_; }
+
+    // per-candidate microbenchmarks on one slot's frame
+    bool candidates(int slot, int n, const int32_t *sx, const int32_t *sz, const float *steer,
+                    const float *len, float velocity, float4 *out, unsigned long long *probes);
+    bool hermite(int slot, int n, const int32_t *x, const int32_t *z, const float *lh,
+                 const int32_t *gx, const int32_t *gz, const float *gh, float max_curvature,
+                 int safe, float *out, unsigned long long *probes);
+    bool feasible(int slot, int n, const int32_t *x, const int32_t *z, const float *a, int32_t *out,
+                  unsigned long long *probes);
+
+    Inst &inst(int slot) { return h_inst_[slot]; }
+    const Inst *d_inst() const { return d_inst_; }
+    State *d_state() const { return d_state_; }
+
+private:
+    bool check(cudaError_t e, const char *what);
+    bool ensure_graph();
+    bool upload_slots_list(const std::vector<int> &slots);
+
+    bool ok_ = false;
+    int device_ = 0;
+    int n_slots_ = 0, max_w_ = 0, max_h_ = 0, max_cells_ = 0, mask_words_ = 0;
+    cudaStream_t stream_ = nullptr;
+    Launch L_{};
+    void *arena_ = nullptr;
+    size_t arena_bytes_ = 0;
+    std::vector<Inst> h_inst_;
+    std::vector<Physical> h_phys_;
+    Inst *d_inst_ = nullptr;
+    State *d_state_ = nullptr;
+    State *h_state_ = nullptr;  // pinned
+    Sched h_sched_{};
+    Sched *d_sched_ = nullptr;
+    int *d_sched_arrays_ = nullptr;
+    unsigned *d_grab_ = nullptr;
+    int *d_slots_ = nullptr;
+    float *d_class_costs_ = nullptr;  // per slot, 256 entries
+    uint32_t *d_rowdil_ = nullptr;
+    int *d_bad_ = nullptr;
+    std::vector<uint8_t *> own_cls_;  // per slot frame copies
+    std::vector<float *> intrinsic_;  // per slot intrinsic-cost arrays
+    std::vector<int> ncls_;           // class count of each slot's frame
+    // path extraction / validation scratch
+    int cap_ = 0;
+    float *d_paths_ = nullptr;
+    int *d_path_n_ = nullptr;
+    long long *d_keys_ = nullptr;
+    unsigned *d_counts_ = nullptr;
+    int *d_valid_ = nullptr;
+    float *d_length_ = nullptr;
+    float *d_newcost_ = nullptr;
+    int *d_changed_ = nullptr;
+    int *h_small_ = nullptr;          // pinned scratch
+    std::vector<int> h_path_n_, h_valid_;
+    std::vector<float> h_length_, h_paths_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    bool dirty_ = true;
+};
+
+// host Hermite interpolation (interpolation.cpp:36-135)
+std::vector<float> interpolate_hermite(int W, int H, int p1x, int p1z, float p1h, int p2x, int p2z,
+                                       float p2h);
+std::vector<float> interpolate_path(const std::vector<float> &xyh, int W, int H);
+
+}  // namespace frrt

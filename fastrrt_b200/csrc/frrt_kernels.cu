@@ -1,0 +1,1618 @@
+// frrt_kernels.cu -- planner kernels for sm_100a.
+//
+// One planning iteration (FastRRT::loop, fastrrt.cpp:108-181) over every
+// active slot is a fixed sequence of kernels, captured once into a CUDA
+// graph by the engine:
+//
+//   k_scan        gate + candidate list             (graph_expansion.cu:148-183,
+//                                                    graph_expansion_search_zones.cu:161-194)
+//   k_plan        per-slot work prefix (1 block)
+//   k_expand      integrate + footprint + claim     (expand_node, graph_expansion.cu:103-145)
+//   k_apply       claim winners change the grid
+//   k_post        NODE count + region density       (graph_expansion_search_zones.cu:42-66)
+//   k_erase       colliding subtree erase           (graph_collision.cu:32-83)
+//   k_setnodes    COLLISION -> NODE                 (graph_collision.cu:84-104)
+//   k_accept      TEMP count, all count, TEMP->NODE, node list
+//                                                   (graph_list.cu:7-60, graph_expansion.cu:36-65)
+//   k_plan        node work prefix
+//   k_goal        goal check + best node->cell goal connection
+//                                                   (graph_best_node.cu:181-222,
+//                                                    graph_check_goal_reached.cu:17-139)
+//   k_select      tie-break of the best connection
+//   k_finish      connection / start adds, loop bookkeeping (fastrrt.cpp:130-180)
+//
+// Sweep kernels read the int8 type grid 16 cells at a time (one 16-byte
+// load per thread).  The expansion and goal kernels are persistent: blocks
+// pull chunks of one slot's work from a global counter and stage that
+// slot's bit-packed frame masks into shared memory with the bulk-copy (TMA)
+// engine.  Concurrent claims on one target cell are resolved by
+// atomicMin on the expanding cell index, which makes every iteration
+// deterministic for a given seed.
+#include <climits>
+#include <cstdio>
+
+#include "frrt_device.cuh"
+#include "frrt_kernels.cuh"
+
+namespace frrt {
+
+namespace {
+
+__device__ __forceinline__ int find_slot(const int *prefix, int n, int chunk)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= chunk)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool live(const State &S) { return S.active && !S.done; }
+
+// warp-aggregated append: returns this lane's first output index
+__device__ __forceinline__ int warp_append(int *counter, int n)
+{
+    const int lane = threadIdx.x & 31;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += v;
+    }
+    const int total = __shfl_sync(kFull, incl, 31);
+    int base = 0;
+    if (lane == 31 && total)
+        base = atomicAdd(counter, total);
+    base = __shfl_sync(kFull, base, 31);
+    return base + incl - n;
+}
+
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum64(unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void load16(const int8_t *p, int8_t out[16])
+{
+    const int4 v = *reinterpret_cast<const int4 *>(p);
+    const int8_t *b = reinterpret_cast<const int8_t *>(&v);
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+        out[k] = b[k];
+}
+
+// CudaGraph::add (graph.cu:364-374): bounds, parent child count, overriding set
+__device__ void grid_add(const Inst &I, int x, int z, float heading, int ppx, int ppz, float cost)
+{
+    if (x < 0 || x >= I.W || z < 0 || z >= I.H)
+        return;
+    if (ppx != -1 && ppz != -1 && ppx >= 0 && ppx < I.W && ppz >= 0 && ppz < I.H)
+        I.child[(long)ppz * I.W + ppx]++;
+    const long pos = (long)z * I.W + x;
+    I.type[pos] = T_NODE;
+    I.parent[pos] = pack_xz(ppx, ppz);
+    I.heading[pos] = heading;
+    I.cost[pos] = cost;
+}
+
+__device__ __forceinline__ long long global_ns()
+{
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// frame preparation
+// ---------------------------------------------------------------------------
+
+// one thread per mask word: bit set when class cost < 0
+__global__ void k_blocked(const uint8_t *cls, int W, int H, int rw, const float *costs, int ncls,
+                          uint32_t *blocked, int *bad_class)
+{
+    const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (w >= (long)rw * H)
+        return;
+    const int z = (int)(w / rw);
+    const int x0 = (int)(w - (long)z * rw) * 32;
+    uint32_t bits = 0;
+    for (int b = 0; b < 32; b++) {
+        const int x = x0 + b;
+        if (x >= W)
+            break;
+        const int c = cls[(long)z * W + x];
+        if (c >= ncls) {
+            atomicExch(bad_class, 1);
+            continue;
+        }
+        if (costs[c] < 0)
+            bits |= 1u << b;
+    }
+    blocked[w] = bits;
+}
+
+// 32 row bits starting at bit `start` (may be negative / beyond the row)
+__device__ __forceinline__ uint32_t row_bits(const uint32_t *row, int rw, int start)
+{
+    const int q = start >= 0 ? start >> 5 : -((-start + 31) >> 5);
+    const int r = start - q * 32;
+    const uint32_t lo = (q >= 0 && q < rw) ? row[q] : 0u;
+    const uint32_t hi = (q + 1 >= 0 && q + 1 < rw) ? row[q + 1] : 0u;
+    return r ? (lo >> r) | (hi << (32 - r)) : lo;
+}
+
+// horizontal dilation of the obstacle mask by rc
+__global__ void k_rowdil(const uint32_t *blocked, int W, int H, int rw, int rc, uint32_t *rowdil)
+{
+    const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (w >= (long)rw * H)
+        return;
+    const int z = (int)(w / rw);
+    const int q = (int)(w - (long)z * rw);
+    const uint32_t *row = blocked + (long)z * rw;
+    uint32_t acc = 0;
+    for (int d = -rc; d <= rc; d++)
+        acc |= row_bits(row, rw, q * 32 + d);
+    rowdil[w] = acc;
+}
+
+// vertical dilation + complement: clear = no obstacle within Chebyshev rc
+__global__ void k_clear(const uint32_t *rowdil, int W, int H, int rw, int rc, uint32_t *clear)
+{
+    const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (w >= (long)rw * H)
+        return;
+    const int z = (int)(w / rw);
+    const int q = (int)(w - (long)z * rw);
+    uint32_t acc = 0;
+    const int z0 = max(0, z - rc), z1 = min(H - 1, z + rc);
+    for (int zz = z0; zz <= z1; zz++)
+        acc |= rowdil[(long)zz * rw + q];
+    uint32_t valid = 0xffffffffu;
+    const int left = W - q * 32;
+    if (left < 32)
+        valid = left <= 0 ? 0u : ((1u << left) - 1u);
+    clear[w] = ~acc & valid;
+}
+
+void launch_frame_masks(const Inst &h, const float *d_class_costs, int n_classes,
+                        uint32_t *d_blocked, uint32_t *d_clear, uint32_t *d_rowdil,
+                        int *d_bad_class, cudaStream_t st)
+{
+    const long words = (long)h.mask_rw * h.H;
+    const int grid = (int)((words + 255) / 256);
+    k_blocked<<<grid, 256, 0, st>>>(h.cls, h.W, h.H, h.mask_rw, d_class_costs, n_classes, d_blocked,
+                                    d_bad_class);
+    k_rowdil<<<grid, 256, 0, st>>>(d_blocked, h.W, h.H, h.mask_rw, h.rc, d_rowdil);
+    k_clear<<<grid, 256, 0, st>>>(d_rowdil, h.W, h.H, h.mask_rw, h.rc, d_clear);
+}
+
+// ---------------------------------------------------------------------------
+// goal direct-connection precompute (graph_direct_goal_connection.cu:169-227)
+// ---------------------------------------------------------------------------
+
+struct PrecompTask {
+    HermTask h;
+    __device__ int advance(const Foot &f, unsigned long long &p) { return h.advance(f, p); }
+    __device__ bool resolve(bool ok) { return h.resolve(ok); }
+    __device__ float probe_angle() const { return h.pend_heading; }
+};
+
+__global__ void __launch_bounds__(256) k_direct_goal(const Inst *insts, State *states,
+                                                     const int *slots, float max_curvature,
+                                                     int smem_words)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    const int slot = slots[blockIdx.y];
+    const Inst &I = insts[slot];
+    const int cells = I.W * I.H;
+    if ((long)blockIdx.x * blockDim.x >= cells)
+        return;
+    const uint32_t *blk = I.blocked, *clr = I.clear;
+    bool use_smem = smem_words > 0 && I.mask_words <= smem_words;
+    unsigned phase = 0;
+    if (use_smem) {
+        if (threadIdx.x == 0)
+            mbar_init(&bar, 1);
+        __syncthreads();
+        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase)) {
+            blk = smem;
+            clr = smem + smem_words;
+        } else {
+            if (threadIdx.x == 0)
+                atomicExch(&states[slot].error, 1);
+            for (long k = 0; k < kWaitLimit; k++)
+                if (mbar_try_wait(&bar, phase ^ 1u))
+                    break;
+        }
+    }
+    const Foot f = foot_of(I, blk, clr);
+    const float maxc = max_curvature < 0 ? I.max_curvature : max_curvature;
+    unsigned long long probes = 0;
+    for (long base = (long)blockIdx.x * blockDim.x; base < cells; base += (long)gridDim.x * blockDim.x) {
+        const long pos = base + threadIdx.x;
+        const bool has = pos < cells;
+        PrecompTask t;
+        float lh = 0.0f;
+        int x = 0, z = 0;
+        if (has) {
+            z = (int)(pos / I.W);
+            x = (int)(pos - (long)z * I.W);
+            I.gd_flag[pos] = 0;
+            lh = compute_heading(x, z, I.goal_x, I.goal_z);
+            t.h.init(I, f, maxc, x, z, lh, I.goal_x, I.goal_z, I.goal_heading, 0, I.cost[pos]);
+        }
+        run_warp(t, has, f, probes, [](const PrecompTask &q) { return q.h.last_x; },
+                 [](const PrecompTask &q) { return q.h.last_z; });
+        if (has && t.h.ok) {
+            I.gd_flag[pos] = 1;
+            I.gd_heading[pos] = lh;
+            I.gd_cost[pos] = t.h.nodeCost;
+        }
+    }
+    probes = warp_sum64(probes);
+    if ((threadIdx.x & 31) == 0 && probes)
+        atomicAdd(&states[slot].probes, probes);
+}
+
+void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                        int max_cells, float max_curvature, const Launch &L, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    const int bx = (max_cells + 255) / 256;
+    const dim3 grid(bx, n);
+    const size_t smem = (size_t)L.smem_words * 2 * 4;
+    k_direct_goal<<<grid, 256, smem, st>>>(d_inst, d_state, d_slots, max_curvature, L.smem_words);
+}
+
+// ---------------------------------------------------------------------------
+// search_init (fastrrt.cpp:85-98): clear() only resets the type
+// (graph.cu:400-427), then the start node is added
+// ---------------------------------------------------------------------------
+
+__global__ void k_clear_types(const Inst *insts, const int *slots)
+{
+    const Inst &I = insts[slots[blockIdx.y]];
+    const long cells = (long)I.W * I.H;
+    for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < cells;
+         base += (long)gridDim.x * blockDim.x * 16)
+        *reinterpret_cast<int4 *>(I.type + base) = make_int4(0, 0, 0, 0);
+}
+
+__global__ void k_init_state(const Inst *insts, State *states, const int *slots, int n,
+                             int reset_regions)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const int slot = slots[k];
+    const Inst &I = insts[slot];
+    State &S = states[slot];
+    grid_add(I, I.start_x, I.start_z, I.start_heading, -1, -1, 0.0f);
+    S.active = 1;
+    S.done = 0;
+    S.goal_reached = 0;
+    S.collision = 0;
+    S.iter = 0;
+    S.last_expanded = 0;
+    S.n_cand = 0;
+    S.node_count = 0;
+    S.temp_count = 0;
+    S.all_count = 0;
+    S.n_nodes = 0;
+    S.skip = 0;
+    S.found = 0;
+    S.winner = 0;
+    S.best = kBigCost;
+    S.loops = 0;
+    S.error = 0;
+    if (reset_regions)
+        for (int r = 0; r < kMaxRegions; r++)
+            I.region_count[r] = 0;
+    for (int r = 0; r < kMaxRegions; r++)
+        I.region_new[r] = 0;
+}
+
+void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                        int max_cells, int reset_regions, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    const int bx = (max_cells / 16 + 255) / 256;
+    k_clear_types<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots);
+    k_init_state<<<(n + 127) / 128, 128, 0, st>>>(d_inst, d_state, d_slots, n, reset_regions);
+}
+
+// ---------------------------------------------------------------------------
+// iteration kernels
+// ---------------------------------------------------------------------------
+
+// candidate gate + list (graph_expansion.cu:157-164,
+// graph_expansion_search_zones.cu:358-368, 461-473)
+__global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->sweep_total;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->sweep_start, n, c);
+        State &S = states[slot];
+        if (!live(S))
+            continue;
+        const Inst &I = insts[slot];
+        const int cells = I.W * I.H;
+        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
+        const int last = S.last_expanded;
+        const bool frontier = last >= kFrontierThreshold;
+        const bool force = last == 0;
+        const int dw = I.W / kRegion + 1;
+        int32_t mine[16];
+        int cnt = 0;
+        if (base < cells) {
+            int8_t t[16];
+            load16(I.type + base, t);
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int pos = base + k;
+                if (t[k] != T_NODE || pos >= cells)
+                    continue;
+                bool take;
+                if (I.smart) {
+                    if (force)
+                        take = true;
+                    else if (frontier)
+                        take = I.child[pos] == 0;
+                    else {
+                        const int z = pos / I.W, x = pos - z * I.W;
+                        take = I.region_count[(z / kRegion) * dw + x / kRegion] <= 0.5 * kRegion;
+                    }
+                } else {
+                    take = !(frontier && I.child[pos] > 0);
+                }
+                if (take)
+                    mine[cnt++] = pos;
+            }
+        }
+        const int at = warp_append(&S.n_cand, cnt);
+        for (int k = 0; k < cnt; k++)
+            I.cand[at + k] = mine[k];
+    }
+}
+
+// prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
+__global__ void __launch_bounds__(1024) k_plan(const State *states, Sched *sc, int which)
+{
+    __shared__ int warp_tot[32];
+    const int n = sc->n_slots;
+    int *out = which == 0 ? sc->cand_start : sc->node_start;
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int s0 = threadIdx.x * per;
+    int local = 0;
+    for (int s = s0; s < s0 + per && s < n; s++) {
+        const State &S = states[s];
+        if (!live(S))
+            continue;
+        local += which == 0 ? (S.n_cand + kCandChunk - 1) / kCandChunk
+                            : (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
+    }
+    // block exclusive scan of `local`
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += v;
+    }
+    if (lane == 31)
+        warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int v = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(kFull, v, o);
+            if (lane >= o)
+                v += u;
+        }
+        warp_tot[lane] = v;
+    }
+    __syncthreads();
+    int run = incl - local + (wid ? warp_tot[wid - 1] : 0);
+    for (int s = s0; s < s0 + per && s < n; s++) {
+        out[s] = run;
+        const State &S = states[s];
+        if (live(S))
+            run += which == 0 ? (S.n_cand + kCandChunk - 1) / kCandChunk
+                              : (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
+    }
+    if (threadIdx.x == blockDim.x - 1)
+        out[n] = run;
+    if (threadIdx.x == 0)
+        sc->grab[which] = 0;
+}
+
+struct KinLane {
+    KinTask k;
+    __device__ int advance(const Foot &f, unsigned long long &p) { return k.advance(f, p); }
+    __device__ bool resolve(bool ok) { return k.resolve(ok); }
+    __device__ float probe_angle() const { return k.heading; }
+};
+
+// shared-memory frame staging state of a persistent block
+struct Stage {
+    int cur;
+    bool broken;
+    unsigned phase;
+};
+
+__device__ inline void stage_for(const Inst &I, int slot, Stage &sg, uint32_t *smem, int smem_words,
+                                 uint64_t *bar, State *states, const uint32_t *&blk,
+                                 const uint32_t *&clr)
+{
+    const bool fits = smem_words > 0 && I.mask_words <= smem_words && !sg.broken;
+    if (fits) {
+        if (slot != sg.cur) {
+            if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, bar, sg.phase))
+                sg.cur = slot;
+            else {
+                sg.broken = true;
+                sg.cur = -1;
+                if (threadIdx.x == 0)
+                    atomicExch(&states[slot].error, 1);
+            }
+        }
+    }
+    if (fits && !sg.broken) {
+        blk = smem;
+        clr = smem + smem_words;
+    } else {
+        blk = I.blocked;
+        clr = I.clear;
+    }
+}
+
+__device__ inline void stage_drain(Stage &sg, uint64_t *bar)
+{
+    if (sg.broken)
+        for (long k = 0; k < kWaitLimit; k++)
+            if (mbar_try_wait(bar, sg.phase ^ 1u))
+                break;
+}
+
+// expand_node (graph_expansion.cu:103-145): every listed NODE cell draws a
+// steering angle and a length, integrates, and claims its end cell
+__global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states, Sched *sc,
+                                                int smem_words)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_chunk;
+    const int n = sc->n_slots;
+    const int total = sc->cand_start[n];
+    Stage sg{-1, false, 0u};
+    if (threadIdx.x == 0)
+        mbar_init(&bar, 1);
+    __syncthreads();
+    while (true) {
+        if (threadIdx.x == 0)
+            s_chunk = (int)atomicAdd(&sc->grab[0], 1u);
+        __syncthreads();
+        const int c = s_chunk;
+        __syncthreads();
+        if (c >= total)
+            break;
+        const int slot = find_slot(sc->cand_start, n, c);
+        const Inst &I = insts[slot];
+        State &S = states[slot];
+        const uint32_t *blk, *clr;
+        stage_for(I, slot, sg, smem, smem_words, &bar, states, blk, clr);
+        const Foot f = foot_of(I, blk, clr);
+        const int idx = (c - sc->cand_start[slot]) * kCandChunk + threadIdx.x;
+        const bool has = idx < S.n_cand;
+        KinLane t;
+        int pos = 0;
+        unsigned long long probes = 0;
+        if (has) {
+            pos = I.cand[idx];
+            const int z = pos / I.W, x = pos - z * I.W;
+            float steer, len;
+            draw_expansion(I.seed, (uint32_t)pos, S.iter, (float)I.max_steer, I.max_path, steer, len);
+            t.k.init(I, x, z, steer, len, I.velocity, I.heading[pos], I.cost[pos]);
+        }
+        run_warp(t, has, f, probes, [](const KinLane &q) { return q.k.pend_x; },
+                 [](const KinLane &q) { return q.k.pend_z; });
+        if (has) {
+            int end = -1;
+            if (t.k.ok) {
+                const int ex = t.k.last_x, ez = t.k.last_z;
+                if (!(ex == I.og_x && ez == I.og_z)) {
+                    const int ep = ez * I.W + ex;
+                    if (ep != pos)
+                        end = ep;
+                }
+            }
+            I.cand_end[idx] = end;
+            I.cand_heading[idx] = t.k.heading;
+            I.cand_cost[idx] = t.k.nodeCost;
+            if (end >= 0)
+                atomicMin(&I.claim[end], pos);
+        }
+        probes = warp_sum64(probes);
+        if ((threadIdx.x & 31) == 0 && probes)
+            atomicAdd(&S.probes, probes);
+    }
+    stage_drain(sg, &bar);
+}
+
+// the winner of each claimed cell applies expand_node's transitions
+__global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->cand_start[n];
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->cand_start, n, c);
+        const Inst &I = insts[slot];
+        State &S = states[slot];
+        const int idx = (c - sc->cand_start[slot]) * kCandChunk + threadIdx.x;
+        if (idx >= S.n_cand)
+            continue;
+        const int end = I.cand_end[idx];
+        if (end < 0)
+            continue;
+        const int pos = I.cand[idx];
+        if (I.claim[end] != pos)
+            continue;
+        I.claim[end] = kClaimFree;
+        const int z = pos / I.W, x = pos - z * I.W;
+        const int8_t t = I.type[end];
+        if (t == T_NULL) {
+            I.child[pos] += 1;
+            I.type[end] = T_TEMP;
+        } else if (t == T_NODE) {
+            I.type[end] = T_COLLISION;
+            S.collision = 1;
+            I.child[pos] -= 1;
+        } else {
+            continue;
+        }
+        I.parent[end] = pack_xz(x, z);
+        I.heading[end] = I.cand_heading[idx];
+        I.cost[end] = I.cand_cost[idx];
+    }
+}
+
+// NODE count (erase bound) and region density after the expansion
+__global__ void __launch_bounds__(256) k_post(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->sweep_total;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->sweep_start, n, c);
+        State &S = states[slot];
+        if (!live(S))
+            continue;
+        const Inst &I = insts[slot];
+        const int cells = I.W * I.H;
+        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
+        int nodes = 0;
+        if (base < cells) {
+            int8_t t[16];
+            load16(I.type + base, t);
+            const int dw = I.W / kRegion + 1;
+            int reg = -1, rc = 0;
+            for (int k = 0; k < 16; k++) {
+                const int pos = base + k;
+                if (pos >= cells)
+                    break;
+                nodes += t[k] == T_NODE;
+                if (I.smart && t[k] != T_NULL && t[k] != T_PROCESSING) {
+                    const int z = pos / I.W, x = pos - z * I.W;
+                    const int r = (z / kRegion) * dw + x / kRegion;
+                    if (r != reg) {
+                        if (rc)
+                            atomicAdd(&I.region_new[reg], (unsigned)rc);
+                        reg = r;
+                        rc = 0;
+                    }
+                    rc++;
+                }
+            }
+            if (rc)
+                atomicAdd(&I.region_new[reg], (unsigned)rc);
+        }
+        nodes = warp_sum(nodes);
+        if ((threadIdx.x & 31) == 0 && nodes)
+            atomicAdd(&S.node_count, nodes);
+    }
+}
+
+// erase every node whose ancestor chain meets a COLLISION or NULL node within
+// numNodes + 4 hops (graph_collision.cu:32-83; an exhausted walk keeps the node)
+__global__ void __launch_bounds__(256) k_erase(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->sweep_total;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->sweep_start, n, c);
+        const State &S = states[slot];
+        if (!live(S) || !S.collision || S.node_count <= 2)
+            continue;
+        const Inst &I = insts[slot];
+        volatile int8_t *type = I.type;
+        const int cells = I.W * I.H;
+        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
+        if (base >= cells)
+            continue;
+        int8_t t[16];
+        load16(I.type + base, t);
+        for (int k = 0; k < 16; k++) {
+            const int pos = base + k;
+            if (pos >= cells || t[k] == T_NULL)
+                continue;
+            int curr = pos;
+            int i = S.node_count + 4;
+            while (i-- > 0) {
+                const int32_t p = I.parent[curr];
+                const int px = unpack_x(p), pz = unpack_z(p);
+                if (px == -1 && pz == -1)
+                    break;
+                if (px < 0 || px >= I.W || pz < 0 || pz >= I.H)
+                    break;
+                const int next = pz * I.W + px;
+                const int8_t tn = type[next];
+                if (tn == T_COLLISION || tn == T_NULL) {
+                    type[pos] = T_NULL;
+                    break;
+                }
+                curr = next;
+            }
+        }
+    }
+}
+
+// COLLISION -> NODE, child count reset, parent child count + 1
+// (graph_collision.cu:84-104)
+__global__ void __launch_bounds__(256) k_setnodes(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->sweep_total;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->sweep_start, n, c);
+        const State &S = states[slot];
+        if (!live(S) || !S.collision || S.node_count <= 2)
+            continue;
+        const Inst &I = insts[slot];
+        const int cells = I.W * I.H;
+        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
+        if (base >= cells)
+            continue;
+        int8_t t[16];
+        load16(I.type + base, t);
+        for (int k = 0; k < 16; k++) {
+            const int pos = base + k;
+            if (pos >= cells || t[k] != T_COLLISION)
+                continue;
+            I.type[pos] = T_NODE;
+            I.child[pos] = 0;
+            const int32_t p = I.parent[pos];
+            const int px = unpack_x(p), pz = unpack_z(p);
+            if (px >= 0 && px < I.W && pz >= 0 && pz < I.H)
+                atomicAdd(&I.child[pz * I.W + px], 1);
+        }
+    }
+}
+
+// TEMP count, non-NULL count, TEMP -> NODE, and the NODE list
+__global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->sweep_total;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->sweep_start, n, c);
+        State &S = states[slot];
+        if (!live(S))
+            continue;
+        const Inst &I = insts[slot];
+        const int cells = I.W * I.H;
+        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
+        int temps = 0, all = 0, cnt = 0;
+        int32_t mine[16];
+        if (base < cells) {
+            int4 v = *reinterpret_cast<const int4 *>(I.type + base);
+            int8_t *t = reinterpret_cast<int8_t *>(&v);
+            bool changed = false;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                if (base + k >= cells)
+                    continue;
+                temps += t[k] == T_TEMP;
+                all += t[k] != T_NULL;
+                if (t[k] == T_TEMP) {
+                    t[k] = T_NODE;
+                    changed = true;
+                }
+                if (t[k] == T_NODE)
+                    mine[cnt++] = base + k;
+            }
+            if (changed)
+                *reinterpret_cast<int4 *>(I.type + base) = v;
+        }
+        const int at = warp_append(&S.n_nodes, cnt);
+        for (int k = 0; k < cnt; k++)
+            I.nodes[at + k] = mine[k];
+        temps = warp_sum(temps);
+        all = warp_sum(all);
+        if ((threadIdx.x & 31) == 0) {
+            if (temps)
+                atomicAdd(&S.temp_count, temps);
+            if (all)
+                atomicAdd(&S.all_count, all);
+        }
+    }
+}
+
+// best connection of one graph node to a precomputed goal-connected cell in
+// its window (graph_check_goal_reached.cu:17-70), plus checkGoalReached for
+// the node (graph_best_node.cu:181-222)
+struct GoalLane {
+    HermTask h;
+    int w, wtotal, nx, zlo, xlo;
+    bool in_task;
+    int x, z;
+    float heading, cost, gd_cost_cur;
+    int cell_cur;
+    long long best;
+    int best_cell;
+    float best_seg;
+    const Inst *I;
+    const volatile long long *global_best;
+    bool prune;
+
+    __device__ int advance(const Foot &f, unsigned long long &probes)
+    {
+        while (true) {
+            if (!in_task) {
+                if (w >= wtotal)
+                    return 0;
+                const int zp = zlo + w / nx, xp = xlo + w % nx;
+                w += 32;
+                if (zp < 0 || zp >= I->H)
+                    continue;
+                if (xp < 0 || xp >= I->W)
+                    continue;
+                const int cell = zp * I->W + xp;
+                if (!(I->gd_flag[cell] > 0))
+                    continue;
+                const float gdc = I->gd_cost[cell];
+                if (prune) {
+                    // the connection costs at least cost + 1 (the first sample)
+                    const float lb_total = (cost + 1.0f) + gdc;
+                    const long long lb = __float2ll_rd(100 * lb_total);
+                    if (lb > *global_best)
+                        continue;
+                }
+                h.init(*I, f, I->max_curvature, x, z, heading, xp, zp, I->gd_heading[cell], 1, cost);
+                cell_cur = cell;
+                gd_cost_cur = gdc;
+                in_task = true;
+            }
+            if (h.advance(f, probes))
+                return 1;
+            in_task = false;
+            if (h.ok) {
+                const float c = h.nodeCost;
+                const float total = c + gd_cost_cur;
+                const long long lc = __float2ll_rd(100 * total);
+                if (lc <= best) {
+                    best = lc;
+                    best_cell = cell_cur;
+                    best_seg = c;
+                }
+            }
+        }
+    }
+    __device__ bool resolve(bool ok)
+    {
+        if (!h.resolve(ok))
+            in_task = false;
+        return true;
+    }
+    __device__ float probe_angle() const { return h.pend_heading; }
+};
+
+__device__ __forceinline__ int window_count(int c, float r, int &lo)
+{
+    lo = (int)(c - r);
+    const float hi = c + r;
+    const int k0 = (int)ceilf(hi);
+    return k0 > lo ? k0 - lo : 0;
+}
+
+__global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, Sched *sc,
+                                              int smem_words)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_chunk;
+    const int n = sc->n_slots;
+    const int total = sc->node_start[n];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Stage sg{-1, false, 0u};
+    if (threadIdx.x == 0)
+        mbar_init(&bar, 1);
+    __syncthreads();
+    while (true) {
+        if (threadIdx.x == 0)
+            s_chunk = (int)atomicAdd(&sc->grab[1], 1u);
+        __syncthreads();
+        const int c = s_chunk;
+        __syncthreads();
+        if (c >= total)
+            break;
+        const int slot = find_slot(sc->node_start, n, c);
+        const Inst &I = insts[slot];
+        State &S = states[slot];
+        const uint32_t *blk, *clr;
+        stage_for(I, slot, sg, smem, smem_words, &bar, states, blk, clr);
+        const Foot f = foot_of(I, blk, clr);
+        const int idx = (c - sc->node_start[slot]) * kNodeChunk + warp;
+        const bool has = idx < S.n_nodes;  // uniform across the warp
+        unsigned long long probes = 0;
+        if (has) {
+            const int pos = I.nodes[idx];
+            GoalLane g;
+            g.I = &I;
+            g.z = pos / I.W;
+            g.x = pos - g.z * I.W;
+            g.heading = I.heading[pos];
+            g.cost = I.cost[pos];
+            if (lane == 0) {
+                const double dx = I.goal_x - g.x, dz = I.goal_z - g.z;
+                if (!(sqrt(dx * dx + dz * dz) > I.dist_tol) &&
+                    fabsf(g.heading - I.goal_heading) <= I.heading_tol)
+                    S.goal_reached = 1;
+            }
+            const int nz = window_count(g.z, I.dist_tol, g.zlo);
+            g.nx = window_count(g.x, I.dist_tol, g.xlo);
+            g.wtotal = g.nx > 0 ? nz * g.nx : 0;
+            g.w = lane;
+            g.in_task = false;
+            g.best = kBigCost;
+            g.best_cell = -1;
+            g.best_seg = 0.0f;
+            g.global_best = &S.best;
+            g.prune = I.intrinsic == nullptr;
+            run_warp(g, true, f, probes, [](const GoalLane &q) { return q.h.last_x; },
+                     [](const GoalLane &q) { return q.h.last_z; });
+            // warp minimum of best, ties to the highest cell index
+            long long b = g.best;
+            int bc = g.best_cell;
+            float bs = g.best_seg;
+            for (int o = 16; o; o >>= 1) {
+                const long long ob = __shfl_xor_sync(kFull, b, o);
+                const int oc = __shfl_xor_sync(kFull, bc, o);
+                const float os = __shfl_xor_sync(kFull, bs, o);
+                if (ob < b || (ob == b && oc > bc)) {
+                    b = ob;
+                    bc = oc;
+                    bs = os;
+                }
+            }
+            if (lane == 0) {
+                I.node_best[idx] = b;
+                I.node_best_cell[idx] = bc;
+                I.node_best_seg[idx] = bs;
+                if (b < kBigCost)
+                    atomicMin(&S.best, b);
+            }
+        }
+        probes = warp_sum64(probes);
+        if (lane == 0 && probes)
+            atomicAdd(&S.probes, probes);
+    }
+    stage_drain(sg, &bar);
+}
+
+// among listed nodes with the minimum, the highest node cell index wins
+__global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const long entries = (long)sc->node_start[n] * kNodeChunk;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < entries;
+         e += (long)gridDim.x * blockDim.x) {
+        const int chunk = (int)(e / kNodeChunk);
+        const int slot = find_slot(sc->node_start, n, chunk);
+        const Inst &I = insts[slot];
+        State &S = states[slot];
+        const int idx = (chunk - sc->node_start[slot]) * kNodeChunk + (int)(e % kNodeChunk);
+        if (idx >= S.n_nodes || S.best >= kBigCost)
+            continue;
+        if (I.node_best[idx] == S.best) {
+            const unsigned long long key =
+                ((unsigned long long)(unsigned)I.nodes[idx] << 32) | (unsigned)idx;
+            atomicMax(&S.winner, key);
+        }
+    }
+}
+
+// the host-side tail of FastRRT::loop, per slot
+__global__ void k_finish(const Inst *insts, State *states, int n)
+{
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= n)
+        return;
+    State &S = states[slot];
+    if (!live(S))
+        return;
+    const Inst &I = insts[slot];
+    S.last_expanded = S.temp_count;
+    if (S.temp_count == 0 && S.all_count == 0) {
+        // empty graph: the start is added again (fastrrt.cpp:132-139)
+        grid_add(I, I.start_x, I.start_z, I.start_heading, -1, -1, 0.0f);
+    } else if (S.best < kBigCost) {
+        // fastrrt.cpp:145-167
+        const int idx = (int)(S.winner & 0xffffffffu);
+        const int ppos = I.nodes[idx];
+        const int pz = ppos / I.W, px = ppos - pz * I.W;
+        const int cell = I.node_best_cell[idx];
+        const int cz = cell / I.W, cx = cell - cz * I.W;
+        const float base = I.cost[ppos];
+        const float child_heading = I.gd_heading[cell];
+        grid_add(I, cx, cz, child_heading, px, pz, I.node_best_seg[idx] + base);
+        const float child_cost = child_heading + base;
+        grid_add(I, I.goal_x, I.goal_z, I.goal_heading, cx, cz, child_cost);
+        if (I.goal_x >= 0 && I.goal_x < I.W && I.goal_z >= 0 && I.goal_z < I.H &&
+            !(0.0 > I.dist_tol) && fabsf(I.goal_heading - I.goal_heading) <= I.heading_tol)
+            S.goal_reached = 1;
+        S.found = 1;
+    }
+    S.loops++;
+    S.iter++;
+    if (S.goal_reached && I.stop_on_goal)
+        S.done = 1;
+    else if (I.max_iter > 0 && S.loops >= I.max_iter)
+        S.done = 1;
+    else if (S.deadline_ns > 0 && global_ns() > S.deadline_ns)
+        S.done = 1;
+    // per-iteration resets
+    S.n_cand = 0;
+    S.node_count = 0;
+    S.temp_count = 0;
+    S.all_count = 0;
+    S.n_nodes = 0;
+    S.collision = 0;
+    S.best = kBigCost;
+    S.winner = 0;
+    if (I.smart) {
+        const int regions = (I.W / kRegion + 1) * (I.H / kRegion + 1);
+        for (int r = 0; r < regions; r++) {
+            I.region_count[r] = I.region_new[r];
+            I.region_new[r] = 0;
+        }
+    }
+}
+
+void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
+                      const Launch &L, cudaStream_t st)
+{
+    const size_t smem = (size_t)L.smem_words * 2 * 4;
+    k_scan<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 0);
+    k_expand<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    k_apply<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_post<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_erase<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_setnodes<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_accept<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 1);
+    k_goal<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    k_select<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_finish<<<(n_slots + 127) / 128, 128, 0, st>>>(d_inst, d_state, n_slots);
+}
+
+// ---------------------------------------------------------------------------
+// standalone goal check, path extraction, optimisation, validation
+// ---------------------------------------------------------------------------
+
+// checkGoalReached (graph_best_node.cu:181-250); sticky flag
+__global__ void k_goal_check(const Inst *insts, State *states, const int *slots)
+{
+    const int slot = slots[blockIdx.y];
+    const Inst &I = insts[slot];
+    State &S = states[slot];
+    if (S.goal_reached)
+        return;
+    const long cells = (long)I.W * I.H;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < cells;
+         pos += (long)gridDim.x * blockDim.x) {
+        if (I.type[pos] != T_NODE)
+            continue;
+        const int z = (int)(pos / I.W), x = (int)(pos - (long)z * I.W);
+        const double dx = I.goal_x - x, dz = I.goal_z - z;
+        if (sqrt(dx * dx + dz * dz) > I.dist_tol)
+            continue;
+        if (fabsf(I.heading[pos] - I.goal_heading) <= I.heading_tol)
+            S.goal_reached = 1;
+    }
+}
+
+void launch_goal_check(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                       int max_cells, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_goal_check<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_state, d_slots);
+}
+
+// findBestNode pass 1 (graph_best_node.cu:15-75): key = cost * 2^32 +
+// (2^32 - 1 - cell), so the minimum is the lowest cost and, among equal
+// costs, the highest cell index (the last writer of the sequential pass 2)
+__global__ void k_best_node(const Inst *insts, const int *slots, long long *keys)
+{
+    const int k = blockIdx.y;
+    const Inst &I = insts[slots[k]];
+    const long cells = (long)I.W * I.H;
+    const Foot f = foot_of(I, I.blocked, I.clear);
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < cells;
+         pos += (long)gridDim.x * blockDim.x) {
+        if (I.type[pos] != T_NODE)
+            continue;
+        const int z = (int)(pos / I.W), x = (int)(pos - (long)z * I.W);
+        const int dx = I.goal_x - x, dz = I.goal_z - z;
+        const float dist = sqrtf(dx * dx + dz * dz);
+        if (dist > I.dist_tol)
+            continue;
+        const float heading = I.heading[pos];
+        if (fabsf(heading - I.goal_heading) > I.heading_tol)
+            continue;
+        unsigned long long pr = 0;
+        if (!feasible_scalar(f, x, z, heading, pr))
+            continue;
+        // __compute_cost_findBestNode (graph_best_node.cu:16-18)
+        const long long cost = __float2ll_rd(1 * dist + 3 * kToDeg * heading + 1 * I.cost[pos]);
+        const long long key = cost * 4294967296LL + (long long)(0xffffffffu - (unsigned)pos);
+        atomicMin(&keys[k], key);
+    }
+}
+
+// parent walk from the best node (fastrrt.cpp:214-231), one thread per slot
+__global__ void k_walk(const Inst *insts, const int *slots, int n, const long long *keys,
+                       float *paths, int *path_n, int cap)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const Inst &I = insts[slots[k]];
+    float *out = paths + (long)k * cap * 3;
+    path_n[k] = 0;
+    const long long key = keys[k];
+    if (key == LLONG_MAX)
+        return;
+    const unsigned inv = (unsigned)(key & 0xffffffffLL);
+    int pos = (int)(0xffffffffu - inv);
+    int bx = pos % I.W, bz = pos / I.W;
+    int m = 0;
+    long i = 0;
+    while (bx != -1 && bz != -1) {
+        if (m < cap) {
+            out[3 * m] = (float)bx;
+            out[3 * m + 1] = (float)bz;
+            out[3 * m + 2] = I.heading[(long)bz * I.W + bx];
+        }
+        m++;
+        // CudaGraph::getParent (graph.cu:446-453)
+        int nx = -1, nz = -1;
+        if (bx >= 0 && bx < I.W && bz >= 0 && bz < I.H && I.type[(long)bz * I.W + bx] != T_NULL) {
+            const int32_t p = I.parent[(long)bz * I.W + bx];
+            nx = unpack_x(p);
+            nz = unpack_z(p);
+        }
+        bx = nx;
+        bz = nz;
+        if (i++ >= 1000000) {
+            m = 0;
+            break;
+        }
+    }
+    if (m > cap)
+        m = cap;
+    for (int a = 0, b = m - 1; a < b; a++, b--)
+        for (int q = 0; q < 3; q++) {
+            const float t = out[3 * a + q];
+            out[3 * a + q] = out[3 * b + q];
+            out[3 * b + q] = t;
+        }
+    path_n[k] = m;
+}
+
+__global__ void k_fill_keys(long long *keys, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        keys[k] = LLONG_MAX;
+}
+
+void launch_extract_paths(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                          int max_cells, float *d_paths, int *d_path_n, long long *d_keys, int cap,
+                          cudaStream_t st)
+{
+    (void)d_state;
+    if (n <= 0)
+        return;
+    k_fill_keys<<<(n + 255) / 256, 256, 0, st>>>(d_keys, n);
+    k_best_node<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, d_keys);
+    k_walk<<<(n + 63) / 64, 64, 0, st>>>(d_inst, d_slots, n, d_keys, d_paths, d_path_n, cap);
+}
+
+// optimizePathLoop (graph_optimization.cu:25-56, 92-195): every pair (i, j),
+// j >= i + 2, of path waypoints is tested with checkDirectConnectionToGoal
+struct PairLane {
+    HermTask h;
+    __device__ int advance(const Foot &f, unsigned long long &p) { return h.advance(f, p); }
+    __device__ bool resolve(bool ok) { return h.resolve(ok); }
+    __device__ float probe_angle() const { return h.pend_heading; }
+};
+
+__global__ void k_opt_pairs(const Inst *insts, int slot, const float *path, const int *path_n,
+                            float *newcost)
+{
+    const Inst &I = insts[slot];
+    const int n = *path_n;
+    const long pairs = (long)n * n;
+    const Foot f = foot_of(I, I.blocked, I.clear);
+    unsigned long long probes = 0;
+    for (long base = (long)blockIdx.x * blockDim.x; base < pairs; base += (long)gridDim.x * blockDim.x) {
+        const long p = base + threadIdx.x;
+        const int i = (int)(p / (n > 0 ? n : 1)), j = (int)(p - (long)i * (n > 0 ? n : 1));
+        const bool has = p < pairs && j >= i + 2 && i < n - 2;
+        PairLane t;
+        if (has) {
+            const int x = (int)path[3 * i], z = (int)path[3 * i + 1];
+            t.h.init(I, f, I.max_curvature, x, z, path[3 * i + 2], (int)path[3 * j],
+                     (int)path[3 * j + 1], path[3 * j + 2], 1, I.cost[(long)z * I.W + x]);
+        }
+        run_warp(t, has, f, probes, [](const PairLane &q) { return q.h.last_x; },
+                 [](const PairLane &q) { return q.h.last_z; });
+        if (p < pairs)
+            newcost[p] = has ? t.h.result() : -1.0f;
+    }
+}
+
+__global__ void k_opt_select(const Inst *insts, int slot, float *path, int *path_n,
+                             float *newcost, int *changed, int cap)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    const Inst &I = insts[slot];
+    int n = *path_n;
+    *changed = 0;
+    // path[].w = getCost of each waypoint (convertPlannedPath, graph_optimization.cu:76-90)
+    float maxGain = -1;
+    int mg = -1, mg_j = -1;
+    float mg_cost = 0;
+    for (int i = 0; i < n - 2; i++) {
+        int sel = -1;
+        float sel_cost = 0, sel_gain = 0;
+        for (int j = i + 2; j < n; j++) {
+            const int xj = (int)path[3 * j], zj = (int)path[3 * j + 1];
+            const float cur = (xj >= 0 && xj < I.W && zj >= 0 && zj < I.H) ? I.cost[(long)zj * I.W + xj] : -1.0f;
+            const float nc = newcost[(long)i * n + j];
+            if (nc > 0 && nc < cur) {
+                sel = j;
+                sel_cost = nc;
+                sel_gain = cur - nc;
+            }
+        }
+        if (sel >= 0 && maxGain < sel_gain) {
+            maxGain = sel_gain;
+            mg = i;
+            mg_j = sel;
+            mg_cost = sel_cost;
+        }
+    }
+    if (mg < 0)
+        return;
+    const int next_pos = mg_j;
+    // the waypoint costs (path[].w) travel in newcost[0, n) from here on,
+    // because the grid is cleared before the path is added back
+    for (int j = 0; j < n; j++) {
+        const int xj = (int)path[3 * j], zj = (int)path[3 * j + 1];
+        newcost[j] = (xj >= 0 && xj < I.W && zj >= 0 && zj < I.H) ? I.cost[(long)zj * I.W + xj] : -1.0f;
+    }
+    if (next_pos > mg + 1) {
+        newcost[next_pos] = mg_cost;
+        const int rm = next_pos - mg - 1;
+        for (int i = mg + 1; i + rm < n; ++i) {
+            path[3 * i] = path[3 * (i + rm)];
+            path[3 * i + 1] = path[3 * (i + rm) + 1];
+            path[3 * i + 2] = path[3 * (i + rm) + 2];
+            newcost[i] = newcost[i + rm];
+        }
+        n -= rm;
+    }
+    *path_n = n;
+    *changed = 1;
+    (void)cap;
+}
+
+__global__ void k_opt_rebuild(const Inst *insts, int slot, const float *path, const int *path_n,
+                              const float *costs, const int *changed)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0 || !*changed)
+        return;
+    const Inst &I = insts[slot];
+    const int n = *path_n;
+    int ppx = (int)path[0], ppz = (int)path[1];
+    grid_add(I, ppx, ppz, path[2], -1, -1, costs[0]);
+    for (int i = 1; i < n; i++) {
+        const int x = (int)path[3 * i], z = (int)path[3 * i + 1];
+        grid_add(I, x, z, path[3 * i + 2], ppx, ppz, costs[i]);
+        ppx = x;
+        ppz = z;
+    }
+}
+
+__global__ void k_clear_types_if(const Inst *insts, int slot, const int *changed)
+{
+    if (!*changed)
+        return;
+    const Inst &I = insts[slot];
+    const long cells = (long)I.W * I.H;
+    for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < cells;
+         base += (long)gridDim.x * blockDim.x * 16)
+        *reinterpret_cast<int4 *>(I.type + base) = make_int4(0, 0, 0, 0);
+}
+
+void launch_optimize(const Inst *d_inst, int slot, int cells, float *d_path, int *d_path_n,
+                     float *d_newcost, int *d_changed, int cap, const Launch &L, cudaStream_t st)
+{
+    const long pairs = (long)cap * cap;
+    int grid = (int)((pairs + 255) / 256);
+    if (grid > L.sms * 8)
+        grid = L.sms * 8;
+    k_opt_pairs<<<grid, 256, 0, st>>>(d_inst, slot, d_path, d_path_n, d_newcost);
+    k_opt_select<<<1, 32, 0, st>>>(d_inst, slot, d_path, d_path_n, d_newcost, d_changed, cap);
+    k_clear_types_if<<<(cells / 16 + 255) / 256, 256, 0, st>>>(d_inst, slot, d_changed);
+    k_opt_rebuild<<<1, 32, 0, st>>>(d_inst, slot, d_path, d_path_n, d_newcost, d_changed);
+}
+
+// count of one node type (type < 0: all non-NULL) per listed slot
+__global__ void k_count(const Inst *insts, const int *slots, int type, unsigned *out)
+{
+    const Inst &I = insts[slots[blockIdx.y]];
+    const long cells = (long)I.W * I.H;
+    int c = 0;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < cells;
+         pos += (long)gridDim.x * blockDim.x) {
+        const int8_t t = I.type[pos];
+        c += type < 0 ? t != T_NULL : t == type;
+    }
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(&out[blockIdx.y], (unsigned)c);
+}
+
+void launch_count(const Inst *d_inst, const int *d_slots, int n, int max_cells, int type,
+                  unsigned *d_out, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    cudaMemsetAsync(d_out, 0, sizeof(unsigned) * n, st);
+    k_count<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, type, d_out);
+}
+
+// checkGraphIsConsistent (graph_check_dag_consistency.cpp:33-76) in parallel:
+// every non-NULL cell walks at most count(NODE) + 4 parents
+__global__ void k_dag(const Inst *insts, const int *slots, const unsigned *node_counts, int *valid)
+{
+    const int k = blockIdx.y;
+    const Inst &I = insts[slots[k]];
+    const long cells = (long)I.W * I.H;
+    const int maxLoop = (int)node_counts[k] + 4;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < cells;
+         pos += (long)gridDim.x * blockDim.x) {
+        if (I.type[pos] == T_NULL)
+            continue;
+        int cx = (int)(pos % I.W), cz = (int)(pos / I.W);
+        int i = maxLoop;
+        bool bad = false;
+        while (i-- > 0) {
+            int px = -1, pz = -1;
+            if (I.type[(long)cz * I.W + cx] != T_NULL) {
+                const int32_t p = I.parent[(long)cz * I.W + cx];
+                px = unpack_x(p);
+                pz = unpack_z(p);
+            }
+            if (px == cx && pz == cz) {
+                bad = true;
+                break;
+            }
+            if (px == -1)
+                break;
+            const bool in = px >= 0 && px < I.W && pz >= 0 && pz < I.H;
+            const int pt = in ? I.type[(long)pz * I.W + px] : -1;
+            if (pt != T_NODE && pt != T_COLLISION && pt != T_CONNECT_TO_GOAL) {
+                bad = true;
+                break;
+            }
+            cx = px;
+            cz = pz;
+        }
+        // the reference reports an inconsistency whenever the counter ends <= 0
+        if (bad || i <= 0)
+            valid[k] = 0;
+    }
+}
+
+__device__ __forceinline__ float wrap_pi(float a)
+{
+    const float tp = (float)(2 * kPi);
+    while (a > (float)kPi)
+        a -= tp;
+    while (a < -(float)kPi)
+        a += tp;
+    return a;
+}
+
+// per-path checks, one thread per slot (the path is short)
+__global__ void k_path_check(const Inst *insts, const int *slots, int n, const float *paths,
+                             const int *path_n, int cap, int *valid, float *length)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const Inst &I = insts[slots[k]];
+    const float *p = paths + (long)k * cap * 3;
+    const int m = path_n[k];
+    length[k] = 0.0f;
+    if (m < 2 || (int)p[0] != I.start_x || (int)p[1] != I.start_z) {
+        valid[k] = 0;
+        return;
+    }
+    const Foot f = foot_of(I, I.blocked, I.clear);
+    const double steer = tan(I.max_steer), beta = atan(steer / 2);
+    double kappa = cos(beta) * steer / (2 * I.lr);
+    if (I.max_curvature > kappa)
+        kappa = I.max_curvature;
+    if (0.8 > kappa)
+        kappa = 0.8;
+    float len = 0.0f;
+    bool ok = true;
+    for (int i = 0; i < m && ok; i++) {
+        const int x = (int)p[3 * i], z = (int)p[3 * i + 1];
+        const float h = p[3 * i + 2];
+        if (x < 0 || x >= I.W || z < 0 || z >= I.H) {
+            ok = false;
+            break;
+        }
+        const bool in_ego = x >= I.lbx && x <= I.ubx && z >= I.ubz && z <= I.lbz;
+        unsigned long long pr = 0;
+        if (!in_ego && !feasible_scalar(f, x, z, h, pr)) {
+            ok = false;
+            break;
+        }
+        if (i > 0) {
+            const int px = (int)p[3 * (i - 1)], pz = (int)p[3 * (i - 1) + 1];
+            if (px == x && pz == z) {
+                ok = false;
+                break;
+            }
+            const int32_t par = I.parent[(long)z * I.W + x];
+            if (I.type[(long)z * I.W + x] == T_NULL || unpack_x(par) != px || unpack_z(par) != pz) {
+                ok = false;
+                break;
+            }
+            const double chord = sqrt((double)(x - px) * (x - px) + (double)(z - pz) * (z - pz));
+            const float dh = wrap_pi(h - p[3 * (i - 1) + 2]);
+            if (fabs(dh) > (kPi / 2) * kappa * chord + 1e-3) {
+                ok = false;
+                break;
+            }
+            len += sqrtf((float)((x - px) * (x - px) + (z - pz) * (z - pz)));
+        }
+    }
+    if (ok) {
+        const int lx = (int)p[3 * (m - 1)], lz = (int)p[3 * (m - 1) + 1];
+        const double gdx = lx - I.goal_x, gdz = lz - I.goal_z;
+        if (sqrt(gdx * gdx + gdz * gdz) > I.dist_tol)
+            ok = false;
+        if (fabsf(p[3 * (m - 1) + 2] - I.goal_heading) > I.heading_tol)
+            ok = false;
+    }
+    if (!ok)
+        valid[k] = 0;
+    length[k] = len;
+}
+
+__global__ void k_fill_int(int *v, int n, int value)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        v[k] = value;
+}
+
+void launch_validate(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_cells,
+                     const float *d_paths, const int *d_path_n, int cap, unsigned *d_counts,
+                     int *d_valid, float *d_length, cudaStream_t st)
+{
+    (void)d_state;
+    if (n <= 0)
+        return;
+    k_fill_int<<<(n + 255) / 256, 256, 0, st>>>(d_valid, n, 1);
+    launch_count(d_inst, d_slots, n, max_cells, T_NODE, d_counts, st);
+    k_dag<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, d_counts, d_valid);
+    k_path_check<<<(n + 63) / 64, 64, 0, st>>>(d_inst, d_slots, n, d_paths, d_path_n, cap, d_valid,
+                                               d_length);
+}
+
+// ---------------------------------------------------------------------------
+// per-candidate microbenchmarks (one frame slot)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_candidates(const Inst *insts, int slot, int n,
+                                                    const int32_t *sx, const int32_t *sz,
+                                                    const float *steer, const float *len,
+                                                    float velocity, float4 *out,
+                                                    unsigned long long *probes_out, int smem_words)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    const Inst &I = insts[slot];
+    const uint32_t *blk = I.blocked, *clr = I.clear;
+    unsigned phase = 0;
+    if (smem_words > 0 && I.mask_words <= smem_words) {
+        if (threadIdx.x == 0)
+            mbar_init(&bar, 1);
+        __syncthreads();
+        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase)) {
+            blk = smem;
+            clr = smem + smem_words;
+        } else {
+            for (long k = 0; k < kWaitLimit; k++)
+                if (mbar_try_wait(&bar, phase ^ 1u))
+                    break;
+        }
+    }
+    const Foot f = foot_of(I, blk, clr);
+    unsigned long long probes = 0;
+    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
+        const long i = base + threadIdx.x;
+        const bool has = i < n;
+        KinLane t;
+        if (has) {
+            const long pos = (long)sz[i] * I.W + sx[i];
+            t.k.init(I, sx[i], sz[i], steer[i], len[i], velocity, I.heading[pos], I.cost[pos]);
+        }
+        run_warp(t, has, f, probes, [](const KinLane &q) { return q.k.pend_x; },
+                 [](const KinLane &q) { return q.k.pend_z; });
+        if (has)
+            out[i] = t.k.ok ? make_float4((float)t.k.last_x, (float)t.k.last_z, t.k.nodeCost, t.k.heading)
+                            : make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
+    }
+    probes = warp_sum64(probes);
+    if ((threadIdx.x & 31) == 0 && probes && probes_out)
+        atomicAdd(probes_out, probes);
+}
+
+void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, const int32_t *sz,
+                       const float *steer, const float *len, float velocity, float4 *out,
+                       unsigned long long *probes, const Launch &L, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    int grid = (n + 255) / 256;
+    if (grid > L.work_blocks)
+        grid = L.work_blocks;
+    const size_t smem = (size_t)L.smem_words * 2 * 4;
+    k_candidates<<<grid, 256, smem, st>>>(d_inst, slot, n, sx, sz, steer, len, velocity, out, probes,
+                                          L.smem_words);
+}
+
+__global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, int n, const int32_t *x,
+                                                 const int32_t *z, const float *lh, const int32_t *gx,
+                                                 const int32_t *gz, const float *gh, float maxc,
+                                                 int safe, float *out, unsigned long long *probes_out,
+                                                 int smem_words)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    const Inst &I = insts[slot];
+    const uint32_t *blk = I.blocked, *clr = I.clear;
+    unsigned phase = 0;
+    if (smem_words > 0 && I.mask_words <= smem_words) {
+        if (threadIdx.x == 0)
+            mbar_init(&bar, 1);
+        __syncthreads();
+        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase)) {
+            blk = smem;
+            clr = smem + smem_words;
+        } else {
+            for (long k = 0; k < kWaitLimit; k++)
+                if (mbar_try_wait(&bar, phase ^ 1u))
+                    break;
+        }
+    }
+    const Foot f = foot_of(I, blk, clr);
+    unsigned long long probes = 0;
+    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
+        const long i = base + threadIdx.x;
+        const bool has = i < n;
+        PairLane t;
+        if (has)
+            t.h.init(I, f, maxc, x[i], z[i], lh[i], gx[i], gz[i], gh[i], safe,
+                     I.cost[(long)z[i] * I.W + x[i]]);
+        run_warp(t, has, f, probes, [](const PairLane &q) { return q.h.last_x; },
+                 [](const PairLane &q) { return q.h.last_z; });
+        if (has)
+            out[i] = t.h.result();
+    }
+    probes = warp_sum64(probes);
+    if ((threadIdx.x & 31) == 0 && probes && probes_out)
+        atomicAdd(probes_out, probes);
+}
+
+void launch_hermite_pairs(const Inst *d_inst, int slot, int n, const int32_t *x, const int32_t *z,
+                          const float *lh, const int32_t *gx, const int32_t *gz, const float *gh,
+                          float max_curvature, int safe, float *out, unsigned long long *probes,
+                          const Launch &L, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    int grid = (n + 255) / 256;
+    if (grid > L.work_blocks)
+        grid = L.work_blocks;
+    const size_t smem = (size_t)L.smem_words * 2 * 4;
+    k_hermite<<<grid, 256, smem, st>>>(d_inst, slot, n, x, z, lh, gx, gz, gh, max_curvature, safe, out,
+                                       probes, L.smem_words);
+}
+
+__global__ void k_feasible(const Inst *insts, int slot, int n, const int32_t *x, const int32_t *z,
+                           const float *a, int32_t *out, unsigned long long *probes_out)
+{
+    const Inst &I = insts[slot];
+    const Foot f = foot_of(I, I.blocked, I.clear);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long pr = 0;
+    if (i < n)
+        out[i] = feasible_scalar(f, x[i], z[i], a[i], pr) ? 1 : 0;
+    pr = warp_sum64(pr);
+    if ((threadIdx.x & 31) == 0 && pr && probes_out)
+        atomicAdd(probes_out, pr);
+}
+
+void configure_kernels(int smem_bytes)
+{
+    cudaFuncSetAttribute(k_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    cudaFuncSetAttribute(k_goal, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    cudaFuncSetAttribute(k_direct_goal, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    cudaFuncSetAttribute(k_candidates, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    cudaFuncSetAttribute(k_hermite, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+}
+
+void launch_feasible(const Inst *d_inst, int slot, int n, const int32_t *x, const int32_t *z,
+                     const float *a, int32_t *out, unsigned long long *probes, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_feasible<<<(n + 255) / 256, 256, 0, st>>>(d_inst, slot, n, x, z, a, out, probes);
+}
+
+}  // namespace frrt

@@ -1,0 +1,78 @@
+// frrt_kernels.cuh -- kernel launch interface of the planner engine.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "frrt_common.cuh"
+
+namespace frrt {
+
+constexpr int kSweepCells = 4096;   // cells per sweep chunk (256 threads x 16)
+constexpr int kCandChunk = 256;     // candidates per expansion chunk (one per thread)
+constexpr int kNodeChunk = 8;       // listed nodes per goal-search chunk (one per warp)
+constexpr int32_t kClaimFree = 0x7F7F7F7F;
+
+// Scheduling tables shared by the iteration kernels (device memory).
+struct Sched {
+    int n_slots;
+    int sweep_total;          // total sweep chunks
+    int *sweep_start;         // [n_slots + 1] prefix of sweep chunks per slot
+    int *cand_start;          // [n_slots + 1] prefix of candidate chunks per slot
+    int *node_start;          // [n_slots + 1] prefix of node chunks per slot
+    unsigned *grab;           // [4] dynamic work counters
+};
+
+struct Launch {
+    int sms;                  // multiprocessors
+    int sweep_blocks;         // grid of the sweep kernels
+    int work_blocks;          // grid of the persistent expansion / goal kernels
+    int smem_words;           // words per mask staged in shared memory (0 = global masks)
+};
+
+// allows `smem_bytes` of dynamic shared memory on the mask-staging kernels
+void configure_kernels(int smem_bytes);
+
+// frame preparation for one slot: obstacle and clear masks
+void launch_frame_masks(const Inst &h, const float *d_class_costs, int n_classes,
+                        uint32_t *d_blocked, uint32_t *d_clear, uint32_t *d_rowdil,
+                        int *d_bad_class, cudaStream_t st);
+// goal direct-connection precompute for the n slots listed in d_slots
+void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                        int max_cells, float max_curvature, const Launch &L, cudaStream_t st);
+// search_init for listed slots: reset node types, add the start, reset state
+void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                        int max_cells, int reset_regions, cudaStream_t st);
+// one planning iteration (loop()) over all active slots
+void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
+                      const Launch &L, cudaStream_t st);
+// standalone goal check (checkGoalReached) for listed slots
+void launch_goal_check(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                       int max_cells, cudaStream_t st);
+// best node (findBestNode) + parent walk into per-slot path buffers of
+// `cap` (x, z, heading) triples; d_path_n[k] gets the count
+void launch_extract_paths(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                          int max_cells, float *d_paths, int *d_path_n, long long *d_keys, int cap,
+                          cudaStream_t st);
+// one path_optimize() pass on the path of one slot; d_changed gets 0/1
+void launch_optimize(const Inst *d_inst, int slot, int cells, float *d_path, int *d_path_n,
+                     float *d_newcost, int *d_changed, int cap, const Launch &L, cudaStream_t st);
+// validator over listed slots: DAG + waypoint footprint + curvature + goal
+void launch_validate(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_cells,
+                     const float *d_paths, const int *d_path_n, int cap, unsigned *d_counts,
+                     int *d_valid, float *d_length, cudaStream_t st);
+// count cells of `type` (type < 0: all non-NULL) for listed slots into d_out[k]
+void launch_count(const Inst *d_inst, const int *d_slots, int n, int max_cells, int type,
+                  unsigned *d_out, cudaStream_t st);
+
+// per-candidate microbenchmarks over one frame slot
+void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, const int32_t *sz,
+                       const float *steer, const float *len, float velocity, float4 *out,
+                       unsigned long long *probes, const Launch &L, cudaStream_t st);
+void launch_hermite_pairs(const Inst *d_inst, int slot, int n, const int32_t *x, const int32_t *z,
+                          const float *lh, const int32_t *gx, const int32_t *gz, const float *gh,
+                          float max_curvature, int safe, float *out, unsigned long long *probes,
+                          const Launch &L, cudaStream_t st);
+void launch_feasible(const Inst *d_inst, int slot, int n, const int32_t *x, const int32_t *z,
+                     const float *a, int32_t *out, unsigned long long *probes, cudaStream_t st);
+
+}  // namespace frrt

@@ -1,0 +1,187 @@
+/*
+ * fastrrt_b200.h -- C ABI of the B200 FastRRT planner (libfastrrt_b200.so).
+ *
+ * Part 1 keeps the reference's planner ABI (out0/FastRRT src/python_bind.cpp)
+ * name for name, so the reference's ctypes layer binds it unchanged.  The
+ * one difference is the frame argument of set_plan_data: the reference takes
+ * a driveless SearchFrame*, this library takes a handle from
+ * fastrrt_frame_create*().  Errors never cross the ABI as C++ exceptions;
+ * calls that fail return NULL / false / a negative status and leave a message
+ * for fastrrt_last_error().
+ *
+ * Part 2 adds frame handles and deterministic seeding; part 3 the
+ * per-candidate kernels (kinematic expansion, Hermite connection, footprint)
+ * used for bit-exact parity and microbenchmarks; part 4 the batched planner
+ * that plans many instances in one CUDA graph per iteration; part 5 the
+ * served planner.
+ */
+#ifndef FASTRRT_B200_H
+#define FASTRRT_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- part 1: the reference planner ABI --------------------------------- */
+
+/* replaces fastrrt_initialize (src/python_bind.cpp:7-30).  class_costs[0] is
+ * the class count followed by the costs; like the reference, the frame's own
+ * class costs are what the planner uses. */
+void *fastrrt_initialize(int width, int height, float perceptionWidthSize_m,
+                         float perceptionHeightSize_m, float maxSteeringAngle_deg,
+                         float vehicleLength, int lowerBound_x, int lowerBound_z,
+                         int upperBound_x, int upperBound_z, float *classCosts,
+                         float max_curvature);
+/* replaces fastrrt_destroy (src/python_bind.cpp:32-36) */
+void fastrrt_destroy(void *ptr);
+/* replaces set_plan_data (src/python_bind.cpp:38-64); `frame` is a handle
+ * from fastrrt_frame_create*() */
+void set_plan_data(void *ptr, void *frame, int start_x, int start_z, float start_heading_rad,
+                   int goal_x, int goal_z, float goal_heading_rad, float velocity_m_s,
+                   int min_dist_x, int min_dist_z, int timeout_ms, float maxPathSize,
+                   float distToGoalTolerance, float headingErrorTolerance_rad);
+/* replaces goal_reached (src/python_bind.cpp:66-70) */
+bool goal_reached(void *ptr);
+/* replaces search_init (src/python_bind.cpp:72-76) */
+void search_init(void *ptr, bool copyIntrinsicCostsFromFrame);
+/* replaces loop (src/python_bind.cpp:77-81) */
+bool loop(void *ptr, bool smartExpansion);
+/* replaces path_optimize (src/python_bind.cpp:83-87) */
+bool path_optimize(void *ptr);
+/* replaces export_graph_nodes (src/python_bind.cpp:89-108): [n, x, z, type, ...] */
+int *export_graph_nodes(void *ptr);
+/* replaces release_export_graph_nodes (src/python_bind.cpp:109-112) */
+void release_export_graph_nodes(int *ptr);
+/* replace get_planned_path / interpolate_planned_path (src/python_bind.cpp:138-150):
+ * [n, x0, z0, heading0, ...] */
+float *get_planned_path(void *ptr);
+float *interpolate_planned_path(void *ptr);
+/* replaces release_planned_path_data (src/python_bind.cpp:152-155) */
+void release_planned_path_data(float *ptr);
+/* replaces interpolate_planned_path_p (src/python_bind.cpp:157-171) */
+float *interpolate_planned_path_p(void *ptr, float *p, int size);
+/* replaces ideal_curve (src/python_bind.cpp:173-180) */
+float *ideal_curve(void *ptr, int goal_x, int goal_z, float goal_heading_rad);
+/* replaces compute_region_debug_performance (src/python_bind.cpp:182-186) */
+void compute_region_debug_performance(void *ptr);
+/* replace save_current_graph_state / load_graph_state (src/python_bind.cpp:188-198);
+ * text dump, one line per cell: "px pz type childcount heading cost intrinsic direct" */
+void save_current_graph_state(void *ptr, const char *filename);
+void load_graph_state(void *ptr, const char *filename);
+
+/* ---- part 2: frames, seeding, errors ------------------------------------ */
+
+/* last error message of the calling thread ("" when none) */
+const char *fastrrt_last_error(void);
+/* a BEV frame: W*H class ids (uint8), class costs (cost < 0 = obstacle),
+ * optional W*H traversability bits (NULL = none) */
+void *fastrrt_frame_create(int width, int height, const uint8_t *class_ids,
+                           const float *class_costs, int n_classes, const int32_t *trav_bits);
+/* the reference SearchFrame layout: W*H float3 (class id, distance, bits) */
+void *fastrrt_frame_create_f3(int width, int height, const float *xyz, const float *class_costs,
+                              int n_classes);
+void fastrrt_frame_destroy(void *frame);
+/* expansion RNG seed (default: wall-clock milliseconds, like the reference) */
+int fastrrt_set_seed(void *ptr, uint64_t seed);
+/* footprint probes of the reference algorithm run so far (instrumentation) */
+int fastrrt_probe_count(void *ptr, uint64_t *probes);
+/* loop() calls and expansion passes run since search_init */
+int fastrrt_loop_count(void *ptr);
+
+/* ---- part 3: per-candidate kernels -------------------------------------- */
+
+/* A footprint/kinematics context over one frame: the planner's parameters
+ * (min distances are halved like CudaGraph::setSearchParams, graph.cu:306-314)
+ * and a node grid whose heading/cost per cell the candidates start from
+ * (NULL = zeros). */
+void *fastrrt_candidates_create(void *frame, int min_dist_x, int min_dist_z, int lowerBound_x,
+                                int lowerBound_z, int upperBound_x, int upperBound_z,
+                                double max_steering_rad, double lr_m, const float *heading_grid,
+                                const float *cost_grid);
+void fastrrt_candidates_destroy(void *ctx);
+/* check_kinematic_new_path (src/cuda/kinematics.cu:123-231) for n candidates;
+ * out4 = (end x, end z, cost, heading) or (-1, -1, 0, 0).  Host buffers. */
+int fastrrt_candidates_kinematic(void *ctx, int n, const int32_t *sx, const int32_t *sz,
+                                 const float *steer, const float *length, float velocity_m_s,
+                                 float *out4, uint64_t *probes);
+/* same with device pointers on `stream` (cudaStream_t, NULL = default) */
+int fastrrt_candidates_kinematic_device(void *ctx, int n, const int32_t *sx, const int32_t *sz,
+                                        const float *steer, const float *length,
+                                        float velocity_m_s, float *out4, uint64_t *probes,
+                                        void *stream);
+/* checkDirectConnectionToGoal (src/cuda/graph_direct_goal_connection.cu:16-167);
+ * out = cost or -1.  Host buffers. */
+int fastrrt_candidates_hermite(void *ctx, int n, const int32_t *x, const int32_t *z,
+                               const float *local_heading, const int32_t *goal_x,
+                               const int32_t *goal_z, const float *goal_heading,
+                               float max_curvature, int safe_zone_checked, float *out,
+                               uint64_t *probes);
+int fastrrt_candidates_hermite_device(void *ctx, int n, const int32_t *x, const int32_t *z,
+                                      const float *local_heading, const int32_t *goal_x,
+                                      const int32_t *goal_z, const float *goal_heading,
+                                      float max_curvature, int safe_zone_checked, float *out,
+                                      uint64_t *probes, void *stream);
+/* __computeFeasibleForAngle (src/cuda/path_feasible.cu:18-78). Host buffers. */
+int fastrrt_candidates_feasible(void *ctx, int n, const int32_t *x, const int32_t *z,
+                                const float *angle, int32_t *out, uint64_t *probes);
+
+/* ---- part 4: batched planner -------------------------------------------- */
+
+/* One planning request: FastRRT(ego) + set_plan_data + search_init + loop
+ * until goal, as a batch slot.  No counterpart in the reference (it plans one
+ * instance per CudaGraph). */
+typedef struct {
+    int width, height;
+    const uint8_t *class_ids;  /* host, width*height */
+    const float *class_costs;
+    int n_classes;
+    float perception_w_m, perception_h_m;
+    float max_steering_deg;
+    float vehicle_length_m;
+    float max_curvature;       /* < 0: derived (graph.cu:297-303) */
+    int lb_x, lb_z, ub_x, ub_z;
+    int start_x, start_z;
+    float start_heading;
+    int goal_x, goal_z;
+    float goal_heading;
+    float velocity_m_s;
+    int min_dist_x, min_dist_z;
+    float max_path_size;
+    float dist_to_goal_tol;
+    float heading_tol_rad;
+    uint64_t seed;
+    int smart;
+    int max_iterations;        /* 0 = unlimited */
+} fastrrt_request;
+
+void *fastrrt_batch_create(int n_slots, int max_width, int max_height);
+void fastrrt_batch_destroy(void *batch);
+/* loads a request into a slot (frame upload, masks, goal precompute, start) */
+int fastrrt_batch_admit(void *batch, int slot, const fastrrt_request *req, int timeout_ms);
+/* loads n requests into slots 0..n-1 in one pass */
+int fastrrt_batch_admit_many(void *batch, int n, const fastrrt_request *reqs, int timeout_ms);
+/* runs iterations until every admitted slot is done or `max_launches` graph
+ * launches ran; returns the number of launches */
+int fastrrt_batch_run(void *batch, int max_launches, int check_every);
+/* one graph launch (no host synchronisation) */
+int fastrrt_batch_step(void *batch);
+/* done flags, goal flags and loop counts of all slots (host arrays of n_slots) */
+int fastrrt_batch_status(void *batch, int32_t *done, int32_t *goal, int32_t *loops);
+/* extracts and validates the paths of the n listed slots; valid[k] = path
+ * passed the validator, length[k] = coarse path length in cells */
+int fastrrt_batch_collect(void *batch, int n, const int32_t *slots, int32_t *valid,
+                          float *length, int32_t *path_n);
+/* copies the last collected path of list entry k: up to cap (x, z, heading) */
+int fastrrt_batch_path(void *batch, int k, float *xyh, int cap);
+/* frees a slot */
+int fastrrt_batch_release(void *batch, int slot);
+/* device time of the last fastrrt_batch_run, milliseconds */
+float fastrrt_batch_last_ms(void *batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
