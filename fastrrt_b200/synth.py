@@ -71,8 +71,15 @@ def make_frame(seed, size=256, n_rect=12, n_disk=6, coverage=None, start=None, g
         for _ in range(n_disk):
             add_disk()
     else:
+        # coverage counts only obstacles outside the start / goal neighbourhoods,
+        # which are cleared afterwards
+        keep = np.ones((H, W), bool)
+        for p in (start, goal):
+            if p is not None:
+                keep[max(0, p[1] - keep_clear[1]):p[1] + keep_clear[1] + 1,
+                     max(0, p[0] - keep_clear[0]):p[0] + keep_clear[0] + 1] = False
         k = 0
-        while (cls == CLASS_OBSTACLE).mean() < coverage and k < 10000:
+        while ((cls == CLASS_OBSTACLE) & keep).mean() < coverage and k < 10000:
             add_rect() if k % 3 != 2 else add_disk()
             k += 1
     if start is not None:

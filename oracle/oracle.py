@@ -540,3 +540,78 @@ class RefCase:
         if rc != 0:
             raise RuntimeError("reference direct-connection entry point failed")
         return out
+
+
+class RefPlanner:
+    """The reference's own FastRRT (src/fastrrt.cpp) through its C ABI
+    (src/python_bind.cpp) in oracle/_ref, on the GPU.  Its RNG is seeded from
+    the wall clock (random_number_gen.cu:40), so runs are not repeatable."""
+
+    def __init__(self, cls, class_costs, pw_m, ph_m, max_steer_deg, vehicle_len,
+                 lb=(-1, -1), ub=(-1, -1), max_curvature=-1.0):
+        L = ref_lib()
+        self.L = L
+        for name, res, args in [
+            ("fastrrt_initialize", C.c_void_p, [C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                                C.c_float, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.c_void_p, C.c_float]),
+            ("fastrrt_destroy", None, [C.c_void_p]),
+            ("set_plan_data", None, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int,
+                                     C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
+                                     C.c_float, C.c_float, C.c_float]),
+            ("goal_reached", C.c_bool, [C.c_void_p]),
+            ("search_init", None, [C.c_void_p, C.c_bool]),
+            ("loop", C.c_bool, [C.c_void_p, C.c_bool]),
+            ("path_optimize", C.c_bool, [C.c_void_p]),
+            ("get_planned_path", C.POINTER(C.c_float), [C.c_void_p]),
+            ("release_planned_path_data", None, [C.POINTER(C.c_float)])]:
+            getattr(L, name).restype = res
+            getattr(L, name).argtypes = args
+        cls = np.ascontiguousarray(cls, np.uint8)
+        self.H, self.W = cls.shape
+        xyz = np.zeros((self.H, self.W, 3), np.float32)
+        xyz[..., 0] = cls
+        self.costs = np.ascontiguousarray(class_costs, np.float32)
+        self._xyz = np.ascontiguousarray(xyz.reshape(-1))
+        self.lb, self.ub = lb, ub
+        head = np.ascontiguousarray(np.concatenate(([len(self.costs)], self.costs)), np.float32)
+        self.p = L.fastrrt_initialize(self.W, self.H, pw_m, ph_m, max_steer_deg, vehicle_len,
+                                      lb[0], lb[1], ub[0], ub[1], head.ctypes.data, max_curvature)
+        self.frame = None
+
+    def set_plan_data(self, start, goal, velocity, min_dist, timeout_ms=-1, max_path=40.0,
+                      dist_tol=20.0, heading_tol=None):
+        if heading_tol is None:
+            heading_tol = float(np.float32(np.radians(10.0)))
+        mdx, mdz = int(float(np.float32(min_dist[0]) / 2)), int(float(np.float32(min_dist[1]) / 2))
+        if self.frame is not None:
+            self.L.ref_frame_free(self.frame)
+        self.frame = self.L.ref_frame_new(self.W, self.H, self._xyz, self.costs, len(self.costs),
+                                          self.lb[0], self.lb[1], self.ub[0], self.ub[1], mdx, mdz)
+        self.L.set_plan_data(self.p, self.frame, start[0], start[1], start[2], goal[0], goal[1],
+                             goal[2], velocity, min_dist[0], min_dist[1], timeout_ms, max_path,
+                             dist_tol, heading_tol)
+
+    def plan(self, smart=False, max_iter=1000):
+        self.L.search_init(self.p, False)
+        it = 0
+        while not self.L.goal_reached(self.p) and it < max_iter:
+            it += 1
+            if not self.L.loop(self.p, smart):
+                break
+        return bool(self.L.goal_reached(self.p)), it
+
+    def path(self):
+        ptr = self.L.get_planned_path(self.p)
+        n = int(ptr[0])
+        arr = np.array([ptr[1 + i] for i in range(3 * n)], np.float32).reshape(n, 3)
+        self.L.release_planned_path_data(ptr)
+        return arr
+
+    def __del__(self):
+        try:
+            if self.frame is not None:
+                self.L.ref_frame_free(self.frame)
+            self.L.fastrrt_destroy(self.p)
+        except Exception:
+            pass

@@ -1,0 +1,62 @@
+"""The oracle (host arithmetic) against golden vectors produced by the
+reference's own host-compiled functions (tests/golden/make_golden.py)."""
+import os
+
+import numpy as np
+
+from fastrrt_b200 import synth
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def test_kinematic_golden(orc):
+    d = load("kinematic_c0.npz")
+    fr = orc.Frame(d["cls"], synth.CLASS_COSTS)
+    g = orc.Graph(256, 256, 34.56, 34.56, 40.0, 5.4, -1.0, (22, 40))
+    g.g.pp.lr = float(d["lr"])
+    g.g.pp.max_steer_rad = float(d["max_steer"])
+    g.heading[:] = d["heading"]
+    out, _, _ = g.kinematic_batch(fr, d["sx"], d["sz"], d["steer"], d["length"], float(d["velocity"]))
+    assert np.array_equal(out.view(np.uint32), d["out"].view(np.uint32))
+    assert 0.2 < (d["out"][:, 0] >= 0).mean() < 0.9
+
+
+def test_hermite_golden(orc):
+    d = load("hermite_c0.npz")
+    fr = orc.Frame(d["cls"], synth.CLASS_COSTS)
+    g = orc.Graph(256, 256, 34.56, 34.56, 40.0, 5.4, -1.0, (22, 40))
+    out, _ = g.direct_batch(fr, float(d["max_curvature"]), d["x"], d["z"], d["lh"], d["gx"], d["gz"],
+                            d["gh"])
+    assert np.array_equal(out.view(np.uint32), d["out"].view(np.uint32))
+    assert (d["out"] >= 0).any() and (d["out"] < 0).any()
+
+
+def test_feasible_golden(orc):
+    d = load("feasible_c0.npz")
+    fr = orc.Frame(d["cls"], synth.CLASS_COSTS)
+    sp = orc.search(256, 256, 22, 40)
+    out, _ = orc.feasible_batch(fr, sp, d["x"], d["z"], d["a"])
+    assert np.array_equal(out, d["out"])
+
+
+def test_graph_dump_fixtures_stay_dag_after_solve(orc):
+    # assertGraphRemainsDAGAfterCollision (test_graph_solve_collisions.cpp:144-176)
+    # on the reference's recorded graph states (unittests/src/test_data)
+    d = load("graph_dumps.npz")
+    for name in d.files:
+        g = orc.Graph(256, 256, 256.0, 256.0, 40.0, 5.412658773, -1.0, (0, 0))
+        for x, z, h, t, px, pz, _, c in d[name]:
+            x, z, t, px, pz = int(x), int(z), int(t), int(px), int(pz)
+            if t == 1:
+                g.add(x, z, h, px, pz, c)
+            elif t == 2:
+                g.add_temporary(x, z, h, px, pz, c)
+            elif t == 4:
+                g.add(x, z, h, px, pz, c)
+                g.set_collision(x, z, px, pz, h, c)
+        g.solve_collisions()
+        assert g.consistent(), name
