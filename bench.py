@@ -1,0 +1,395 @@
+"""Benchmark of the B200 FastRRT planner: validated plans/s and plan latency
+on batched 256x256 planning, beside the plain single-instance GPU loop.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl mine|reference]
+
+A step plans one batch of B fresh requests (seeded 256x256 frames: road
+corridor, 12 rectangles and 6 disks of obstacles, start (128,128,0), goal
+(128,0,0), 40 deg steering, 5.4 m vehicle, 22x40 px footprint, 2 m/s, loop
+cap 200): admission (frame masks + goal direct-connection precompute),
+loop() until every request reached its goal or its loop cap, path extraction
+and validation.  Only validated plans count.
+
+  value : validated plans/s with the frames already in HBM (device clock)
+  e2e   : the same through the C ABI with host frames (host -> device copies
+          of the frames and device -> host copies of the results inside)
+  cpu_baseline / --impl reference : the CPU restatement of the same planner
+          (oracle/, all host cores) on a bounded sample of the same workload
+
+Each step uses frames never planned before, and the per-step working set
+(B x 256 x 256 cells x ~80 B of node grid and scratch) exceeds L2.
+Under torchrun, every rank plans its own requests (weak scaling, no
+collective on the data path); the time is the maximum over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+M_PER_PX = 0.135
+SIZE = 256
+MAX_ITER = 200
+METRIC = "validated plans/s (batched 256x256 planning)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", type=int, default=16, help="plans of the plain single-instance loop")
+    return ap.parse_args()
+
+
+def dist_setup(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def workload(rank, step, B):
+    """seeded requests of one step: (frames, starts, goals, seeds)"""
+    from fastrrt_b200 import synth
+    frames, starts, goals, seeds = [], [], [], []
+    for k in range(B):
+        seed = (rank * 1000003 + step * B + k) & 0xFFFFFFFF
+        cls, st, gl = synth.c0_request(seed, SIZE)
+        frames.append(cls)
+        starts.append(st)
+        goals.append(gl)
+        seeds.append(seed)
+    return np.stack(frames), starts, goals, seeds
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True,
+                                         text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([c.strip() for c in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_baseline(B_sample=None, threads=None, timeout_ms=30000):
+    """the CPU restatement of the planner (oracle/, OpenMP over plans) on a
+    bounded sample of the workload; a plan that runs past timeout_ms fails"""
+    from fastrrt_b200 import synth
+    from oracle import oracle as O
+    cores = threads or os.cpu_count() or 1
+    n = B_sample or max(8, min(64, 2 * cores))
+    frames, sg, seeds = [], [], []
+    for k in range(n):
+        seed = 7_000_000 + k
+        cls, st, gl = synth.c0_request(seed, SIZE)
+        frames.append(cls)
+        sg.append([st[0], st[1], int(st[2] * 1e6), gl[0], gl[1], int(gl[2] * 1e6)])
+        seeds.append(seed)
+    t0 = time.time()
+    ok, iters, cost, ms = O.plan_batch(
+        np.stack(frames), synth.CLASS_COSTS, np.array(sg, np.int32), np.array(seeds, np.uint64),
+        pw_m=SIZE * M_PER_PX, ph_m=SIZE * M_PER_PX, max_steer_deg=40.0, vehicle_len=5.4,
+        min_dist=(22, 40), velocity=2.0, max_path=40.0, dist_tol=20.0,
+        heading_tol=float(np.float32(math.radians(10))), timeout_ms=timeout_ms, max_iter=MAX_ITER,
+        smart=False, threads=cores)
+    wall = time.time() - t0
+    return {"value": float(ok.sum()) / wall, "unit": "plans/s", "cores": cores, "kind": "port",
+            "sample": f"{n} seeded 256x256 plans (same generator and parameters, "
+                      f"{timeout_ms / 1e3:.0f} s cap per plan), {int(ok.sum())} validated, "
+                      f"{wall:.1f} s wall on {cores} threads",
+            "success_rate": float(ok.mean()), "median_plan_s": float(np.median(ms) / 1e3)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU planner (oracle port) on the host cores"""
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    per_step = max(cores, 8)
+    for _ in range(args.warmup):
+        cpu_baseline(cores, cores, timeout_ms=2000)
+    vals, walls = [], []
+    for _ in range(args.steps):
+        t0 = time.time()
+        r = cpu_baseline(per_step, cores)
+        walls.append(time.time() - t0)
+        vals.append(r["value"])
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "plans/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * float(np.mean(walls)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"plans of seeded {SIZE}x{SIZE} frames, {per_step} per step",
+                       "parallelism": f"{cores} host threads"},
+            "cpu_baseline": {"value": value, "unit": "plans/s", "cores": cores, "kind": "port",
+                             "sample": f"{per_step} plans per step"},
+            "e2e": {"value": value, "unit": "plans/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def plain_loop(n, rank):
+    """the drop-in single-instance API (FastRRT loop) on n fresh frames"""
+    import fastrrt_b200 as F
+    from fastrrt_b200 import synth
+    ok = 0
+    lat = []
+    frames = [synth.c0_request(9_000_000 + rank * 1000 + k, SIZE) for k in range(n)]
+    p = F.FastRRT(F.EgoParams.init(SIZE, SIZE).with_search_physical_size(SIZE * M_PER_PX, SIZE * M_PER_PX)
+                  .with_max_steering_angle(F.angle.new_deg(40.0)).with_vehicle_length(5.4)
+                  .with_segmentation_class_costs(synth.CLASS_COSTS).build(),
+                  min_dist_x=22, min_dist_z=40)
+    t0 = time.time()
+    for k, (cls, st, gl) in enumerate(frames):
+        t1 = time.time()
+        fr = F.SearchFrame(class_ids=cls, class_costs=synth.CLASS_COSTS)
+        p.set_seed(k)
+        p.set_plan_data(fr, st, gl, 2.0)
+        p.search_init()
+        it = 0
+        while not p.goal_reached() and it < MAX_ITER:
+            it += 1
+            if not p.loop(False):
+                break
+        path = p.get_planned_path_array()
+        lat.append((time.time() - t1) * 1e3)
+        ok += int(p.goal_reached() and len(path) >= 2)
+    wall = time.time() - t0
+    return {"plans_per_s": ok / wall, "plans": n, "ok": ok,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "note": "one FastRRT object, set_plan_data + search_init + loop() per plan through the "
+                    "reference API, host wall clock"}
+
+
+def run_mine(args, rank, world, local):
+    import torch
+
+    import fastrrt_b200 as F
+    from fastrrt_b200 import synth
+    F._lib.require_cuda()
+    torch.cuda.set_device(local)
+    B = args.batch
+    total_steps = args.warmup + args.steps
+    t_gen = time.time()
+    work = [workload(rank, s, B) for s in range(total_steps)]
+    gen_s = time.time() - t_gen
+    planner = F.BatchPlanner(B, SIZE, SIZE)
+    costs = synth.CLASS_COSTS
+
+    def requests(step, device_frames=None):
+        frames, starts, goals, seeds = work[step]
+        reqs = []
+        for k in range(B):
+            r = F.make_request(frames[k], costs, starts[k], goals[k], seed=seeds[k],
+                               max_iterations=MAX_ITER, m_per_px=M_PER_PX)
+            if device_frames is not None:
+                r = F.batch.device_request(r, device_frames[k].data_ptr())
+            reqs.append(r)
+        return reqs
+
+    # frames resident in HBM for `value`
+    dev = [torch.from_numpy(work[s][0]).cuda() for s in range(total_steps)]
+    torch.cuda.synchronize()
+    for s in range(args.warmup):
+        planner.plan(requests(s, dev[s]), max_launches=MAX_ITER + 8)
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    dev_ms = 0.0
+    valid_total = 0
+    lat = []
+    lengths = []
+    for s in range(args.warmup, total_steps):
+        reqs = requests(s, dev[s])
+        v, length, latency, ms = planner.plan(reqs, max_launches=MAX_ITER + 8)
+        dev_ms += ms
+        valid_total += int(v.sum())
+        lat.extend(latency[v > 0].tolist())
+        lengths.extend(length[v > 0].tolist())
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    t_max = max_over_ranks(dev_ms, world)
+    plans = sum_over_ranks(valid_total, world)
+    value = plans / (t_max / 1e3)
+
+    # e2e: host frames through the C ABI (H2D of frames, D2H of results inside)
+    e2e_ms = 0.0
+    e2e_valid = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    for s in range(args.warmup, total_steps):
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        reqs = requests(s)
+        v, _, _, ms = planner.plan(reqs, max_launches=MAX_ITER + 8)
+        t1.record()
+        torch.cuda.synchronize()
+        e2e_ms += max(ms, t0.elapsed_time(t1))
+        e2e_valid += int(v.sum())
+    barrier(world)
+    e2e_t = max_over_ranks(e2e_ms, world)
+    e2e_plans = sum_over_ranks(e2e_valid, world)
+    h2d = B * (SIZE * SIZE + 4 * len(costs))
+    d2h = B * (4 * 3 + 3 * 4 * 1024 + 4 * 3)
+
+    # kernel timing replay of one step (same inputs, kernels launched one by one)
+    planner.profile(True)
+    planner.plan(requests(args.warmup, dev[args.warmup]), max_launches=MAX_ITER + 8)
+    ktimes = planner.kernel_times()
+    probes = planner.probes()
+    planner.profile(False)
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
+    name, (kms, kn) = dom
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    alg_bytes = probes.get(name.split("(")[0], 0)  # 1 byte per reference footprint probe
+    per_launch_ms = kms / max(kn, 1)
+    achieved = (alg_bytes / max(kn, 1)) / (per_launch_ms * 1e-3) / 1e9 if alg_bytes else 0.0
+    total_k = sum(v[0] for v in ktimes.values())
+
+    line = None
+    if rank == 0:
+        plain = plain_loop(args.plain, rank)
+        cpu = None if args.no_cpu_baseline else cpu_baseline()
+        line = {
+            "metric": METRIC, "value": value, "unit": "plans/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched planning, {B} requests of seeded {SIZE}x{SIZE} frames "
+                                   f"per step and GPU (loop cap {MAX_ITER})",
+                       "batch_per_gpu": B, "frame": f"{SIZE}x{SIZE} @ {M_PER_PX} m/px",
+                       "parallelism": f"request sharding x{world}",
+                       "l2": "fresh frames every step; per-step working set > L2"},
+            "p50_ms": float(np.percentile(lat, 50)) if lat else None,
+            "p99_ms": float(np.percentile(lat, 99)) if lat else None,
+            "success_rate": valid_total / float(B * args.steps),
+            "mean_path_len_px": float(np.mean(lengths)) if lengths else None,
+            "plain_gpu_loop": plain,
+            "batched_over_plain": value / plain["plans_per_s"] if plain["plans_per_s"] else None,
+            "e2e": {"value": e2e_plans / (e2e_t / 1e3), "unit": "plans/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(sum(v[1] for v in ktimes.values()) * args.steps),
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm if hbm else None,
+                         "traffic": None,
+                         "algorithmic": "1 byte (frame class) per footprint probe of the reference "
+                                        "algorithm executed by this kernel's work",
+                         "avg_launch_ms": per_launch_ms, "launches": kn,
+                         "share_of_device_time": kms / total_k if total_k else None},
+            "kernel_ms": {k: round(v[0], 3) for k, v in ktimes.items()},
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "workload_generation_s": gen_s,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    run_mine(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

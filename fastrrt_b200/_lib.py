@@ -32,7 +32,7 @@ class Request(C.Structure):
                 ("velocity_m_s", C.c_float), ("min_dist_x", C.c_int), ("min_dist_z", C.c_int),
                 ("max_path_size", C.c_float), ("dist_to_goal_tol", C.c_float),
                 ("heading_tol_rad", C.c_float), ("seed", C.c_uint64), ("smart", C.c_int),
-                ("max_iterations", C.c_int)]
+                ("max_iterations", C.c_int), ("class_ids_on_device", C.c_int)]
 
 
 EXPORTS = [
@@ -53,7 +53,9 @@ EXPORTS = [
     "fastrrt_batch_create", "fastrrt_batch_destroy", "fastrrt_batch_admit",
     "fastrrt_batch_admit_many", "fastrrt_batch_run", "fastrrt_batch_step", "fastrrt_batch_status",
     "fastrrt_batch_collect", "fastrrt_batch_path", "fastrrt_batch_release",
-    "fastrrt_batch_last_ms",
+    "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
+    "fastrrt_batch_kernel_times", "fastrrt_kernel_count", "fastrrt_kernel_name",
+    "fastrrt_batch_probes",
 ]
 
 
@@ -125,6 +127,14 @@ def lib():
         "fastrrt_batch_path": (C.c_int, [vp, C.c_int, f32p, C.c_int]),
         "fastrrt_batch_release": (C.c_int, [vp, C.c_int]),
         "fastrrt_batch_last_ms": (C.c_float, [vp]),
+        "fastrrt_batch_plan": (C.c_int, [vp, C.c_int, P(Request), C.c_int, C.c_int, i32p, f32p,
+                                         f32p, P(C.c_float)]),
+        "fastrrt_batch_profile": (C.c_int, [vp, C.c_int]),
+        "fastrrt_batch_kernel_times": (C.c_int, [vp, np.ctypeslib.ndpointer(np.float64, flags="C"),
+                                                 np.ctypeslib.ndpointer(np.int64, flags="C")]),
+        "fastrrt_kernel_count": (C.c_int, []),
+        "fastrrt_kernel_name": (C.c_char_p, [C.c_int]),
+        "fastrrt_batch_probes": (C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
     }
     for name in EXPORTS:
         fn = getattr(L, name)

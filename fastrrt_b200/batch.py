@@ -41,8 +41,20 @@ def make_request(cls, class_costs, start, goal, *, perception_m=None, m_per_px=0
     r.seed = int(seed)
     r.smart = int(bool(smart))
     r.max_iterations = int(max_iterations)
+    r.class_ids_on_device = 0
     r._keep = (cls, costs)
     return r
+
+
+def device_request(r, device_ptr):
+    """A copy of request `r` whose class ids are read from device memory
+    (e.g. a torch.uint8 tensor's data_ptr())."""
+    d = _lib.Request()
+    _lib.C.pointer(d)[0] = r
+    d.class_ids = _lib.C.cast(_lib.C.c_void_p(device_ptr), _lib.C.POINTER(_lib.C.c_uint8))
+    d.class_ids_on_device = 1
+    d._keep = getattr(r, "_keep", None)
+    return d
 
 
 class BatchPlanner:
@@ -99,6 +111,36 @@ class BatchPlanner:
         buf = np.zeros(3 * cap, np.float32)
         m = _lib.check(_lib.lib().fastrrt_batch_path(self._h, k, buf, cap), "batch_path")
         return buf[:3 * m].reshape(m, 3).copy()
+
+    def plan(self, requests, max_launches=1000, check_every=4):
+        """admit + loop until done + validate; returns (valid, length,
+        latency_ms, device_ms)"""
+        n = len(requests)
+        arr = (_lib.Request * n)(*requests)
+        valid = np.zeros(n, np.int32)
+        length = np.zeros(n, np.float32)
+        lat = np.zeros(n, np.float32)
+        dev = _lib.C.c_float(0)
+        _lib.check(_lib.lib().fastrrt_batch_plan(self._h, n, arr, max_launches, check_every, valid,
+                                                 length, lat, _lib.C.byref(dev)), "batch_plan")
+        return valid, length, lat, dev.value
+
+    def profile(self, on=True):
+        _lib.check(_lib.lib().fastrrt_batch_profile(self._h, int(on)), "batch_profile")
+
+    def kernel_times(self):
+        L = _lib.lib()
+        k = L.fastrrt_kernel_count()
+        ms = np.zeros(k, np.float64)
+        n = np.zeros(k, np.int64)
+        _lib.check(L.fastrrt_batch_kernel_times(self._h, ms, n), "kernel_times")
+        return {L.fastrrt_kernel_name(i).decode(): (float(ms[i]), int(n[i])) for i in range(k)}
+
+    def probes(self):
+        a, g, p = _lib.C.c_uint64(), _lib.C.c_uint64(), _lib.C.c_uint64()
+        _lib.check(_lib.lib().fastrrt_batch_probes(self._h, _lib.C.byref(a), _lib.C.byref(g),
+                                                   _lib.C.byref(p)), "batch_probes")
+        return {"k_expand": a.value, "k_goal": g.value, "k_direct_goal": p.value}
 
     def release(self, slot):
         _lib.check(_lib.lib().fastrrt_batch_release(self._h, slot), "batch_release")

@@ -140,7 +140,8 @@ bool load_request(Engine &e, int slot, const fastrrt_request &r)
     q.max_iter = r.max_iterations;
     q.stop_on_goal = 1;
     e.set_request(slot, q);
-    return e.copy_frame(slot, r.width, r.height, r.class_ids, r.class_costs, r.n_classes);
+    return e.copy_frame(slot, r.width, r.height, r.class_ids, r.class_costs, r.n_classes,
+                        r.class_ids_on_device != 0);
 }
 }  // namespace
 
@@ -512,7 +513,8 @@ int fastrrt_probe_count(void *ptr, uint64_t *probes)
         return -1;
     if (!p->eng->fetch_states(true))
         return -1;
-    *probes = p->eng->state(0).probes;
+    const State &S = p->eng->state(0);
+    *probes = S.probes + S.probes_goal + S.probes_pre;
     return 0;
 }
 
@@ -926,6 +928,145 @@ int fastrrt_batch_path(void *batch, int k, float *xyh, int cap)
     for (int i = 0; i < 3 * m; i++)
         xyh[i] = b->eng->paths()[(size_t)k * stride + i];
     return m;
+}
+
+int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_launches,
+                       int check_every, int32_t *valid, float *length, float *latency_ms,
+                       float *device_ms)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || !reqs || n <= 0 || n > b->eng->n_slots()) {
+        set_error("batch plan: bad arguments");
+        return -1;
+    }
+    Engine &e = *b->eng;
+    cudaEvent_t e0 = b->ev0, e_adm = nullptr;
+    if (cudaEventCreate(&e_adm) != cudaSuccess) {
+        set_error("batch plan: event");
+        return -1;
+    }
+    cudaEventRecord(e0, e.stream());
+    std::vector<int> slots;
+    for (int k = 0; k < n; k++) {
+        if (!load_request(e, k, reqs[k])) {
+            cudaEventDestroy(e_adm);
+            return -1;
+        }
+        slots.push_back(k);
+    }
+    for (int s = n; s < e.n_slots(); s++)
+        if (e.state(s).active)
+            e.deactivate(s);
+    const bool adm = e.prepare(slots, 0.8f) && e.search_init(slots, true);
+    cudaEventRecord(e_adm, e.stream());
+    if (!adm) {
+        cudaEventDestroy(e_adm);
+        return -1;
+    }
+    int launches = 0;
+    if (check_every <= 0)
+        check_every = 1;
+    bool ok = true;
+    while (ok && launches < max_launches) {
+        for (int k = 0; k < check_every && launches < max_launches && ok; k++, launches++)
+            ok = e.iterate();
+        ok = ok && e.fetch_states(true);
+        if (!ok)
+            break;
+        bool all_done = true;
+        for (int s = 0; s < n; s++)
+            if (e.state(s).active && !e.state(s).done) {
+                all_done = false;
+                break;
+            }
+        if (all_done)
+            break;
+    }
+    ok = ok && e.extract_and_validate(slots, 1024);
+    cudaEventRecord(b->ev1, e.stream());
+    cudaEventSynchronize(b->ev1);
+    float adm_ms = 0, total_ms = 0;
+    cudaEventElapsedTime(&adm_ms, e0, e_adm);
+    cudaEventElapsedTime(&total_ms, e0, b->ev1);
+    cudaEventDestroy(e_adm);
+    if (!ok)
+        return -1;
+    b->last_ms = total_ms;
+    if (device_ms)
+        *device_ms = total_ms;
+    int good = 0;
+    for (int k = 0; k < n; k++) {
+        const State &S = e.state(k);
+        const int v = e.valid()[k] && S.goal_reached;
+        good += v;
+        if (valid)
+            valid[k] = v;
+        if (length)
+            length[k] = e.lengths()[k];
+        if (latency_ms) {
+            const long long fin = S.finish_ns ? S.finish_ns : S.start_ns;
+            latency_ms[k] = adm_ms + (float)((fin - S.start_ns) * 1e-6);
+        }
+    }
+    return good;
+}
+
+int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || !b->eng->fetch_states(true))
+        return -1;
+    uint64_t a = 0, g = 0, p = 0;
+    for (int s = 0; s < b->eng->n_slots(); s++) {
+        a += b->eng->state(s).probes;
+        g += b->eng->state(s).probes_goal;
+        p += b->eng->state(s).probes_pre;
+    }
+    if (expand)
+        *expand = a;
+    if (goal)
+        *goal = g;
+    if (precompute)
+        *precompute = p;
+    return 0;
+}
+
+int fastrrt_batch_profile(void *batch, int on)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b)
+        return -1;
+    return b->eng->set_profiling(on != 0) ? 0 : -1;
+}
+
+int fastrrt_kernel_count(void) { return kIterKernels + 1; }
+
+const char *fastrrt_kernel_name(int k)
+{
+    if (k >= 0 && k < kIterKernels)
+        return kIterKernelNames[k];
+    if (k == kIterKernels)
+        return "k_direct_goal";
+    return "";
+}
+
+int fastrrt_batch_kernel_times(void *batch, double *ms, int64_t *launches)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || !ms || !launches)
+        return -1;
+    Engine &e = *b->eng;
+    if (e.kernel_ms().size() < (size_t)kIterKernels) {
+        set_error("kernel times: profiling is off");
+        return -1;
+    }
+    for (int k = 0; k < kIterKernels; k++) {
+        ms[k] = e.kernel_ms()[k];
+        launches[k] = e.kernel_launches()[k];
+    }
+    ms[kIterKernels] = e.precompute_ms();
+    launches[kIterKernels] = e.precompute_launches();
+    return 0;
 }
 
 int fastrrt_batch_release(void *batch, int slot)

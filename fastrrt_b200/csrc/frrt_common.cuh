@@ -72,6 +72,9 @@ struct Inst {
     float *node_best_seg;      // per listed node: node -> cell segment cost
     unsigned *region_count;    // [kMaxRegions] density used by the gate
     unsigned *region_new;      // [kMaxRegions] density counted after this expansion
+    uint32_t *rowdil;          // mask scratch of the clear-mask dilation
+    const float *class_costs;  // class-cost table of the frame
+    int n_classes;
     // parameters
     float og_x, og_z;          // coordinate origin (frame centre)
     int mdx, mdz;              // half footprint
@@ -111,7 +114,11 @@ struct State {
     int loops;                 // loop() calls run
     int error;                 // bounded-wait / consistency error code
     long long deadline_ns;     // device-clock deadline (0 = none)
-    unsigned long long probes; // footprint probes of the reference algorithm
+    long long start_ns;        // device clock at search_init
+    long long finish_ns;       // device clock when the slot finished
+    unsigned long long probes;        // footprint probes of the reference algorithm: expansion
+    unsigned long long probes_goal;   // ... goal-connection search
+    unsigned long long probes_pre;    // ... goal direct-connection precompute
 };
 
 }  // namespace frrt

@@ -145,6 +145,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         4 * (size_t)mask_words_,            // 21 clear
         4 * (size_t)kMaxRegions,            // 22 region_count
         4 * (size_t)kMaxRegions,            // 23 region_new
+        4 * (size_t)mask_words_,            // 24 clear-mask scratch
     };
     constexpr int kParts = sizeof(parts) / sizeof(parts[0]);
     size_t per_slot = 0;
@@ -195,6 +196,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         I.clear = (const uint32_t *)ptr[21];
         I.region_count = (unsigned *)ptr[22];
         I.region_new = (unsigned *)ptr[23];
+        I.rowdil = (uint32_t *)ptr[24];
         I.lbx = I.lbz = I.ubx = I.ubz = -1;
         I.stop_on_goal = 1;
         if (!check(cudaMemsetAsync(I.claim, 0x7F, 4 * C, stream_), "claim init"))
@@ -209,7 +211,6 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMalloc(&d_grab_, sizeof(unsigned) * 4), "grab counters") &&
               check(cudaMalloc(&d_slots_, sizeof(int) * n_slots), "slot list") &&
               check(cudaMalloc(&d_class_costs_, sizeof(float) * kMaxClasses * n_slots), "class costs") &&
-              check(cudaMalloc(&d_rowdil_, sizeof(uint32_t) * mask_words_), "mask scratch") &&
               check(cudaMalloc(&d_bad_, sizeof(int)), "flag") &&
               check(cudaMallocHost(&h_small_, sizeof(int) * 64), "pinned scratch") &&
               check(cudaMalloc(&d_newcost_, sizeof(float) * kOptCap * kOptCap), "optimize scratch") &&
@@ -220,6 +221,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
     if (!ok)
         return;
     memset(h_state_, 0, sizeof(State) * n_slots);
+    for (int s = 0; s < n_slots; s++)
+        h_inst_[s].class_costs = d_class_costs_ + (size_t)s * kMaxClasses;
     // stage both bit-packed masks of a slot in shared memory when they fit
     const int smem_bytes = 2 * 4 * mask_words_;
     L_.sms = sms;
@@ -253,7 +256,6 @@ Engine::~Engine()
     cudaFree(d_grab_);
     cudaFree(d_slots_);
     cudaFree(d_class_costs_);
-    cudaFree(d_rowdil_);
     cudaFree(d_bad_);
     if (h_small_)
         cudaFreeHost(h_small_);
@@ -309,6 +311,7 @@ bool Engine::bind_frame(int slot, const Frame *f)
     I.cls = f->d_cls;  // read in place
     I.trav = f->d_trav;
     ncls_[slot] = f->n_classes;
+    I.n_classes = f->n_classes;
     dirty_ = true;
     return check(cudaMemcpyAsync(d_class_costs_ + (size_t)slot * kMaxClasses, f->d_costs,
                                  sizeof(float) * kMaxClasses, cudaMemcpyDeviceToDevice, stream_),
@@ -327,6 +330,7 @@ bool Engine::copy_frame(int slot, int W, int H, const uint8_t *cls, const float 
     I.cls = own_cls_[slot];
     I.trav = nullptr;
     ncls_[slot] = n_classes;
+    I.n_classes = n_classes;
     dirty_ = true;
     return check(cudaMemcpyAsync(own_cls_[slot], cls, (size_t)W * H,
                                  cls_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
@@ -443,22 +447,34 @@ bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
         return true;
     if (!check(cudaMemsetAsync(d_bad_, 0, sizeof(int), stream_), "flag reset"))
         return false;
-    int max_cells = 0;
+    int max_cells = 0, max_words = 0;
     for (int s : slots) {
         const Inst &I = h_inst_[s];
         if (I.W <= 0) {
             set_error("slot has no frame");
             return false;
         }
-        launch_frame_masks(I, d_class_costs_ + (size_t)s * kMaxClasses, ncls_[s],
-                           const_cast<uint32_t *>(I.blocked), const_cast<uint32_t *>(I.clear),
-                           d_rowdil_, d_bad_, stream_);
         max_cells = std::max(max_cells, I.W * I.H);
+        max_words = std::max(max_words, I.mask_rw * I.H);
     }
     if (!upload_slots_list(slots))
         return false;
+    launch_frame_masks(d_inst_, d_state_, d_slots_, (int)slots.size(), max_words, kMaxClasses, d_bad_,
+                       stream_);
+    if (profiling_)
+        cudaEventRecord(prof_ev_[kIterKernels + 1], stream_);
     launch_direct_goal(d_inst_, d_state_, d_slots_, (int)slots.size(), max_cells,
                        direct_max_curvature, L_, stream_);
+    if (profiling_) {
+        cudaEventRecord(prof_ev_[kIterKernels + 2], stream_);
+        float ms = 0;
+        if (check(cudaEventSynchronize(prof_ev_[kIterKernels + 2]), "profiling sync") &&
+            check(cudaEventElapsedTime(&ms, prof_ev_[kIterKernels + 1], prof_ev_[kIterKernels + 2]),
+                  "profiling time")) {
+            prof_pre_ms_ += ms;
+            prof_pre_n_ += 1;
+        }
+    }
     if (!check(cudaGetLastError(), "precompute launch") ||
         !check(cudaMemcpyAsync(h_small_, d_bad_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "flag") ||
         !check(cudaStreamSynchronize(stream_), "precompute"))
@@ -500,10 +516,38 @@ bool Engine::ensure_graph()
     return check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
 }
 
+bool Engine::set_profiling(bool on)
+{
+    profiling_ = on;
+    if (on && prof_ev_.empty()) {
+        prof_ev_.resize(kIterKernels + 3);
+        for (auto &e : prof_ev_)
+            if (!check(cudaEventCreate(&e), "profiling events"))
+                return false;
+    }
+    prof_ms_.assign(kIterKernels, 0.0);
+    prof_n_.assign(kIterKernels, 0);
+    prof_pre_ms_ = 0;
+    prof_pre_n_ = 0;
+    return true;
+}
+
 bool Engine::iterate()
 {
     if (dirty_ && !commit())
         return false;
+    if (profiling_) {
+        launch_iteration(d_inst_, d_state_, d_sched_, n_slots_, L_, stream_, prof_ev_.data());
+        if (!check(cudaGetLastError(), "iteration launch") || !sync())
+            return false;
+        for (int k = 0; k < kIterKernels; k++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, prof_ev_[k], prof_ev_[k + 1]);
+            prof_ms_[k] += ms;
+            prof_n_[k] += 1;
+        }
+        return true;
+    }
     if (!ensure_graph())
         return false;
     return check(cudaGraphLaunch(graph_exec_, stream_), "graph launch");

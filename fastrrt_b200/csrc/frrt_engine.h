@@ -92,6 +92,14 @@ public:
     bool search_init(const std::vector<int> &slots, bool reset_regions);
     // one loop() over every live slot (graph launch); no host sync
     bool iterate();
+    // kernel timing mode: iterate() launches the kernels one by one between
+    // CUDA events and accumulates each kernel's device time
+    bool set_profiling(bool on);
+    const std::vector<double> &kernel_ms() const { return prof_ms_; }
+    const std::vector<long> &kernel_launches() const { return prof_n_; }
+    // device time spent in the direct-goal precompute by prepare() (profiling mode)
+    double precompute_ms() const { return prof_pre_ms_; }
+    long precompute_launches() const { return prof_pre_n_; }
     bool sync();
     // copy the small head of the state of every slot to host memory
     bool fetch_states(bool synchronous = true);
@@ -160,7 +168,6 @@ private:
     unsigned *d_grab_ = nullptr;
     int *d_slots_ = nullptr;
     float *d_class_costs_ = nullptr;  // per slot, 256 entries
-    uint32_t *d_rowdil_ = nullptr;
     int *d_bad_ = nullptr;
     std::vector<uint8_t *> own_cls_;  // per slot frame copies
     std::vector<float *> intrinsic_;  // per slot intrinsic-cost arrays
@@ -178,6 +185,12 @@ private:
     int *h_small_ = nullptr;          // pinned scratch
     std::vector<int> h_path_n_, h_valid_;
     std::vector<float> h_length_, h_paths_;
+    bool profiling_ = false;
+    std::vector<cudaEvent_t> prof_ev_;
+    std::vector<double> prof_ms_;
+    std::vector<long> prof_n_;
+    double prof_pre_ms_ = 0;
+    long prof_pre_n_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     bool dirty_ = true;

@@ -124,29 +124,32 @@ __device__ __forceinline__ long long global_ns()
 // frame preparation
 // ---------------------------------------------------------------------------
 
-// one thread per mask word: bit set when class cost < 0
-__global__ void k_blocked(const uint8_t *cls, int W, int H, int rw, const float *costs, int ncls,
-                          uint32_t *blocked, int *bad_class)
+// one thread per mask word of every listed slot: bit set when class cost < 0
+__global__ void k_blocked(const Inst *insts, State *states, const int *slots, int *bad_class)
 {
-    const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (w >= (long)rw * H)
-        return;
-    const int z = (int)(w / rw);
-    const int x0 = (int)(w - (long)z * rw) * 32;
-    uint32_t bits = 0;
-    for (int b = 0; b < 32; b++) {
-        const int x = x0 + b;
-        if (x >= W)
-            break;
-        const int c = cls[(long)z * W + x];
-        if (c >= ncls) {
-            atomicExch(bad_class, 1);
-            continue;
+    const Inst &I = insts[slots[blockIdx.y]];
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        states[slots[blockIdx.y]].probes_pre = 0;
+    const long words = (long)I.mask_rw * I.H;
+    for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < words;
+         w += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(w / I.mask_rw);
+        const int x0 = (int)(w - (long)z * I.mask_rw) * 32;
+        uint32_t bits = 0;
+        for (int b = 0; b < 32; b++) {
+            const int x = x0 + b;
+            if (x >= I.W)
+                break;
+            const int c = I.cls[(long)z * I.W + x];
+            if (c >= I.n_classes) {
+                atomicExch(bad_class, 1);
+                continue;
+            }
+            if (I.class_costs[c] < 0)
+                bits |= 1u << b;
         }
-        if (costs[c] < 0)
-            bits |= 1u << b;
+        const_cast<uint32_t *>(I.blocked)[w] = bits;
     }
-    blocked[w] = bits;
 }
 
 // 32 row bits starting at bit `start` (may be negative / beyond the row)
@@ -160,49 +163,53 @@ __device__ __forceinline__ uint32_t row_bits(const uint32_t *row, int rw, int st
 }
 
 // horizontal dilation of the obstacle mask by rc
-__global__ void k_rowdil(const uint32_t *blocked, int W, int H, int rw, int rc, uint32_t *rowdil)
+__global__ void k_rowdil(const Inst *insts, const int *slots)
 {
-    const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (w >= (long)rw * H)
-        return;
-    const int z = (int)(w / rw);
-    const int q = (int)(w - (long)z * rw);
-    const uint32_t *row = blocked + (long)z * rw;
-    uint32_t acc = 0;
-    for (int d = -rc; d <= rc; d++)
-        acc |= row_bits(row, rw, q * 32 + d);
-    rowdil[w] = acc;
+    const Inst &I = insts[slots[blockIdx.y]];
+    const long words = (long)I.mask_rw * I.H;
+    for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < words;
+         w += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(w / I.mask_rw);
+        const int q = (int)(w - (long)z * I.mask_rw);
+        const uint32_t *row = I.blocked + (long)z * I.mask_rw;
+        uint32_t acc = 0;
+        for (int d = -I.rc; d <= I.rc; d++)
+            acc |= row_bits(row, I.mask_rw, q * 32 + d);
+        I.rowdil[w] = acc;
+    }
 }
 
 // vertical dilation + complement: clear = no obstacle within Chebyshev rc
-__global__ void k_clear(const uint32_t *rowdil, int W, int H, int rw, int rc, uint32_t *clear)
+__global__ void k_clear(const Inst *insts, const int *slots)
 {
-    const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (w >= (long)rw * H)
-        return;
-    const int z = (int)(w / rw);
-    const int q = (int)(w - (long)z * rw);
-    uint32_t acc = 0;
-    const int z0 = max(0, z - rc), z1 = min(H - 1, z + rc);
-    for (int zz = z0; zz <= z1; zz++)
-        acc |= rowdil[(long)zz * rw + q];
-    uint32_t valid = 0xffffffffu;
-    const int left = W - q * 32;
-    if (left < 32)
-        valid = left <= 0 ? 0u : ((1u << left) - 1u);
-    clear[w] = ~acc & valid;
+    const Inst &I = insts[slots[blockIdx.y]];
+    const long words = (long)I.mask_rw * I.H;
+    for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < words;
+         w += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(w / I.mask_rw);
+        const int q = (int)(w - (long)z * I.mask_rw);
+        uint32_t acc = 0;
+        const int z0 = max(0, z - I.rc), z1 = min(I.H - 1, z + I.rc);
+        for (int zz = z0; zz <= z1; zz++)
+            acc |= I.rowdil[(long)zz * I.mask_rw + q];
+        uint32_t valid = 0xffffffffu;
+        const int left = I.W - q * 32;
+        if (left < 32)
+            valid = left <= 0 ? 0u : ((1u << left) - 1u);
+        const_cast<uint32_t *>(I.clear)[w] = ~acc & valid;
+    }
 }
 
-void launch_frame_masks(const Inst &h, const float *d_class_costs, int n_classes,
-                        uint32_t *d_blocked, uint32_t *d_clear, uint32_t *d_rowdil,
-                        int *d_bad_class, cudaStream_t st)
+void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_words,
+                        int ncls_max, int *d_bad_class, cudaStream_t st)
 {
-    const long words = (long)h.mask_rw * h.H;
-    const int grid = (int)((words + 255) / 256);
-    k_blocked<<<grid, 256, 0, st>>>(h.cls, h.W, h.H, h.mask_rw, d_class_costs, n_classes, d_blocked,
-                                    d_bad_class);
-    k_rowdil<<<grid, 256, 0, st>>>(d_blocked, h.W, h.H, h.mask_rw, h.rc, d_rowdil);
-    k_clear<<<grid, 256, 0, st>>>(d_rowdil, h.W, h.H, h.mask_rw, h.rc, d_clear);
+    if (n <= 0)
+        return;
+    const dim3 grid((max_words + 255) / 256, n);
+    (void)ncls_max;
+    k_blocked<<<grid, 256, 0, st>>>(d_inst, d_state, d_slots, d_bad_class);
+    k_rowdil<<<grid, 256, 0, st>>>(d_inst, d_slots);
+    k_clear<<<grid, 256, 0, st>>>(d_inst, d_slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -271,7 +278,7 @@ __global__ void __launch_bounds__(256) k_direct_goal(const Inst *insts, State *s
     }
     probes = warp_sum64(probes);
     if ((threadIdx.x & 31) == 0 && probes)
-        atomicAdd(&states[slot].probes, probes);
+        atomicAdd(&states[slot].probes_pre, probes);
 }
 
 void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
@@ -326,6 +333,10 @@ __global__ void k_init_state(const Inst *insts, State *states, const int *slots,
     S.best = kBigCost;
     S.loops = 0;
     S.error = 0;
+    S.probes = 0;
+    S.probes_goal = 0;
+    S.start_ns = global_ns();
+    S.finish_ns = 0;
     if (reset_regions)
         for (int r = 0; r < kMaxRegions; r++)
             I.region_count[r] = 0;
@@ -926,7 +937,7 @@ __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, 
         }
         probes = warp_sum64(probes);
         if (lane == 0 && probes)
-            atomicAdd(&S.probes, probes);
+            atomicAdd(&S.probes_goal, probes);
     }
     stage_drain(sg, &bar);
 }
@@ -986,12 +997,15 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
     }
     S.loops++;
     S.iter++;
+    const long long now = global_ns();
     if (S.goal_reached && I.stop_on_goal)
         S.done = 1;
     else if (I.max_iter > 0 && S.loops >= I.max_iter)
         S.done = 1;
-    else if (S.deadline_ns > 0 && global_ns() > S.deadline_ns)
+    else if (S.deadline_ns > 0 && now > S.deadline_ns)
         S.done = 1;
+    if (S.done)
+        S.finish_ns = now;
     // per-iteration resets
     S.n_cand = 0;
     S.node_count = 0;
@@ -1010,22 +1024,45 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
     }
 }
 
+const char *const kIterKernelNames[kIterKernels] = {
+    "k_scan", "k_plan(cand)", "k_expand", "k_apply", "k_post", "k_erase",
+    "k_setnodes", "k_accept", "k_plan(nodes)", "k_goal", "k_select", "k_finish"};
+
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
-                      const Launch &L, cudaStream_t st)
+                      const Launch &L, cudaStream_t st, cudaEvent_t *ev)
 {
     const size_t smem = (size_t)L.smem_words * 2 * 4;
+    int k = 0;
+    auto mark = [&]() {
+        if (ev)
+            cudaEventRecord(ev[k], st);
+        k++;
+    };
+    mark();
     k_scan<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 0);
+    mark();
     k_expand<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    mark();
     k_apply<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_post<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_erase<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_setnodes<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_accept<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 1);
+    mark();
     k_goal<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    mark();
     k_select<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
     k_finish<<<(n_slots + 127) / 128, 128, 0, st>>>(d_inst, d_state, n_slots);
+    mark();
 }
 
 // ---------------------------------------------------------------------------

@@ -32,19 +32,22 @@ struct Launch {
 // allows `smem_bytes` of dynamic shared memory on the mask-staging kernels
 void configure_kernels(int smem_bytes);
 
-// frame preparation for one slot: obstacle and clear masks
-void launch_frame_masks(const Inst &h, const float *d_class_costs, int n_classes,
-                        uint32_t *d_blocked, uint32_t *d_clear, uint32_t *d_rowdil,
-                        int *d_bad_class, cudaStream_t st);
+// frame preparation for listed slots: obstacle and clear masks
+void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_words,
+                        int ncls_max, int *d_bad_class, cudaStream_t st);
 // goal direct-connection precompute for the n slots listed in d_slots
 void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
                         int max_cells, float max_curvature, const Launch &L, cudaStream_t st);
 // search_init for listed slots: reset node types, add the start, reset state
 void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, int n,
                         int max_cells, int reset_regions, cudaStream_t st);
-// one planning iteration (loop()) over all active slots
+// one planning iteration (loop()) over all active slots; with `ev` (an array
+// of kIterKernels + 1 events) an event is recorded before each kernel and
+// after the last one
+constexpr int kIterKernels = 12;
+extern const char *const kIterKernelNames[kIterKernels];
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
-                      const Launch &L, cudaStream_t st);
+                      const Launch &L, cudaStream_t st, cudaEvent_t *ev = nullptr);
 // standalone goal check (checkGoalReached) for listed slots
 void launch_goal_check(const Inst *d_inst, State *d_state, const int *d_slots, int n,
                        int max_cells, cudaStream_t st);

@@ -155,6 +155,7 @@ typedef struct {
     uint64_t seed;
     int smart;
     int max_iterations;        /* 0 = unlimited */
+    int class_ids_on_device;   /* class_ids points to device memory */
 } fastrrt_request;
 
 void *fastrrt_batch_create(int n_slots, int max_width, int max_height);
@@ -180,6 +181,25 @@ int fastrrt_batch_path(void *batch, int k, float *xyh, int cap);
 int fastrrt_batch_release(void *batch, int slot);
 /* device time of the last fastrrt_batch_run, milliseconds */
 float fastrrt_batch_last_ms(void *batch);
+/* one batched planning pass: admits reqs into slots 0..n-1, loops until all
+ * are done (at most max_launches graph launches), extracts and validates the
+ * paths.  valid / length / latency_ms are per request (latency = admission
+ * + the request's own loop time, device clock); *device_ms = the pass on the
+ * device clock.  Returns the number of validated plans. */
+int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_launches,
+                       int check_every, int32_t *valid, float *length, float *latency_ms,
+                       float *device_ms);
+/* kernel timing mode (1 = on): iterations launch kernels one by one between
+ * CUDA events instead of replaying the CUDA graph */
+int fastrrt_batch_profile(void *batch, int on);
+/* per-kernel device time (ms) and launch counts since profiling was turned
+ * on: fastrrt_kernel_count() entries, the last one the goal precompute */
+int fastrrt_batch_kernel_times(void *batch, double *ms, int64_t *launches);
+int fastrrt_kernel_count(void);
+/* footprint probes of the reference algorithm, summed over the slots of the
+ * last admission: expansion, goal-connection search, goal precompute */
+int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute);
+const char *fastrrt_kernel_name(int k);
 
 #ifdef __cplusplus
 }
