@@ -486,7 +486,7 @@ bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
     return true;
 }
 
-bool Engine::search_init(const std::vector<int> &slots, bool reset_regions)
+bool Engine::search_init(const std::vector<int> &slots, bool fresh)
 {
     if (dirty_ && !commit())
         return false;
@@ -497,7 +497,7 @@ bool Engine::search_init(const std::vector<int> &slots, bool reset_regions)
         max_cells = std::max(max_cells, h_inst_[s].W * h_inst_[s].H);
     if (!upload_slots_list(slots))
         return false;
-    launch_search_init(d_inst_, d_state_, d_slots_, (int)slots.size(), max_cells, reset_regions ? 1 : 0,
+    launch_search_init(d_inst_, d_state_, d_slots_, (int)slots.size(), max_cells, fresh ? 1 : 0,
                        stream_);
     return check(cudaGetLastError(), "search_init launch");
 }

@@ -89,7 +89,8 @@ public:
     // set_plan_data for listed slots: masks + goal direct-connection precompute
     bool prepare(const std::vector<int> &slots, float direct_max_curvature = 0.8f);
     // search_init for listed slots
-    bool search_init(const std::vector<int> &slots, bool reset_regions);
+    // fresh = a new request: the slot starts like a newly constructed planner
+    bool search_init(const std::vector<int> &slots, bool fresh);
     // one loop() over every live slot (graph launch); no host sync
     bool iterate();
     // kernel timing mode: iterate() launches the kernels one by one between

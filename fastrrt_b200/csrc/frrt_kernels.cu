@@ -297,13 +297,30 @@ void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, 
 // (graph.cu:400-427), then the start node is added
 // ---------------------------------------------------------------------------
 
-__global__ void k_clear_types(const Inst *insts, const int *slots)
+// CudaGraph::clear (graph.cu:400-427) sets only the node types to NULL, so a
+// planner that is reused keeps the derive counts, parents, headings and costs
+// of earlier plans in its NULL cells (the derive count steers frontier
+// expansion, graph_expansion.cu:160).  `fresh` zeroes those too, which is the
+// state of a newly constructed planner: a batch slot that takes a new request
+// then plans exactly like a new FastRRT.
+__global__ void k_clear_types(const Inst *insts, const int *slots, int fresh)
 {
     const Inst &I = insts[slots[blockIdx.y]];
     const long cells = (long)I.W * I.H;
+    const int4 zero = make_int4(0, 0, 0, 0);
     for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < cells;
-         base += (long)gridDim.x * blockDim.x * 16)
-        *reinterpret_cast<int4 *>(I.type + base) = make_int4(0, 0, 0, 0);
+         base += (long)gridDim.x * blockDim.x * 16) {
+        *reinterpret_cast<int4 *>(I.type + base) = zero;
+        if (fresh) {
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) {
+                *reinterpret_cast<int4 *>(I.child + base + q) = zero;
+                *reinterpret_cast<int4 *>(I.parent + base + q) = zero;
+                *reinterpret_cast<int4 *>(I.heading + base + q) = zero;
+                *reinterpret_cast<int4 *>(I.cost + base + q) = zero;
+            }
+        }
+    }
 }
 
 __global__ void k_init_state(const Inst *insts, State *states, const int *slots, int n,
@@ -345,13 +362,13 @@ __global__ void k_init_state(const Inst *insts, State *states, const int *slots,
 }
 
 void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, int n,
-                        int max_cells, int reset_regions, cudaStream_t st)
+                        int max_cells, int fresh, cudaStream_t st)
 {
     if (n <= 0)
         return;
     const int bx = (max_cells / 16 + 255) / 256;
-    k_clear_types<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots);
-    k_init_state<<<(n + 127) / 128, 128, 0, st>>>(d_inst, d_state, d_slots, n, reset_regions);
+    k_clear_types<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots, fresh);
+    k_init_state<<<(n + 127) / 128, 128, 0, st>>>(d_inst, d_state, d_slots, n, fresh);
 }
 
 // ---------------------------------------------------------------------------

@@ -38,9 +38,11 @@ void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, 
 // goal direct-connection precompute for the n slots listed in d_slots
 void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
                         int max_cells, float max_curvature, const Launch &L, cudaStream_t st);
-// search_init for listed slots: reset node types, add the start, reset state
+// search_init for listed slots: reset node types, add the start, reset state;
+// `fresh` (a new request) also zeroes the rest of the node grid and the
+// density-region counts
 void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, int n,
-                        int max_cells, int reset_regions, cudaStream_t st);
+                        int max_cells, int fresh, cudaStream_t st);
 // one planning iteration (loop()) over all active slots; with `ev` (an array
 // of kIterKernels + 1 events) an event is recorded before each kernel and
 // after the last one

@@ -1053,7 +1053,7 @@ void orc_planner_set_plan_data(orc_planner *p, const orc_frame *f, const orc_pla
     orc_search_params(&g->sp, g->W, g->H, min_dist_x, min_dist_z, g->sp.lbx, g->sp.lbz,
                       g->sp.ubx, g->sp.ubz);
     orc_graph_process_direct_goal(g, f, &g->sp, pp->goal_x, pp->goal_z, pp->goal_heading,
-                                  0.8f, &p->probes);
+                                  0.8f, &p->probes_pre);
 }
 
 /* FastRRT::search_init (fastrrt.cpp:85-98) */
@@ -1095,7 +1095,7 @@ int orc_planner_loop(orc_planner *p, int smart)
     orc_graph_accept(g);
 
     orc_f4 bc[2];
-    if (orc_graph_best_goal_connection(g, p->f, p->pp.dist_tol, 1, bc, &p->probes)) {
+    if (orc_graph_best_goal_connection(g, p->f, p->pp.dist_tol, 1, bc, &p->probes_goal)) {
         const int ppx = toi_f(bc[0].x), ppz = toi_f(bc[0].y);
         const float base = in_limits(g, ppx, ppz) ? g->cost[(long)ppz * g->W + ppx] : -1.0f;
         orc_graph_add(g, toi_f(bc[1].x), toi_f(bc[1].y), bc[1].z, ppx, ppz, bc[0].w + base);
@@ -1305,14 +1305,19 @@ static float wrap_pi(float a)
  * largest curvature the planner admits (bicycle model at full steering, the
  * goal-connection and direct-goal Hermite limits), and (5) the last waypoint
  * is within the goal tolerance in distance and heading. */
-int orc_validate_path(orc_planner *p, const float *xyh, int n)
+/* Path checks that need only the frame and the planner's parameters: start
+ * cell, cells in the frame, footprint feasible outside the ego box, no
+ * repeated cell, heading change per chord within the curvature bound, goal
+ * within the distance and heading tolerances.  with_graph adds the graph's
+ * own checks: the graph is a DAG and each waypoint's parent is the one before. */
+static int validate_waypoints(orc_planner *p, const float *xyh, int n, int with_graph)
 {
     const orc_graph *g = p->g;
     if (n < 2)
         return 0;
     if ((int)xyh[0] != p->pp.start_x || (int)xyh[1] != p->pp.start_z)
         return 0;
-    if (!orc_graph_is_consistent(g))
+    if (with_graph && !orc_graph_is_consistent(g))
         return 0;
     const double ms = g->pp.max_steer_rad;
     const double steer = tan(ms), beta = atan(steer / 2);
@@ -1333,10 +1338,12 @@ int orc_validate_path(orc_planner *p, const float *xyh, int n)
             const int px = (int)xyh[3 * (i - 1)], pz = (int)xyh[3 * (i - 1) + 1];
             if (px == x && pz == z)
                 return 0;
-            int ppx, ppz;
-            orc_graph_get_parent(g, x, z, &ppx, &ppz);
-            if (ppx != px || ppz != pz)
-                return 0;
+            if (with_graph) {
+                int ppx, ppz;
+                orc_graph_get_parent(g, x, z, &ppx, &ppz);
+                if (ppx != px || ppz != pz)
+                    return 0;
+            }
             const double chord = sqrt((double)(x - px) * (x - px) + (double)(z - pz) * (z - pz));
             const float dh = wrap_pi(h - xyh[3 * (i - 1) + 2]);
             if (fabs(dh) > (ORC_PI / 2) * kappa * chord + 1e-3)
@@ -1350,6 +1357,16 @@ int orc_validate_path(orc_planner *p, const float *xyh, int n)
     if (fabsf(xyh[3 * (n - 1) + 2] - p->pp.goal_heading) > p->pp.heading_tol)
         return 0;
     return 1;
+}
+
+int orc_validate_path(orc_planner *p, const float *xyh, int n)
+{
+    return validate_waypoints(p, xyh, n, 1);
+}
+
+int orc_validate_waypoints(orc_planner *p, const float *xyh, int n)
+{
+    return validate_waypoints(p, xyh, n, 0);
 }
 
 void orc_kinematic_batch(const orc_graph *g, const orc_frame *f, int n, const int32_t *sx,

@@ -105,7 +105,10 @@ typedef struct {
     uint32_t iter;            /* RNG counter: number of expansions done */
     int smart;
     int has_plan;
-    long long probes;         /* footprint probes executed (reference early exit) */
+    long long probes;         /* footprint probes executed (reference early exit):
+                                 expansion and path optimisation */
+    long long probes_goal;    /* ... of the goal-connection search */
+    long long probes_pre;     /* ... of the goal direct-connection precompute */
 } orc_planner;
 
 /* ---- arithmetic mode ---------------------------------------------------- */
@@ -200,6 +203,9 @@ int orc_interpolate(const float *xyh, int n, int W, int H, float *out, int cap);
 int orc_plan(orc_planner *p, int smart, int max_iter, int *iters);
 /* path validator: DAG, per-waypoint footprint, curvature bound, goal tolerance */
 int orc_validate_path(orc_planner *p, const float *xyh, int n);
+/* the same checks without the graph's own (DAG, parent links): for paths
+ * produced elsewhere, e.g. by the GPU planner */
+int orc_validate_waypoints(orc_planner *p, const float *xyh, int n);
 
 /* batch helpers (OpenMP over candidates) */
 void orc_kinematic_batch(const orc_graph *g, const orc_frame *f, int n, const int32_t *sx,

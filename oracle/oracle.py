@@ -63,7 +63,8 @@ class OrcPlanParams(C.Structure):
 class OrcPlanner(C.Structure):
     _fields_ = [("g", C.POINTER(OrcGraph)), ("f", C.POINTER(OrcFrame)), ("pp", OrcPlanParams),
                 ("last_expanded", C.c_int), ("iter", C.c_uint32), ("smart", C.c_int),
-                ("has_plan", C.c_int), ("probes", C.c_longlong)]
+                ("has_plan", C.c_int), ("probes", C.c_longlong), ("probes_goal", C.c_longlong),
+                ("probes_pre", C.c_longlong)]
 
 
 _lib = None
@@ -159,6 +160,7 @@ def lib():
             "orc_interpolate": (C.c_int, [f32p, C.c_int, C.c_int, C.c_int, f32p, C.c_int]),
             "orc_plan": (C.c_int, [P(OrcPlanner), C.c_int, C.c_int, P(C.c_int)]),
             "orc_validate_path": (C.c_int, [P(OrcPlanner), f32p, C.c_int]),
+            "orc_validate_waypoints": (C.c_int, [P(OrcPlanner), f32p, C.c_int]),
             "orc_kinematic_batch": (None, [P(OrcGraph), P(OrcFrame), C.c_int, i32p, i32p, f32p,
                                            f32p, C.c_float, f32p, i64p, i32p]),
             "orc_feasible_batch": (None, [P(OrcFrame), P(OrcSearch), C.c_int, i32p, i32p, f32p,
@@ -402,6 +404,11 @@ class Planner:
         path = np.ascontiguousarray(path, np.float32).reshape(-1)
         return bool(lib().orc_validate_path(self.p, path, len(path) // 3))
 
+    def validate_waypoints(self, path):
+        """the validator's checks that do not read this planner's graph"""
+        path = np.ascontiguousarray(path, np.float32).reshape(-1)
+        return bool(lib().orc_validate_waypoints(self.p, path, len(path) // 3))
+
     def plan(self, smart=False, max_iter=1000):
         it = C.c_int(0)
         ok = lib().orc_plan(self.p, int(smart), max_iter, C.byref(it))
@@ -409,7 +416,14 @@ class Planner:
 
     @property
     def probes(self):
-        return self.p.contents.probes
+        c = self.p.contents
+        return c.probes + c.probes_goal + c.probes_pre
+
+    @property
+    def probes_by_phase(self):
+        """expansion (+ optimisation), goal-connection search, precompute"""
+        c = self.p.contents
+        return {"expand": c.probes, "goal": c.probes_goal, "pre": c.probes_pre}
 
     @property
     def iterations(self):

@@ -69,27 +69,25 @@ def test_kinematic_matches_golden_fixture(gpu):
     assert np.allclose(out[ok, 2], gold[ok, 2], atol=1e-4, rtol=1e-5)
 
 
-def test_pose_error_against_fp64_integrator(gpu, orc):
-    """Integrated poses: within 1e-4 m / 1e-5 rad of the oracle's FP32
-    integrator (the reference's arithmetic), and the error of both against an
-    FP64 integrator of the same bicycle model stated and bounded.  FP32
-    accumulation over up to ~200 steps of a heading near pi costs ~2.5e-5 rad
-    in the reference itself, so the FP64 bound on heading is 5e-5 rad."""
+def test_pose_error_against_fp64_integrator(gpu, ref, orc):
+    """Integrated poses on an open frame (1-cell footprint, paths run to the
+    frame edge): bit-exact against the reference's kernel, and the error of
+    that FP32 arithmetic against an FP64 integrator of the same bicycle model
+    stated and bounded.  FP32 accumulation over up to ~200 steps of a heading
+    near pi costs ~2.5e-5 rad in the reference itself, so the FP64 bound on
+    heading is 5e-5 rad; positions stay within 1e-4 m."""
     cls = np.zeros((H, W), np.uint8)
     heading, sx, sz, steer, seg = synth.candidates(2000, W, H, 9)
     fr, ctx = ctx_for(gpu, cls, heading, min_dist=(0, 0))
     out, _ = ctx.kinematic(sx, sz, steer, seg, 2.0)
+    rc = ref.RefCase(ref.Frame(cls, synth.CLASS_COSTS), heading=heading, max_steer_rad=MS, lr=LR)
+    r = rc.kinematic(sx, sz, steer, seg, 2.0, device=True)
+    assert np.array_equal(out.view(np.uint32), r.view(np.uint32))
     g = orc.Graph(W, H, 34.56, 34.56, 40.0, 5.4, -1.0, (0, 0))
     g.g.pp.lr, g.g.pp.max_steer_rad = LR, MS
     g.heading[:] = heading
-    orc.set_fp_mode(orc.FP_DEVICE)
-    try:
-        od, _, steps = g.kinematic_batch(orc.Frame(cls, synth.CLASS_COSTS), sx, sz, steer, seg, 2.0)
-    finally:
-        orc.set_fp_mode(orc.FP_HOST)
+    _, _, steps = g.kinematic_batch(orc.Frame(cls, synth.CLASS_COSTS), sx, sz, steer, seg, 2.0)
     ok = out[:, 0] >= 0
-    assert np.array_equal(out[:, :2], od[:, :2])
-    assert np.abs(out[ok, 3] - od[ok, 3]).max() < 1e-5
     p32 = (ctypes.c_double * 3)()
     p64 = (ctypes.c_double * 3)()
     max_m = max_rad = 0.0
