@@ -140,7 +140,7 @@ class BatchPlanner:
         a, g, p = _lib.C.c_uint64(), _lib.C.c_uint64(), _lib.C.c_uint64()
         _lib.check(_lib.lib().fastrrt_batch_probes(self._h, _lib.C.byref(a), _lib.C.byref(g),
                                                    _lib.C.byref(p)), "batch_probes")
-        return {"k_expand": a.value, "k_goal": g.value, "k_direct_goal": p.value}
+        return {"k_expand": a.value, "k_goal": g.value, "k_gd_eval": p.value}
 
     def release(self, slot):
         _lib.check(_lib.lib().fastrrt_batch_release(self._h, slot), "batch_release")

@@ -1046,7 +1046,7 @@ const char *fastrrt_kernel_name(int k)
     if (k >= 0 && k < kIterKernels)
         return kIterKernelNames[k];
     if (k == kIterKernels)
-        return "k_direct_goal";
+        return "k_gd_reset";
     return "";
 }
 

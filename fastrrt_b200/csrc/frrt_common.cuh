@@ -5,7 +5,10 @@
 //   parent  int32  parent cell packed as (x & 0xffff) | (z << 16); (-1,-1) = root
 //   child   int32  child count
 //   heading f32, cost f32, intrinsic f32, direct f32
-//   gd_*    goal direct-connection precompute (flag u8, heading f32, cost f32)
+//   gd_*    goal direct-connection data (flag u8, heading f32, cost f32),
+//           evaluated lazily: flag kGdUnknown until a goal-search window
+//           first covers the cell
+//   memo_*  goal-search result of a node, keyed by its heading and cost bits
 // Frame of one instance: class ids (u8), a bit-packed obstacle mask
 // (class cost < 0) and a bit-packed "clear" mask (no obstacle within the
 // footprint's circumscribed square), optional traversability bits (int32).
@@ -30,6 +33,8 @@ constexpr int kRegion = 128;          // density region edge (graph_expansion_se
 constexpr int kMaxRegions = 1024;     // supports frames up to 4095 x 4095
 constexpr int kFrontierThreshold = 100;  // fastrrt.cpp:116
 constexpr long long kBigCost = 99999999999LL;
+constexpr uint8_t kGdUnknown = 0xFF;  // gd_flag of a cell not evaluated yet
+constexpr unsigned long long kMemoNone = ~0ull;  // memo_key of a cell without a result
 constexpr unsigned kFull = 0xffffffffu;
 
 __host__ __device__ inline int32_t pack_xz(int x, int z)
@@ -57,9 +62,18 @@ struct Inst {
     float *cost;
     float *intrinsic;          // nullptr when all zero
     float *direct;
-    uint8_t *gd_flag;
+    uint8_t *gd_flag;          // 0 / 1, or kGdUnknown
     float *gd_heading;
     float *gd_cost;
+    uint32_t *gd_req;          // bit per cell: evaluation requested
+    int32_t *gd_list;          // cells to evaluate this iteration
+    // goal search of a node is a pure function of (cell, heading, cost) for a
+    // fixed frame, goal and intrinsic costs: results of complete (unpruned)
+    // searches are kept per cell and reused while the node keeps that key
+    unsigned long long *memo_key;  // (heading bits << 32) | cost bits, or kMemoNone
+    long long *memo_best;
+    int32_t *memo_cell;
+    float *memo_seg;
     // per-iteration scratch
     int32_t *claim;
     int32_t *cand;
@@ -83,6 +97,7 @@ struct Inst {
     double max_steer;          // rad
     double lr;                 // vehicle length / 2 (m)
     float max_curvature;       // PHYSICAL_MAX_CURVATURE as float
+    float gd_max_curvature;    // curvature limit of the goal direct connections
     float velocity, max_path, dist_tol, heading_tol;
     int start_x, start_z;
     float start_heading;
@@ -107,6 +122,7 @@ struct State {
     int temp_count;
     int all_count;
     int n_nodes;               // listed NODE cells for the goal search
+    int n_gd;                  // cells listed for goal direct-connection evaluation
     int skip;                  // graph was empty: start re-added, rest skipped
     int found;                 // goal connection found this iteration
     unsigned long long winner; // (cell << 32) | listed index of the best connection

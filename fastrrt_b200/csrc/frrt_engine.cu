@@ -146,6 +146,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         4 * (size_t)kMaxRegions,            // 22 region_count
         4 * (size_t)kMaxRegions,            // 23 region_new
         4 * (size_t)mask_words_,            // 24 clear-mask scratch
+        C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
+        8 * C, 8 * C, 4 * C, 4 * C,         // 27 memo key, 28 best, 29 cell, 30 seg
     };
     constexpr int kParts = sizeof(parts) / sizeof(parts[0]);
     size_t per_slot = 0;
@@ -197,6 +199,12 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         I.region_count = (unsigned *)ptr[22];
         I.region_new = (unsigned *)ptr[23];
         I.rowdil = (uint32_t *)ptr[24];
+        I.gd_req = (uint32_t *)ptr[25];
+        I.gd_list = (int32_t *)ptr[26];
+        I.memo_key = (unsigned long long *)ptr[27];
+        I.memo_best = (long long *)ptr[28];
+        I.memo_cell = (int32_t *)ptr[29];
+        I.memo_seg = (float *)ptr[30];
         I.lbx = I.lbz = I.ubx = I.ubz = -1;
         I.stop_on_goal = 1;
         if (!check(cudaMemsetAsync(I.claim, 0x7F, 4 * C, stream_), "claim init"))
@@ -207,7 +215,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMemsetAsync(d_state_, 0, sizeof(State) * n_slots, stream_), "state init") &&
               check(cudaMallocHost(&h_state_, sizeof(State) * n_slots), "pinned state") &&
               check(cudaMalloc(&d_sched_, sizeof(Sched)), "sched") &&
-              check(cudaMalloc(&d_sched_arrays_, sizeof(int) * 3 * (n_slots + 1)), "sched arrays") &&
+              check(cudaMalloc(&d_sched_arrays_, sizeof(int) * 4 * (n_slots + 1)), "sched arrays") &&
               check(cudaMalloc(&d_grab_, sizeof(unsigned) * 4), "grab counters") &&
               check(cudaMalloc(&d_slots_, sizeof(int) * n_slots), "slot list") &&
               check(cudaMalloc(&d_class_costs_, sizeof(float) * kMaxClasses * n_slots), "class costs") &&
@@ -215,7 +223,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMallocHost(&h_small_, sizeof(int) * 64), "pinned scratch") &&
               check(cudaMalloc(&d_newcost_, sizeof(float) * kOptCap * kOptCap), "optimize scratch") &&
               check(cudaMalloc(&d_changed_, sizeof(int)), "optimize flag") &&
-              check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 3 * (n_slots + 1), stream_), "sched init") &&
+              check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 4 * (n_slots + 1), stream_), "sched init") &&
               check(cudaMemsetAsync(d_grab_, 0, sizeof(unsigned) * 4, stream_), "grab init") &&
               check(cudaMemsetAsync(d_class_costs_, 0, sizeof(float) * kMaxClasses * n_slots, stream_), "costs init");
     if (!ok)
@@ -396,7 +404,7 @@ bool Engine::commit()
                                cudaMemcpyHostToDevice, stream_),
                "inst upload"))
         return false;
-    std::vector<int> arrays(3 * (n_slots_ + 1), 0);
+    std::vector<int> arrays(4 * (n_slots_ + 1), 0);
     int run = 0;
     for (int s = 0; s < n_slots_; s++) {
         arrays[s] = run;
@@ -409,6 +417,7 @@ bool Engine::commit()
     h_sched_.sweep_start = d_sched_arrays_;
     h_sched_.cand_start = d_sched_arrays_ + (n_slots_ + 1);
     h_sched_.node_start = d_sched_arrays_ + 2 * (n_slots_ + 1);
+    h_sched_.gd_start = d_sched_arrays_ + 3 * (n_slots_ + 1);
     h_sched_.grab = d_grab_;
     const int sweep_blocks = std::max(1, std::min(L_.sms * 8, run));
     if (sweep_blocks != L_.sweep_blocks) {
@@ -441,6 +450,12 @@ bool Engine::upload_slots_list(const std::vector<int> &slots)
 
 bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
 {
+    for (int sl : slots) {
+        if (h_inst_[sl].gd_max_curvature != direct_max_curvature) {
+            h_inst_[sl].gd_max_curvature = direct_max_curvature;
+            dirty_ = true;
+        }
+    }
     if (dirty_ && !commit())
         return false;
     if (slots.empty())
@@ -463,8 +478,7 @@ bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
                        stream_);
     if (profiling_)
         cudaEventRecord(prof_ev_[kIterKernels + 1], stream_);
-    launch_direct_goal(d_inst_, d_state_, d_slots_, (int)slots.size(), max_cells,
-                       direct_max_curvature, L_, stream_);
+    launch_direct_goal_reset(d_inst_, d_slots_, (int)slots.size(), max_cells, stream_);
     if (profiling_) {
         cudaEventRecord(prof_ev_[kIterKernels + 2], stream_);
         float ms = 0;
@@ -738,14 +752,33 @@ bool Engine::grid_upload(int slot, const std::vector<int8_t> &type, const std::v
               check(cudaMemcpyAsync(I.heading, heading.data(), 4 * n, cudaMemcpyHostToDevice, stream_), "heading") &&
               check(cudaMemcpyAsync(I.cost, cost.data(), 4 * n, cudaMemcpyHostToDevice, stream_), "cost") &&
               check(cudaMemcpyAsync(I.direct, direct.data(), 4 * n, cudaMemcpyHostToDevice, stream_), "direct");
+    // the deferred goal direct connections read the intrinsic costs of
+    // set_plan_data time: evaluate the rest before they are replaced; kept
+    // goal-search results depend on them too
+    ok = ok && gd_complete(slot) &&
+         check(cudaMemsetAsync(I.memo_key, 0xFF, 8 * n, stream_), "memo reset");
     if (ok)
         ok = set_intrinsic(slot, any_intr ? intrinsic.data() : nullptr);
     return ok && commit();
 }
 
+bool Engine::gd_complete(int slot)
+{
+    const Inst &I = h_inst_[slot];
+    if (I.W <= 0)
+        return true;
+    const std::vector<int> one{slot};
+    if (!upload_slots_list(one))
+        return false;
+    launch_direct_goal_complete(d_inst_, d_state_, d_slots_, 1, I.W * I.H, stream_);
+    return check(cudaGetLastError(), "goal direct-connection completion") && sync();
+}
+
 bool Engine::gd_download(int slot, std::vector<uint8_t> &flag, std::vector<float> &heading,
                          std::vector<float> &cost)
 {
+    if (!gd_complete(slot))
+        return false;
     const Inst &I = h_inst_[slot];
     const size_t n = (size_t)I.W * I.H;
     flag.resize(n);

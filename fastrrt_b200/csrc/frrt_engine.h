@@ -120,6 +120,8 @@ public:
                      const std::vector<int32_t> &child, const std::vector<float> &heading,
                      const std::vector<float> &cost, const std::vector<float> &intrinsic,
                      const std::vector<float> &direct);
+    // evaluates every goal direct connection of the slot still unknown
+    bool gd_complete(int slot);
     bool gd_download(int slot, std::vector<uint8_t> &flag, std::vector<float> &heading,
                      std::vector<float> &cost);
     bool regions_upload(int slot, const std::vector<unsigned> &counts);

@@ -223,73 +223,98 @@ struct PrecompTask {
     __device__ float probe_angle() const { return h.pend_heading; }
 };
 
-__global__ void __launch_bounds__(256) k_direct_goal(const Inst *insts, State *states,
-                                                     const int *slots, float max_curvature,
-                                                     int smem_words)
+// Deferred precompute.  Only the goal search reads a cell's direct connection
+// (graph_check_goal_reached.cu:53-63), and only for cells inside the window
+// of a node it searches, so each cell is evaluated the first time such a
+// window covers it, with the same function and arguments as the eager pass
+// (graph_direct_goal_connection.cu:169-227).
+__global__ void k_gd_reset(const Inst *insts, const int *slots)
 {
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ __align__(8) uint64_t bar;
+    const Inst &I = insts[slots[blockIdx.y]];
+    const long cells = (long)I.W * I.H;
+    const long words = (cells + 31) / 32;
+    const int4 ones = make_int4(-1, -1, -1, -1);
+    for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < cells;
+         base += (long)gridDim.x * blockDim.x * 16) {
+        *reinterpret_cast<int4 *>(I.gd_flag + base) = ones;
+#pragma unroll
+        for (int q = 0; q < 16; q += 2)
+            *reinterpret_cast<int4 *>(I.memo_key + base + q) = ones;
+        // the eager pass starts each curve from the cell's graph cost at
+        // set_plan_data time: keep it until the cell is evaluated
+#pragma unroll
+        for (int q = 0; q < 16; q += 4)
+            *reinterpret_cast<int4 *>(I.gd_cost + base + q) =
+                *reinterpret_cast<const int4 *>(I.cost + base + q);
+    }
+    for (long w = (long)blockIdx.x * blockDim.x + threadIdx.x; w < words;
+         w += (long)gridDim.x * blockDim.x)
+        I.gd_req[w] = 0u;
+}
+
+void launch_direct_goal_reset(const Inst *d_inst, const int *d_slots, int n, int max_cells,
+                              cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    const int bx = (max_cells / 16 + 255) / 256;
+    k_gd_reset<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots);
+}
+
+// Evaluates the goal direct connection of cells: listed ones (list mode, one
+// chunk of kGdChunk list entries per grab) or, without a list, every cell of
+// the slots in `slots` still unknown (one chunk of kGdChunk cells per grab).
+__device__ void gd_eval_cell(const Inst &I, const Foot &f, bool has, int pos,
+                             unsigned long long &probes)
+{
+    PrecompTask t;
+    float lh = 0.0f;
+    if (has) {
+        const int z = pos / I.W;
+        const int x = pos - z * I.W;
+        lh = compute_heading(x, z, I.goal_x, I.goal_z);
+        t.h.init(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading, 0,
+                 I.gd_cost[pos]);
+    }
+    run_warp(t, has, f, probes, [](const PrecompTask &q) { return q.h.last_x; },
+             [](const PrecompTask &q) { return q.h.last_z; });
+    if (has) {
+        if (t.h.ok) {
+            I.gd_heading[pos] = lh;
+            I.gd_cost[pos] = t.h.nodeCost;
+        }
+        I.gd_flag[pos] = t.h.ok ? 1 : 0;
+    }
+}
+
+// every still unknown cell of the listed slots (before the intrinsic costs
+// that the deferred evaluation reads are replaced)
+__global__ void __launch_bounds__(256) k_gd_complete(const Inst *insts, State *states,
+                                                     const int *slots)
+{
     const int slot = slots[blockIdx.y];
     const Inst &I = insts[slot];
     const int cells = I.W * I.H;
     if ((long)blockIdx.x * blockDim.x >= cells)
         return;
-    const uint32_t *blk = I.blocked, *clr = I.clear;
-    bool use_smem = smem_words > 0 && I.mask_words <= smem_words;
-    unsigned phase = 0;
-    if (use_smem) {
-        if (threadIdx.x == 0)
-            mbar_init(&bar, 1);
-        __syncthreads();
-        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase)) {
-            blk = smem;
-            clr = smem + smem_words;
-        } else {
-            if (threadIdx.x == 0)
-                atomicExch(&states[slot].error, 1);
-            for (long k = 0; k < kWaitLimit; k++)
-                if (mbar_try_wait(&bar, phase ^ 1u))
-                    break;
-        }
-    }
-    const Foot f = foot_of(I, blk, clr);
-    const float maxc = max_curvature < 0 ? I.max_curvature : max_curvature;
+    const Foot f = foot_of(I, I.blocked, I.clear);
     unsigned long long probes = 0;
     for (long base = (long)blockIdx.x * blockDim.x; base < cells; base += (long)gridDim.x * blockDim.x) {
         const long pos = base + threadIdx.x;
-        const bool has = pos < cells;
-        PrecompTask t;
-        float lh = 0.0f;
-        int x = 0, z = 0;
-        if (has) {
-            z = (int)(pos / I.W);
-            x = (int)(pos - (long)z * I.W);
-            I.gd_flag[pos] = 0;
-            lh = compute_heading(x, z, I.goal_x, I.goal_z);
-            t.h.init(I, f, maxc, x, z, lh, I.goal_x, I.goal_z, I.goal_heading, 0, I.cost[pos]);
-        }
-        run_warp(t, has, f, probes, [](const PrecompTask &q) { return q.h.last_x; },
-                 [](const PrecompTask &q) { return q.h.last_z; });
-        if (has && t.h.ok) {
-            I.gd_flag[pos] = 1;
-            I.gd_heading[pos] = lh;
-            I.gd_cost[pos] = t.h.nodeCost;
-        }
+        const bool has = pos < cells && I.gd_flag[pos] == kGdUnknown;
+        gd_eval_cell(I, f, has, has ? (int)pos : 0, probes);
     }
     probes = warp_sum64(probes);
     if ((threadIdx.x & 31) == 0 && probes)
         atomicAdd(&states[slot].probes_pre, probes);
 }
 
-void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
-                        int max_cells, float max_curvature, const Launch &L, cudaStream_t st)
+void launch_direct_goal_complete(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                                 int max_cells, cudaStream_t st)
 {
     if (n <= 0)
         return;
-    const int bx = (max_cells + 255) / 256;
-    const dim3 grid(bx, n);
-    const size_t smem = (size_t)L.smem_words * 2 * 4;
-    k_direct_goal<<<grid, 256, smem, st>>>(d_inst, d_state, d_slots, max_curvature, L.smem_words);
+    k_gd_complete<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_state, d_slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -311,6 +336,10 @@ __global__ void k_clear_types(const Inst *insts, const int *slots, int fresh)
     for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < cells;
          base += (long)gridDim.x * blockDim.x * 16) {
         *reinterpret_cast<int4 *>(I.type + base) = zero;
+        // the intrinsic costs that goal searches read may change here
+#pragma unroll
+        for (int q = 0; q < 16; q += 2)
+            *reinterpret_cast<int4 *>(I.memo_key + base + q) = make_int4(-1, -1, -1, -1);
         if (fresh) {
 #pragma unroll
             for (int q = 0; q < 16; q += 4) {
@@ -344,6 +373,7 @@ __global__ void k_init_state(const Inst *insts, State *states, const int *slots,
     S.temp_count = 0;
     S.all_count = 0;
     S.n_nodes = 0;
+    S.n_gd = 0;
     S.skip = 0;
     S.found = 0;
     S.winner = 0;
@@ -427,11 +457,19 @@ __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, 
 }
 
 // prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
+// work chunks of one slot: 0 candidates, 1 listed nodes, 2 listed cells
+__device__ __forceinline__ int chunks_of(const State &S, int which)
+{
+    return which == 0 ? (S.n_cand + kCandChunk - 1) / kCandChunk
+           : which == 1 ? (S.n_nodes + kNodeChunk - 1) / kNodeChunk
+                        : (S.n_gd + kGdChunk - 1) / kGdChunk;
+}
+
 __global__ void __launch_bounds__(1024) k_plan(const State *states, Sched *sc, int which)
 {
     __shared__ int warp_tot[32];
     const int n = sc->n_slots;
-    int *out = which == 0 ? sc->cand_start : sc->node_start;
+    int *out = which == 0 ? sc->cand_start : which == 1 ? sc->node_start : sc->gd_start;
     const int per = (n + blockDim.x - 1) / blockDim.x;
     const int s0 = threadIdx.x * per;
     int local = 0;
@@ -439,8 +477,7 @@ __global__ void __launch_bounds__(1024) k_plan(const State *states, Sched *sc, i
         const State &S = states[s];
         if (!live(S))
             continue;
-        local += which == 0 ? (S.n_cand + kCandChunk - 1) / kCandChunk
-                            : (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
+        local += chunks_of(S, which);
     }
     // block exclusive scan of `local`
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -468,8 +505,7 @@ __global__ void __launch_bounds__(1024) k_plan(const State *states, Sched *sc, i
         out[s] = run;
         const State &S = states[s];
         if (live(S))
-            run += which == 0 ? (S.n_cand + kCandChunk - 1) / kCandChunk
-                              : (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
+            run += chunks_of(S, which);
     }
     if (threadIdx.x == blockDim.x - 1)
         out[n] = run;
@@ -749,6 +785,21 @@ __global__ void __launch_bounds__(256) k_setnodes(const Inst *insts, State *stat
 }
 
 // TEMP count, non-NULL count, TEMP -> NODE, and the NODE list
+__device__ __forceinline__ unsigned long long memo_key_of(const Inst &I, int pos)
+{
+    return ((unsigned long long)__float_as_uint(I.heading[pos]) << 32) |
+           (unsigned long long)__float_as_uint(I.cost[pos]);
+}
+
+// checkGoalReached for one node (graph_best_node.cu:181-222)
+__device__ __forceinline__ void goal_check_node(const Inst &I, State &S, int pos)
+{
+    const int z = pos / I.W, x = pos - z * I.W;
+    const double dx = I.goal_x - x, dz = I.goal_z - z;
+    if (!(sqrt(dx * dx + dz * dz) > I.dist_tol) && fabsf(I.heading[pos] - I.goal_heading) <= I.heading_tol)
+        S.goal_reached = 1;
+}
+
 __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states, const Sched *sc)
 {
     const int n = sc->n_slots;
@@ -777,8 +828,16 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
                     t[k] = T_NODE;
                     changed = true;
                 }
-                if (t[k] == T_NODE)
-                    mine[cnt++] = base + k;
+                if (t[k] != T_NODE)
+                    continue;
+                const int pos = base + k;
+                if (I.memo_key[pos] == memo_key_of(I, pos) && I.memo_best[pos] >= kBigCost) {
+                    // searched before with this heading and cost and no
+                    // connection found: only the goal check remains
+                    goal_check_node(I, S, pos);
+                    continue;
+                }
+                mine[cnt++] = pos;
             }
             if (changed)
                 *reinterpret_cast<int4 *>(I.type + base) = v;
@@ -797,6 +856,100 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
     }
 }
 
+__device__ __forceinline__ int window_count(int c, float r, int &lo)
+{
+    lo = (int)(c - r);
+    const float hi = c + r;
+    const int k0 = (int)ceilf(hi);
+    return k0 > lo ? k0 - lo : 0;
+}
+
+// Lists, once per cell, the cells inside the windows of the nodes that the
+// goal search will search this iteration whose direct connection is unknown.
+__global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *states, const Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->node_start[n];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->node_start, n, c);
+        const Inst &I = insts[slot];
+        State &S = states[slot];
+        const int idx = (c - sc->node_start[slot]) * kNodeChunk + warp;
+        if (idx >= S.n_nodes)
+            continue;  // uniform across the warp
+        const int pos = I.nodes[idx];
+        if (I.memo_key[pos] == memo_key_of(I, pos))
+            continue;  // the search result is known: no window is read
+        const int z = pos / I.W, x = pos - z * I.W;
+        int zlo, xlo;
+        const int nz = window_count(z, I.dist_tol, zlo);
+        const int nx = window_count(x, I.dist_tol, xlo);
+        const int wtotal = nx > 0 ? nz * nx : 0;
+        for (int w0 = 0; w0 < wtotal; w0 += 32) {
+            const int w = w0 + lane;
+            int cell = -1;
+            if (w < wtotal) {
+                const int zp = zlo + w / nx, xp = xlo + w % nx;
+                if (zp >= 0 && zp < I.H && xp >= 0 && xp < I.W) {
+                    const int cc = zp * I.W + xp;
+                    if (I.gd_flag[cc] == kGdUnknown) {
+                        const uint32_t bit = 1u << (cc & 31);
+                        if (!(atomicOr(&I.gd_req[cc >> 5], bit) & bit))
+                            cell = cc;
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(kFull, cell >= 0);
+            if (!m)
+                continue;
+            int at = 0;
+            if (lane == 0)
+                at = atomicAdd(&S.n_gd, __popc(m));
+            at = __shfl_sync(kFull, at, 0);
+            if (cell >= 0)
+                I.gd_list[at + __popc(m & ((1u << lane) - 1u))] = cell;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gd_eval(const Inst *insts, State *states, Sched *sc,
+                                                 int smem_words)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_chunk;
+    const int n = sc->n_slots;
+    const int total = sc->gd_start[n];
+    Stage sg{-1, false, 0u};
+    if (threadIdx.x == 0)
+        mbar_init(&bar, 1);
+    __syncthreads();
+    while (true) {
+        if (threadIdx.x == 0)
+            s_chunk = (int)atomicAdd(&sc->grab[2], 1u);
+        __syncthreads();
+        const int c = s_chunk;
+        __syncthreads();
+        if (c >= total)
+            break;
+        const int slot = find_slot(sc->gd_start, n, c);
+        const Inst &I = insts[slot];
+        State &S = states[slot];
+        const uint32_t *blk, *clr;
+        stage_for(I, slot, sg, smem, smem_words, &bar, states, blk, clr);
+        const Foot f = foot_of(I, blk, clr);
+        const int idx = (c - sc->gd_start[slot]) * kGdChunk + threadIdx.x;
+        const bool has = idx < S.n_gd;
+        unsigned long long probes = 0;
+        gd_eval_cell(I, f, has, has ? I.gd_list[idx] : 0, probes);
+        probes = warp_sum64(probes);
+        if ((threadIdx.x & 31) == 0 && probes)
+            atomicAdd(&S.probes_pre, probes);
+    }
+    stage_drain(sg, &bar);
+}
+
 // best connection of one graph node to a precomputed goal-connected cell in
 // its window (graph_check_goal_reached.cu:17-70), plus checkGoalReached for
 // the node (graph_best_node.cu:181-222)
@@ -813,6 +966,7 @@ struct GoalLane {
     const Inst *I;
     const volatile long long *global_best;
     bool prune;
+    bool pruned;               // a window cell was skipped by the bound
 
     __device__ int advance(const Foot &f, unsigned long long &probes)
     {
@@ -834,8 +988,10 @@ struct GoalLane {
                     // the connection costs at least cost + 1 (the first sample)
                     const float lb_total = (cost + 1.0f) + gdc;
                     const long long lb = __float2ll_rd(100 * lb_total);
-                    if (lb > *global_best)
+                    if (lb > *global_best) {
+                        pruned = true;
                         continue;
+                    }
                 }
                 h.init(*I, f, I->max_curvature, x, z, heading, xp, zp, I->gd_heading[cell], 1, cost);
                 cell_cur = cell;
@@ -865,14 +1021,6 @@ struct GoalLane {
     }
     __device__ float probe_angle() const { return h.pend_heading; }
 };
-
-__device__ __forceinline__ int window_count(int c, float r, int &lo)
-{
-    lo = (int)(c - r);
-    const float hi = c + r;
-    const int k0 = (int)ceilf(hi);
-    return k0 > lo ? k0 - lo : 0;
-}
 
 __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, Sched *sc,
                                               int smem_words)
@@ -906,18 +1054,27 @@ __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, 
         unsigned long long probes = 0;
         if (has) {
             const int pos = I.nodes[idx];
+            if (lane == 0)
+                goal_check_node(I, S, pos);
+            const unsigned long long key = memo_key_of(I, pos);
+            if (I.memo_key[pos] == key) {
+                // a complete search with this heading and cost was kept
+                if (lane == 0) {
+                    const long long b = I.memo_best[pos];
+                    I.node_best[idx] = b;
+                    I.node_best_cell[idx] = I.memo_cell[pos];
+                    I.node_best_seg[idx] = I.memo_seg[pos];
+                    if (b < kBigCost)
+                        atomicMin(&S.best, b);
+                }
+                continue;
+            }
             GoalLane g;
             g.I = &I;
             g.z = pos / I.W;
             g.x = pos - g.z * I.W;
             g.heading = I.heading[pos];
             g.cost = I.cost[pos];
-            if (lane == 0) {
-                const double dx = I.goal_x - g.x, dz = I.goal_z - g.z;
-                if (!(sqrt(dx * dx + dz * dz) > I.dist_tol) &&
-                    fabsf(g.heading - I.goal_heading) <= I.heading_tol)
-                    S.goal_reached = 1;
-            }
             const int nz = window_count(g.z, I.dist_tol, g.zlo);
             g.nx = window_count(g.x, I.dist_tol, g.xlo);
             g.wtotal = g.nx > 0 ? nz * g.nx : 0;
@@ -928,6 +1085,7 @@ __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, 
             g.best_seg = 0.0f;
             g.global_best = &S.best;
             g.prune = I.intrinsic == nullptr;
+            g.pruned = false;
             run_warp(g, true, f, probes, [](const GoalLane &q) { return q.h.last_x; },
                      [](const GoalLane &q) { return q.h.last_z; });
             // warp minimum of best, ties to the highest cell index
@@ -944,12 +1102,19 @@ __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, 
                     bs = os;
                 }
             }
+            const bool complete = !__any_sync(kFull, g.pruned);
             if (lane == 0) {
                 I.node_best[idx] = b;
                 I.node_best_cell[idx] = bc;
                 I.node_best_seg[idx] = bs;
                 if (b < kBigCost)
                     atomicMin(&S.best, b);
+                if (complete) {
+                    I.memo_best[pos] = b;
+                    I.memo_cell[pos] = bc;
+                    I.memo_seg[pos] = bs;
+                    I.memo_key[pos] = key;
+                }
             }
         }
         probes = warp_sum64(probes);
@@ -1029,6 +1194,7 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
     S.temp_count = 0;
     S.all_count = 0;
     S.n_nodes = 0;
+    S.n_gd = 0;
     S.collision = 0;
     S.best = kBigCost;
     S.winner = 0;
@@ -1043,7 +1209,8 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
 
 const char *const kIterKernelNames[kIterKernels] = {
     "k_scan", "k_plan(cand)", "k_expand", "k_apply", "k_post", "k_erase",
-    "k_setnodes", "k_accept", "k_plan(nodes)", "k_goal", "k_select", "k_finish"};
+    "k_setnodes", "k_accept", "k_plan(nodes)", "k_gd_demand", "k_plan(cells)", "k_gd_eval",
+    "k_goal", "k_select", "k_finish"};
 
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
                       const Launch &L, cudaStream_t st, cudaEvent_t *ev)
@@ -1073,6 +1240,12 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     k_accept<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 1);
+    mark();
+    k_gd_demand<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
+    k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 2);
+    mark();
+    k_gd_eval<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
     mark();
     k_goal<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
     mark();
@@ -1656,7 +1829,7 @@ void configure_kernels(int smem_bytes)
 {
     cudaFuncSetAttribute(k_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_goal, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-    cudaFuncSetAttribute(k_direct_goal, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    cudaFuncSetAttribute(k_gd_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_candidates, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_hermite, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
 }

@@ -10,6 +10,7 @@ namespace frrt {
 constexpr int kSweepCells = 4096;   // cells per sweep chunk (256 threads x 16)
 constexpr int kCandChunk = 256;     // candidates per expansion chunk (one per thread)
 constexpr int kNodeChunk = 8;       // listed nodes per goal-search chunk (one per warp)
+constexpr int kGdChunk = 256;       // listed cells per direct-connection chunk (one per thread)
 constexpr int32_t kClaimFree = 0x7F7F7F7F;
 
 // Scheduling tables shared by the iteration kernels (device memory).
@@ -19,6 +20,7 @@ struct Sched {
     int *sweep_start;         // [n_slots + 1] prefix of sweep chunks per slot
     int *cand_start;          // [n_slots + 1] prefix of candidate chunks per slot
     int *node_start;          // [n_slots + 1] prefix of node chunks per slot
+    int *gd_start;            // [n_slots + 1] prefix of direct-connection chunks per slot
     unsigned *grab;           // [4] dynamic work counters
 };
 
@@ -35,9 +37,15 @@ void configure_kernels(int smem_bytes);
 // frame preparation for listed slots: obstacle and clear masks
 void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_words,
                         int ncls_max, int *d_bad_class, cudaStream_t st);
-// goal direct-connection precompute for the n slots listed in d_slots
-void launch_direct_goal(const Inst *d_inst, State *d_state, const int *d_slots, int n,
-                        int max_cells, float max_curvature, const Launch &L, cudaStream_t st);
+// processDirectGoalConnection for the n listed slots, deferred: marks every
+// cell's goal direct connection as not evaluated; the iterations evaluate
+// the cells that goal-search windows reach
+void launch_direct_goal_reset(const Inst *d_inst, const int *d_slots, int n, int max_cells,
+                              cudaStream_t st);
+// evaluates every cell of the listed slots whose goal direct connection is
+// still unknown
+void launch_direct_goal_complete(const Inst *d_inst, State *d_state, const int *d_slots, int n,
+                                 int max_cells, cudaStream_t st);
 // search_init for listed slots: reset node types, add the start, reset state;
 // `fresh` (a new request) also zeroes the rest of the node grid and the
 // density-region counts
@@ -46,7 +54,7 @@ void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, 
 // one planning iteration (loop()) over all active slots; with `ev` (an array
 // of kIterKernels + 1 events) an event is recorded before each kernel and
 // after the last one
-constexpr int kIterKernels = 12;
+constexpr int kIterKernels = 15;
 extern const char *const kIterKernelNames[kIterKernels];
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
                       const Launch &L, cudaStream_t st, cudaEvent_t *ev = nullptr);

@@ -193,11 +193,13 @@ int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_
  * CUDA events instead of replaying the CUDA graph */
 int fastrrt_batch_profile(void *batch, int on);
 /* per-kernel device time (ms) and launch counts since profiling was turned
- * on: fastrrt_kernel_count() entries, the last one the goal precompute */
+ * on: fastrrt_kernel_count() entries, the last one the admission-time reset
+ * of the goal direct connections (which the iterations evaluate on demand) */
 int fastrrt_batch_kernel_times(void *batch, double *ms, int64_t *launches);
 int fastrrt_kernel_count(void);
 /* footprint probes of the reference algorithm, summed over the slots of the
- * last admission: expansion, goal-connection search, goal precompute */
+ * last admission: expansion, goal-connection search, goal direct-connection
+ * evaluation */
 int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute);
 const char *fastrrt_kernel_name(int k);
 

@@ -86,8 +86,17 @@ def test_pose_error_against_fp64_integrator(gpu, ref, orc):
     g = orc.Graph(W, H, 34.56, 34.56, 40.0, 5.4, -1.0, (0, 0))
     g.g.pp.lr, g.g.pp.max_steer_rad = LR, MS
     g.heading[:] = heading
-    _, _, steps = g.kinematic_batch(orc.Frame(cls, synth.CLASS_COSTS), sx, sz, steer, seg, 2.0)
-    ok = out[:, 0] >= 0
+    # the step count of each candidate from the oracle in device arithmetic;
+    # candidates whose end cell differs there (a corner touched in one
+    # rounding and not the other) are left out of the FP64 comparison
+    orc.set_fp_mode(orc.FP_DEVICE)
+    try:
+        od, _, steps = g.kinematic_batch(orc.Frame(cls, synth.CLASS_COSTS), sx, sz, steer, seg, 2.0)
+    finally:
+        orc.set_fp_mode(orc.FP_HOST)
+    same = np.all(od[:, :2] == out[:, :2], axis=1)
+    assert same.mean() > 0.99
+    ok = (out[:, 0] >= 0) & same
     p32 = (ctypes.c_double * 3)()
     p64 = (ctypes.c_double * 3)()
     max_m = max_rad = 0.0
