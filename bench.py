@@ -74,32 +74,36 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(v, world):
+def reduce_over_ranks(v, world, op="max"):
+    """max or sum of a per-rank scalar (NCCL on the GPUs, gloo on the CPU)"""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(v, world):
+    return reduce_over_ranks(v, world, "max")
 
 
 def sum_over_ranks(v, world):
-    if world == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return reduce_over_ranks(v, world, "sum")
+
+
+def request_seeds(rank, step, B):
+    """seeds of the B requests of one step on one rank; ranks never share one"""
+    return [(rank * 1000003 + step * B + k) & 0xFFFFFFFF for k in range(B)]
 
 
 def workload(rank, step, B):
     """seeded requests of one step: (frames, starts, goals, seeds)"""
     from fastrrt_b200 import synth
     frames, starts, goals, seeds = [], [], [], []
-    for k in range(B):
-        seed = (rank * 1000003 + step * B + k) & 0xFFFFFFFF
+    for seed in request_seeds(rank, step, B):
         cls, st, gl = synth.c0_request(seed, SIZE)
         frames.append(cls)
         starts.append(st)
