@@ -49,6 +49,7 @@ EXPORTS = [
     "fastrrt_candidates_create", "fastrrt_candidates_destroy", "fastrrt_candidates_kinematic",
     "fastrrt_candidates_kinematic_device", "fastrrt_candidates_hermite",
     "fastrrt_candidates_hermite_device", "fastrrt_candidates_feasible",
+    "fastrrt_candidates_kinematic_noalloc",
     # batched planner
     "fastrrt_batch_create", "fastrrt_batch_destroy", "fastrrt_batch_admit",
     "fastrrt_batch_admit_many", "fastrrt_batch_run", "fastrrt_batch_step", "fastrrt_batch_status",
@@ -116,6 +117,11 @@ def lib():
                                                         C.c_float, C.c_int, vp, vp, vp]),
         "fastrrt_candidates_feasible": (C.c_int, [vp, C.c_int, i32p, i32p, f32p, i32p,
                                                   P(C.c_uint64)]),
+        "fastrrt_candidates_kinematic_noalloc": (C.c_int, [C.c_int, C.c_int, vp, vp, C.c_int, vp,
+                                                           vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                           C.c_int, C.c_int, C.c_double,
+                                                           C.c_double, C.c_int, vp, vp, vp, vp,
+                                                           C.c_float, vp, vp, vp]),
         "fastrrt_batch_create": (vp, [C.c_int, C.c_int, C.c_int]),
         "fastrrt_batch_destroy": (None, [vp]),
         "fastrrt_batch_admit": (C.c_int, [vp, C.c_int, P(Request), C.c_int]),

@@ -124,6 +124,33 @@ int fastrrt_candidates_hermite_device(void *ctx, int n, const int32_t *x, const 
                                       const int32_t *goal_z, const float *goal_heading,
                                       float max_curvature, int safe_zone_checked, float *out,
                                       uint64_t *probes, void *stream);
+/* No counterpart in the reference.  The kinematic candidate check of
+ * fastrrt_candidates_kinematic_device() for callers that cannot allocate
+ * device memory: a real-time loop whose memory is reserved up front, a
+ * process whose memory-pool policy forbids new device allocations, code that
+ * must not enter the driver's allocator while other work runs.  It calls no
+ * cudaMalloc / cudaFree: its working memory (instance record and frame masks,
+ * about 390 KB) is one static device array that every GPU loading this
+ * library keeps until the process exits.  Every pointer is device memory:
+ * the frame's width*height class ids, its n_classes costs (cost < 0 =
+ * obstacle), the width*height heading and cost grids the candidates start
+ * from, the n candidates and out4 (n float4); *probes, when given, is added
+ * to.  Frames larger than 1024 x 1024 cells are rejected with an error, and
+ * candidate cells must lie in the frame.  The first call on a device looks
+ * up the array's address on that device: make it before any stream capture.
+ * The call runs on `stream` (NULL = default) and returns after the stream
+ * has finished it.  Calls share the array: calls from this library's callers
+ * are serialised by a lock, but work that overlaps on the GPU from another
+ * route (e.g. the same library loaded twice in one process) would race. */
+int fastrrt_candidates_kinematic_noalloc(int width, int height, const uint8_t *class_ids,
+                                         const float *class_costs, int n_classes,
+                                         const float *heading_grid, const float *cost_grid,
+                                         int min_dist_x, int min_dist_z, int lowerBound_x,
+                                         int lowerBound_z, int upperBound_x, int upperBound_z,
+                                         double max_steering_rad, double lr_m, int n,
+                                         const int32_t *sx, const int32_t *sz, const float *steer,
+                                         const float *length, float velocity_m_s, float *out4,
+                                         uint64_t *probes, void *stream);
 /* __computeFeasibleForAngle (src/cuda/path_feasible.cu:18-78). Host buffers. */
 int fastrrt_candidates_feasible(void *ctx, int n, const int32_t *x, const int32_t *z,
                                 const float *angle, int32_t *out, uint64_t *probes);
