@@ -1,25 +1,34 @@
 """Benchmark of the B200 FastRRT planner: validated plans/s and plan latency
-on batched 256x256 planning, beside the plain single-instance GPU loop.
+of served, continuously batched planning on 256x256 frames, beside the plain
+single-instance GPU loop.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl mine|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--requests R] [--slots S]
+                    [--impl mine|reference]
 
-A step plans one batch of B fresh requests (seeded 256x256 frames: road
-corridor, 12 rectangles and 6 disks of obstacles, start (128,128,0), goal
-(128,0,0), 40 deg steering, 5.4 m vehicle, 22x40 px footprint, 2 m/s, loop
-cap 200): admission (frame masks + goal direct-connection precompute),
-loop() until every request reached its goal or its loop cap, path extraction
-and validation.  Only validated plans count.
+Requests are the C0 workload: seeded 256x256 frames (road corridor, 12
+rectangles and 6 disks of obstacles, low/high-cost classes elsewhere), start
+(128,128,0), goal (128,0,0), 40 deg steering, 5.4 m vehicle, 22x40 px
+footprint, 2 m/s, 100 ms timeout per request.  A step serves R fresh
+requests through S slots with continuous batching: a request is admitted
+when a slot frees up (frame masks, deferred goal connections, start node),
+planned in the same graph launches as the others until it reaches its goal
+or its timeout, then extracted and validated on the device.  Only validated
+plans count.
 
-  value : validated plans/s with the frames already in HBM (device clock)
-  e2e   : the same through the C ABI with host frames (host -> device copies
-          of the frames and device -> host copies of the results inside)
+  value   : validated plans/s with the frames already in HBM (device clock,
+            CUDA events around each step, max over ranks)
+  e2e     : the same through the C ABI with host frames (host -> device
+            copies of the frames and device -> host copies of the results
+            inside the timed region)
+  serving : Poisson arrivals at the C3 rates; p50/p95/p99 latency from
+            arrival to finish
   cpu_baseline / --impl reference : the CPU restatement of the same planner
-          (oracle/, all host cores) on a bounded sample of the same workload
+            (oracle/, all host cores) on a bounded sample of the workload
 
-Each step uses frames never planned before, and the per-step working set
-(B x 256 x 256 cells x ~80 B of node grid and scratch) exceeds L2.
-Under torchrun, every rank plans its own requests (weak scaling, no
-collective on the data path); the time is the maximum over ranks.
+Each step plans frames never planned before; the per-step working set (S
+slots x ~6.3 MB of node grid and scratch) exceeds L2.  Under torchrun every
+rank serves its own requests (weak scaling, no collective on the data path);
+the time is the maximum over ranks.
 """
 import argparse
 import json
@@ -38,8 +47,8 @@ sys.path.insert(0, ROOT)
 
 M_PER_PX = 0.135
 SIZE = 256
-MAX_ITER = 200
-METRIC = "validated plans/s (batched 256x256 planning)"
+TIMEOUT_MS = 100
+METRIC = "validated plans/s, served + batched 256x256 planning"
 
 
 def parse():
@@ -47,7 +56,11 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--requests", type=int, default=1024, help="requests per step and GPU")
+    ap.add_argument("--slots", type=int, default=512, help="planning slots per GPU")
+    ap.add_argument("--check-every", type=int, default=2)
+    ap.add_argument("--rates", default="200,1000,5000", help="Poisson arrival rates (req/s)")
+    ap.add_argument("--rate-requests", type=int, default=600)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", type=int, default=16, help="plans of the plain single-instance loop")
@@ -158,8 +171,11 @@ class ClockSampler:
 
 
 def cpu_baseline(B_sample=None, threads=None, timeout_ms=30000):
-    """the CPU restatement of the planner (oracle/, OpenMP over plans) on a
-    bounded sample of the workload; a plan that runs past timeout_ms fails"""
+    """the CPU restatement of the planner (oracle/, OpenMP over plans, one
+    plan per thread) on a bounded sample of the workload.  The restatement
+    follows the reference's eager goal precompute (every cell of the frame,
+    seconds per frame on one core), so at the workload's 100 ms timeout no
+    CPU plan would finish; the sample runs with a 30 s cap instead."""
     from fastrrt_b200 import synth
     from oracle import oracle as O
     cores = threads or os.cpu_count() or 1
@@ -176,13 +192,13 @@ def cpu_baseline(B_sample=None, threads=None, timeout_ms=30000):
         np.stack(frames), synth.CLASS_COSTS, np.array(sg, np.int32), np.array(seeds, np.uint64),
         pw_m=SIZE * M_PER_PX, ph_m=SIZE * M_PER_PX, max_steer_deg=40.0, vehicle_len=5.4,
         min_dist=(22, 40), velocity=2.0, max_path=40.0, dist_tol=20.0,
-        heading_tol=float(np.float32(math.radians(10))), timeout_ms=timeout_ms, max_iter=MAX_ITER,
+        heading_tol=float(np.float32(math.radians(10))), timeout_ms=timeout_ms, max_iter=0,
         smart=False, threads=cores)
     wall = time.time() - t0
     return {"value": float(ok.sum()) / wall, "unit": "plans/s", "cores": cores, "kind": "port",
-            "sample": f"{n} seeded 256x256 plans (same generator and parameters, "
-                      f"{timeout_ms / 1e3:.0f} s cap per plan), {int(ok.sum())} validated, "
-                      f"{wall:.1f} s wall on {cores} threads",
+            "sample": f"{n} seeded 256x256 C0 plans (same generator and parameters; "
+                      f"{timeout_ms / 1e3:.0f} s cap per plan instead of 100 ms), "
+                      f"{int(ok.sum())} validated, {wall:.1f} s wall on {cores} threads",
             "success_rate": float(ok.mean()), "median_plan_s": float(np.median(ms) / 1e3)}
 
 
@@ -191,9 +207,9 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    per_step = max(cores, 8)
+    per_step = cores
     for _ in range(args.warmup):
-        cpu_baseline(cores, cores, timeout_ms=2000)
+        cpu_baseline(cores, cores)
     vals, walls = [], []
     for _ in range(args.steps):
         t0 = time.time()
@@ -205,17 +221,18 @@ def run_reference(args, rank, world):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * float(np.mean(walls)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"plans of seeded {SIZE}x{SIZE} frames, {per_step} per step",
+            "config": {"workload": f"C0 plans of seeded {SIZE}x{SIZE} frames, {per_step} per step",
                        "parallelism": f"{cores} host threads"},
             "cpu_baseline": {"value": value, "unit": "plans/s", "cores": cores, "kind": "port",
-                             "sample": f"{per_step} plans per step"},
+                             "sample": f"{per_step} plans per step, 30 s cap per plan"},
             "e2e": {"value": value, "unit": "plans/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def plain_loop(n, rank):
-    """the drop-in single-instance API (FastRRT loop) on n fresh frames"""
+    """the drop-in single-instance API (FastRRT + loop) on n fresh frames,
+    100 ms timeout per plan as in the workload"""
     import fastrrt_b200 as F
     from fastrrt_b200 import synth
     ok = 0
@@ -224,7 +241,12 @@ def plain_loop(n, rank):
     p = F.FastRRT(F.EgoParams.init(SIZE, SIZE).with_search_physical_size(SIZE * M_PER_PX, SIZE * M_PER_PX)
                   .with_max_steering_angle(F.angle.new_deg(40.0)).with_vehicle_length(5.4)
                   .with_segmentation_class_costs(synth.CLASS_COSTS).build(),
-                  min_dist_x=22, min_dist_z=40)
+                  min_dist_x=22, min_dist_z=40, timeout_ms=TIMEOUT_MS)
+    # one untimed plan first (library load, first launches)
+    fr = F.SearchFrame(class_ids=frames[0][0], class_costs=synth.CLASS_COSTS)
+    p.set_plan_data(fr, frames[0][1], frames[0][2], 2.0)
+    p.search_init()
+    p.loop(False)
     t0 = time.time()
     for k, (cls, st, gl) in enumerate(frames):
         t1 = time.time()
@@ -232,9 +254,7 @@ def plain_loop(n, rank):
         p.set_seed(k)
         p.set_plan_data(fr, st, gl, 2.0)
         p.search_init()
-        it = 0
-        while not p.goal_reached() and it < MAX_ITER:
-            it += 1
+        while not p.goal_reached():
             if not p.loop(False):
                 break
         path = p.get_planned_path_array()
@@ -243,8 +263,12 @@ def plain_loop(n, rank):
     wall = time.time() - t0
     return {"plans_per_s": ok / wall, "plans": n, "ok": ok,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "note": "one FastRRT object, set_plan_data + search_init + loop() per plan through the "
-                    "reference API, host wall clock"}
+            "note": "one FastRRT object, set_plan_data + search_init + loop() until the goal or "
+                    "the 100 ms timeout, per plan through the reference API, host wall clock"}
+
+
+def pct(a, q):
+    return float(np.percentile(a, q)) if len(a) else None
 
 
 def run_mine(args, rank, world, local):
@@ -254,45 +278,49 @@ def run_mine(args, rank, world, local):
     from fastrrt_b200 import synth
     F._lib.require_cuda()
     torch.cuda.set_device(local)
-    B = args.batch
+    R = args.requests
     total_steps = args.warmup + args.steps
     t_gen = time.time()
-    work = [workload(rank, s, B) for s in range(total_steps)]
+    work = [workload(rank, s, R) for s in range(total_steps)]
     gen_s = time.time() - t_gen
-    planner = F.BatchPlanner(B, SIZE, SIZE)
+    planner = F.BatchPlanner(args.slots, SIZE, SIZE)
     costs = synth.CLASS_COSTS
 
-    def requests(step, device_frames=None):
-        frames, starts, goals, seeds = work[step]
+    def requests(frames, starts, goals, seeds, device_frames=None):
         reqs = []
-        for k in range(B):
+        for k in range(len(seeds)):
             r = F.make_request(frames[k], costs, starts[k], goals[k], seed=seeds[k],
-                               max_iterations=MAX_ITER, m_per_px=M_PER_PX)
+                               m_per_px=M_PER_PX, timeout_ms=TIMEOUT_MS)
             if device_frames is not None:
                 r = F.batch.device_request(r, device_frames[k].data_ptr())
             reqs.append(r)
         return reqs
 
+    def serve(reqs, arrival=None):
+        return planner.serve(reqs, arrival_ms=arrival, timeout_ms=TIMEOUT_MS,
+                             check_every=args.check_every)
+
     # frames resident in HBM for `value`
     dev = [torch.from_numpy(work[s][0]).cuda() for s in range(total_steps)]
+    reqs_dev = [requests(*work[s], device_frames=dev[s]) for s in range(total_steps)]
     torch.cuda.synchronize()
     for s in range(args.warmup):
-        planner.plan(requests(s, dev[s]), max_launches=MAX_ITER + 8)
+        serve(reqs_dev[s])
     sampler = ClockSampler(local)
     sampler.start()
     barrier(world)
     torch.cuda.synchronize()
     dev_ms = 0.0
     valid_total = 0
-    lat = []
-    lengths = []
+    service, lengths, loops = [], [], []
     for s in range(args.warmup, total_steps):
-        reqs = requests(s, dev[s])
-        v, length, latency, ms = planner.plan(reqs, max_launches=MAX_ITER + 8)
-        dev_ms += ms
+        out = serve(reqs_dev[s])
+        dev_ms += out["device_ms"]
+        v = out["valid"] > 0
         valid_total += int(v.sum())
-        lat.extend(latency[v > 0].tolist())
-        lengths.extend(length[v > 0].tolist())
+        service.extend(out["service_ms"][v].tolist())
+        lengths.extend(out["length"][v].tolist())
+        loops.extend(out["loops"].tolist())
     torch.cuda.synchronize()
     barrier(world)
     clocks = sampler.stop()
@@ -306,24 +334,36 @@ def run_mine(args, rank, world, local):
     barrier(world)
     torch.cuda.synchronize()
     for s in range(args.warmup, total_steps):
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record()
-        reqs = requests(s)
-        v, _, _, ms = planner.plan(reqs, max_launches=MAX_ITER + 8)
-        t1.record()
-        torch.cuda.synchronize()
-        e2e_ms += max(ms, t0.elapsed_time(t1))
-        e2e_valid += int(v.sum())
+        out = serve(requests(*work[s]))
+        e2e_ms += out["device_ms"]
+        e2e_valid += int((out["valid"] > 0).sum())
     barrier(world)
     e2e_t = max_over_ranks(e2e_ms, world)
     e2e_plans = sum_over_ranks(e2e_valid, world)
-    h2d = B * (SIZE * SIZE + 4 * len(costs))
-    d2h = B * (4 * 3 + 3 * 4 * 1024 + 4 * 3)
+    h2d = R * (SIZE * SIZE + 4 * len(costs))
+    d2h = R * (4 * 5 + 3 * 4 * 1024)
+
+    # served at the C3 Poisson rates (latency from arrival to finish)
+    serving = {}
+    rng = np.random.default_rng(1234 + rank)
+    n_rate = args.rate_requests
+    rate_work = workload(rank, 10_000, n_rate)
+    rate_dev = torch.from_numpy(rate_work[0]).cuda()
+    rate_reqs = requests(*rate_work, device_frames=rate_dev)
+    for rate in [float(x) for x in args.rates.split(",") if x]:
+        arrival = np.cumsum(rng.exponential(1e3 / rate, n_rate))
+        out = serve(rate_reqs, arrival)
+        v = out["valid"] > 0
+        lat = out["latency_ms"][v]
+        serving[f"{rate:g}_req_s"] = {
+            "offered": rate, "requests": n_rate,
+            "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
+            "success_rate": float(v.mean()),
+            "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
 
     # kernel timing replay of one step (same inputs, kernels launched one by one)
     planner.profile(True)
-    planner.plan(requests(args.warmup, dev[args.warmup]), max_launches=MAX_ITER + 8)
+    serve(reqs_dev[args.warmup])
     ktimes = planner.kernel_times()
     probes = planner.probes()
     planner.profile(False)
@@ -349,17 +389,20 @@ def run_mine(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched planning, {B} requests of seeded {SIZE}x{SIZE} frames "
-                                   f"per step and GPU (loop cap {MAX_ITER})",
-                       "batch_per_gpu": B, "frame": f"{SIZE}x{SIZE} @ {M_PER_PX} m/px",
+            "config": {"workload": f"served C0 planning: {R} requests of seeded {SIZE}x{SIZE} "
+                                   f"frames per step and GPU, continuous batching over "
+                                   f"{args.slots} slots, {TIMEOUT_MS} ms timeout per request",
+                       "requests_per_step_per_gpu": R, "slots_per_gpu": args.slots,
+                       "frame": f"{SIZE}x{SIZE} @ {M_PER_PX} m/px",
                        "parallelism": f"request sharding x{world}",
                        "l2": "fresh frames every step; per-step working set > L2"},
-            "p50_ms": float(np.percentile(lat, 50)) if lat else None,
-            "p99_ms": float(np.percentile(lat, 99)) if lat else None,
-            "success_rate": valid_total / float(B * args.steps),
+            "success_rate": valid_total / float(R * args.steps),
+            "service_p50_ms": pct(service, 50), "service_p99_ms": pct(service, 99),
+            "mean_loops": float(np.mean(loops)) if loops else None,
             "mean_path_len_px": float(np.mean(lengths)) if lengths else None,
+            "serving": serving,
             "plain_gpu_loop": plain,
-            "batched_over_plain": value / plain["plans_per_s"] if plain["plans_per_s"] else None,
+            "served_over_plain": value / plain["plans_per_s"] if plain["plans_per_s"] else None,
             "e2e": {"value": e2e_plans / (e2e_t / 1e3), "unit": "plans/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(v[1] for v in ktimes.values()) * args.steps),

@@ -32,7 +32,8 @@ class Request(C.Structure):
                 ("velocity_m_s", C.c_float), ("min_dist_x", C.c_int), ("min_dist_z", C.c_int),
                 ("max_path_size", C.c_float), ("dist_to_goal_tol", C.c_float),
                 ("heading_tol_rad", C.c_float), ("seed", C.c_uint64), ("smart", C.c_int),
-                ("max_iterations", C.c_int), ("class_ids_on_device", C.c_int)]
+                ("max_iterations", C.c_int), ("class_ids_on_device", C.c_int),
+                ("timeout_ms", C.c_int)]
 
 
 EXPORTS = [
@@ -56,7 +57,7 @@ EXPORTS = [
     "fastrrt_batch_collect", "fastrrt_batch_path", "fastrrt_batch_release",
     "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
     "fastrrt_batch_kernel_times", "fastrrt_kernel_count", "fastrrt_kernel_name",
-    "fastrrt_batch_probes",
+    "fastrrt_batch_probes", "fastrrt_batch_serve",
 ]
 
 
@@ -141,6 +142,8 @@ def lib():
         "fastrrt_kernel_count": (C.c_int, []),
         "fastrrt_kernel_name": (C.c_char_p, [C.c_int]),
         "fastrrt_batch_probes": (C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+        "fastrrt_batch_serve": (C.c_int, [vp, C.c_int, P(Request), vp, C.c_int, C.c_int, i32p, f32p,
+                                          f32p, f32p, i32p, P(C.c_double), P(C.c_float)]),
     }
     for name in EXPORTS:
         fn = getattr(L, name)

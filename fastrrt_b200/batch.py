@@ -11,7 +11,7 @@ def make_request(cls, class_costs, start, goal, *, perception_m=None, m_per_px=0
                  max_steering_deg=40.0, vehicle_length_m=5.4, max_curvature=-1.0,
                  velocity_m_s=2.0, min_dist=(22, 40), max_path_size=40.0, dist_to_goal_tol=20.0,
                  heading_tol_rad=None, seed=0, smart=False, max_iterations=0,
-                 lower_bound=(-1, -1), upper_bound=(-1, -1)):
+                 lower_bound=(-1, -1), upper_bound=(-1, -1), timeout_ms=0):
     """A fastrrt_request; the returned object keeps its arrays alive."""
     cls = np.ascontiguousarray(cls, np.uint8)
     costs = np.ascontiguousarray(class_costs, np.float32)
@@ -42,6 +42,7 @@ def make_request(cls, class_costs, start, goal, *, perception_m=None, m_per_px=0
     r.smart = int(bool(smart))
     r.max_iterations = int(max_iterations)
     r.class_ids_on_device = 0
+    r.timeout_ms = int(timeout_ms)
     r._keep = (cls, costs)
     return r
 
@@ -124,6 +125,29 @@ class BatchPlanner:
         _lib.check(_lib.lib().fastrrt_batch_plan(self._h, n, arr, max_launches, check_every, valid,
                                                  length, lat, _lib.C.byref(dev)), "batch_plan")
         return valid, length, lat, dev.value
+
+    def serve(self, requests, arrival_ms=None, timeout_ms=100, check_every=2):
+        """Continuous batching over `requests` (admitted as they arrive and
+        slots free up); returns a dict of per-request arrays (valid, length,
+        latency_ms from arrival, service_ms from admission, loops) and the
+        wall and device (CUDA event) time of the call in ms."""
+        n = len(requests)
+        arr = (_lib.Request * n)(*requests) if n else None
+        out = {"valid": np.zeros(n, np.int32), "length": np.zeros(n, np.float32),
+               "latency_ms": np.zeros(n, np.float32), "service_ms": np.zeros(n, np.float32),
+               "loops": np.zeros(n, np.int32)}
+        arrival = None
+        if arrival_ms is not None:
+            arrival = np.ascontiguousarray(arrival_ms, np.float64)
+        wall = _lib.C.c_double(0)
+        dev = _lib.C.c_float(0)
+        _lib.check(_lib.lib().fastrrt_batch_serve(
+            self._h, n, arr, None if arrival is None else arrival.ctypes.data, int(timeout_ms),
+            int(check_every), out["valid"], out["length"], out["latency_ms"], out["service_ms"],
+            out["loops"], _lib.C.byref(wall), _lib.C.byref(dev)), "batch_serve")
+        out["wall_ms"] = wall.value
+        out["device_ms"] = dev.value
+        return out
 
     def profile(self, on=True):
         _lib.check(_lib.lib().fastrrt_batch_profile(self._h, int(on)), "batch_profile")

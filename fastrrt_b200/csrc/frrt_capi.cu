@@ -1,7 +1,9 @@
 // frrt_capi.cu -- extern "C" ABI of libfastrrt_b200.so (include/fastrrt_b200.h).
 #include "fastrrt_b200.h"
 
+#include <algorithm>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -109,7 +111,7 @@ struct Batch {
     }
 };
 
-bool load_request(Engine &e, int slot, const fastrrt_request &r)
+bool load_request(Engine &e, int slot, const fastrrt_request &r, int timeout_ms = 0)
 {
     Physical ph{};
     ph.pw_m = r.perception_w_m;
@@ -139,6 +141,7 @@ bool load_request(Engine &e, int slot, const fastrrt_request &r)
     q.smart = r.smart;
     q.max_iter = r.max_iterations;
     q.stop_on_goal = 1;
+    q.timeout_ms = r.timeout_ms > 0 ? r.timeout_ms : timeout_ms;
     e.set_request(slot, q);
     return e.copy_frame(slot, r.width, r.height, r.class_ids, r.class_costs, r.n_classes,
                         r.class_ids_on_device != 0);
@@ -792,17 +795,12 @@ int fastrrt_batch_admit_many(void *batch, int n, const fastrrt_request *reqs, in
     Engine &e = *b->eng;
     std::vector<int> slots;
     for (int k = 0; k < n; k++) {
-        if (!load_request(e, k, reqs[k]))
+        if (!load_request(e, k, reqs[k], timeout_ms))
             return -1;
         slots.push_back(k);
     }
-    if (!e.prepare(slots, 0.8f) || !e.search_init(slots, true) || !e.sync())
+    if (!e.prepare(slots, 0.8f, true) || !e.search_init(slots, true) || !e.sync())
         return -1;
-    if (timeout_ms > 0) {
-        // deadlines on the device clock, read by the iteration's last kernel
-        for (int s : slots)
-            e.set_deadline(s, 0);
-    }
     b->admitted = slots;
     return 0;
 }
@@ -814,9 +812,8 @@ int fastrrt_batch_admit(void *batch, int slot, const fastrrt_request *req, int t
         set_error("batch admit: bad arguments");
         return -1;
     }
-    (void)timeout_ms;
     Engine &e = *b->eng;
-    if (!load_request(e, slot, *req) || !e.prepare({slot}, 0.8f) || !e.search_init({slot}, true) ||
+    if (!load_request(e, slot, *req, timeout_ms) || !e.prepare({slot}, 0.8f, true) || !e.search_init({slot}, true) ||
         !e.sync())
         return -1;
     return 0;
@@ -957,7 +954,7 @@ int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_
     for (int s = n; s < e.n_slots(); s++)
         if (e.state(s).active)
             e.deactivate(s);
-    const bool adm = e.prepare(slots, 0.8f) && e.search_init(slots, true);
+    const bool adm = e.prepare(slots, 0.8f, true) && e.search_init(slots, true);
     cudaEventRecord(e_adm, e.stream());
     if (!adm) {
         cudaEventDestroy(e_adm);
@@ -1008,6 +1005,127 @@ int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_
             latency_ms[k] = adm_ms + (float)((fin - S.start_ns) * 1e-6);
         }
     }
+    return good;
+}
+
+int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const double *arrival_ms,
+                        int timeout_ms, int check_every, int32_t *valid, float *length,
+                        float *latency_ms, float *service_ms, int32_t *loops, double *wall_ms,
+                        float *device_ms)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || n < 0 || (n > 0 && !reqs)) {
+        set_error("batch serve: bad arguments");
+        return -1;
+    }
+    if (arrival_ms)
+        for (int k = 0; k < n; k++)
+            if (!(arrival_ms[k] >= 0.0) || (k > 0 && arrival_ms[k] < arrival_ms[k - 1])) {
+                set_error("batch serve: arrival times must be finite, >= 0 and non-decreasing");
+                return -1;
+            }
+    Engine &e = *b->eng;
+    const int n_slots = e.n_slots();
+    if (check_every <= 0)
+        check_every = 1;
+    // slots left live by an earlier call take no part
+    if (!e.fetch_states(true))
+        return -1;
+    for (int s = 0; s < n_slots; s++)
+        if (e.state(s).active && !e.state(s).done && !e.deactivate(s))
+            return -1;
+    // device clock -> host clock: one read bracketed by host reads
+    long long dev0 = 0;
+    const double ha = now_ms();
+    if (!e.device_clock(dev0))
+        return -1;
+    const double host_at_dev0 = 0.5 * (ha + now_ms());
+    const double t0 = now_ms();
+    cudaEventRecord(b->ev0, e.stream());
+    auto finish_ms = [&](long long ns) { return host_at_dev0 + (double)(ns - dev0) * 1e-6 - t0; };
+
+    std::vector<int> free_slots, owner(n_slots, -1), list;
+    for (int s = n_slots - 1; s >= 0; s--)
+        free_slots.push_back(s);
+    std::vector<double> admitted_at(n, 0.0);
+    int next = 0, finished = 0, in_flight = 0, good = 0;
+    while (finished < n) {
+        // admit every request that has arrived while a slot is free
+        const double now = now_ms() - t0;
+        list.clear();
+        while (next < n && !free_slots.empty() && (!arrival_ms || arrival_ms[next] <= now)) {
+            const int s = free_slots.back();
+            free_slots.pop_back();
+            if (!load_request(e, s, reqs[next], timeout_ms))
+                return -1;
+            owner[s] = next;
+            admitted_at[next] = now;
+            list.push_back(s);
+            next++;
+        }
+        if (!list.empty()) {
+            if (!e.prepare(list, 0.8f, true) || !e.search_init(list, true))
+                return -1;
+            in_flight += (int)list.size();
+        }
+        if (in_flight == 0) {
+            if (!arrival_ms || next >= n) {
+                set_error("batch serve: no free slot");
+                return -1;
+            }
+            // nothing on the GPU: wait for the next arrival
+            const double wait = arrival_ms[next] - (now_ms() - t0);
+            if (wait > 0)
+                std::this_thread::sleep_for(std::chrono::microseconds(
+                    (long long)std::min(wait * 1000.0, 200.0)));
+            continue;
+        }
+        for (int k = 0; k < check_every; k++)
+            if (!e.iterate())
+                return -1;
+        if (!e.fetch_states(true))
+            return -1;
+        // harvest finished slots and free them
+        list.clear();
+        for (int s = 0; s < n_slots; s++)
+            if (owner[s] >= 0 && e.state(s).done)
+                list.push_back(s);
+        if (list.empty())
+            continue;
+        if (!e.extract_and_validate(list, 1024))
+            return -1;
+        for (size_t k = 0; k < list.size(); k++) {
+            const int s = list[k];
+            const int r = owner[s];
+            const State &S = e.state(s);
+            const int v = e.valid()[k] && S.goal_reached;
+            good += v;
+            const double fin = finish_ms(S.finish_ns);
+            if (valid)
+                valid[r] = v;
+            if (length)
+                length[r] = e.lengths()[k];
+            if (latency_ms)
+                latency_ms[r] = (float)(fin - (arrival_ms ? arrival_ms[r] : 0.0));
+            if (service_ms)
+                service_ms[r] = (float)(fin - admitted_at[r]);
+            if (loops)
+                loops[r] = S.loops;
+            owner[s] = -1;
+            free_slots.push_back(s);
+            in_flight--;
+            finished++;
+        }
+    }
+    cudaEventRecord(b->ev1, e.stream());
+    cudaEventSynchronize(b->ev1);
+    if (wall_ms)
+        *wall_ms = now_ms() - t0;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->last_ms = ms;
+    if (device_ms)
+        *device_ms = ms;
     return good;
 }
 

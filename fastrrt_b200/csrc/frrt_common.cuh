@@ -10,8 +10,9 @@
 //           first covers the cell
 //   memo_*  goal-search result of a node, keyed by its heading and cost bits
 // Frame of one instance: class ids (u8), a bit-packed obstacle mask
-// (class cost < 0) and a bit-packed "clear" mask (no obstacle within the
-// footprint's circumscribed square), optional traversability bits (int32).
+// (class cost < 0), a bit-packed "clear" mask (no obstacle within the
+// footprint's circumscribed square), a summed-area table of the obstacle mask
+// (u16) for footprint bounding-box tests, optional traversability bits (int32).
 // Masks are row-padded: row z starts at word z * mask_rw, pixel x is bit
 // (x & 31) of word (x >> 5).
 #pragma once
@@ -52,6 +53,8 @@ struct Inst {
     const uint32_t *blocked;   // bit i: class cost of pixel i < 0
     const uint32_t *clear;     // bit i: no blocked pixel within Chebyshev radius rc
     const int32_t *trav;       // traversability bits or nullptr
+    const uint16_t *sat;       // (W+1) x (H+1) summed-area table of the obstacle
+                               // mask, counts mod 2^16, or nullptr
     int mask_rw;               // words per mask row = ceil(W / 32)
     int mask_words;            // words per mask, padded to a multiple of 4
     // node grid
@@ -107,6 +110,7 @@ struct Inst {
     int smart;
     int max_iter;              // 0 = unlimited
     int stop_on_goal;          // batched planning stops a slot at its goal
+    long long timeout_ns;      // > 0: deadline after search_init (device clock)
 };
 
 // Mutable per-instance state.

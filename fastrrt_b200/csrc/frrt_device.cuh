@@ -79,6 +79,7 @@ struct Foot {
     const uint32_t *blocked;
     const uint32_t *clear;
     const int32_t *trav;
+    const uint16_t *sat;   // obstacle counts, summed-area table mod 2^16, or nullptr
 };
 
 __device__ __forceinline__ Foot foot_of(const Inst &I, const uint32_t *blocked, const uint32_t *clear)
@@ -88,12 +89,51 @@ __device__ __forceinline__ Foot foot_of(const Inst &I, const uint32_t *blocked, 
     f.lbx = I.lbx; f.lbz = I.lbz; f.ubx = I.ubx; f.ubz = I.ubz;
     f.rw = I.mask_rw;
     f.blocked = blocked; f.clear = clear; f.trav = I.trav;
+    // a box count is exact mod 2^16 only while the box holds fewer cells
+    f.sat = (I.mdx + I.mdz <= 120) ? I.sat : nullptr;
     return f;
 }
+
+
 
 __device__ __forceinline__ unsigned full_probes(const Foot &f)
 {
     return (unsigned)((2 * f.mdx + 1) * (2 * f.mdz + 1));
+}
+
+// No obstacle in the box [x0, x1] x [z0, z1] (clipped to the frame), from the
+// summed-area table: S[z][x] = obstacles in [0, x) x [0, z), (W+1) columns.
+__device__ __forceinline__ bool box_clear(const Foot &f, int x0, int z0, int x1, int z1)
+{
+    x0 = max(x0, 0);
+    z0 = max(z0, 0);
+    x1 = min(x1, f.W - 1);
+    z1 = min(z1, f.H - 1);
+    if (x0 > x1 || z0 > z1)
+        return true;
+    const long w = f.W + 1;
+    const uint16_t a = f.sat[(z1 + 1) * w + x1 + 1], b = f.sat[(long)z0 * w + x1 + 1];
+    const uint16_t c = f.sat[(z1 + 1) * w + x0], d = f.sat[(long)z0 * w + x0];
+    return (uint16_t)(a - b - c + d) == 0;
+}
+
+// The footprint at heading direction (|cos|, |sin|) = (ac, as) probes only
+// cells within its axis-aligned bounding box: offsets j c - i s and j s + i c
+// with |j| <= mdx, |i| <= mdz, truncated toward zero, plus one cell for the
+// truncation and the rounding of the reference's cosf / sinf.  An empty box
+// means every probe misses, so the footprint is feasible and the reference
+// runs all its probes.
+__device__ __forceinline__ bool box_feasible(const Foot &f, int x, int z, float ac, float as,
+                                             unsigned long long &probes)
+{
+    if (!f.sat || !(ac <= 1.5f) || !(as <= 1.5f))
+        return false;
+    const int ex = (int)ceilf(f.mdx * ac + f.mdz * as + 1e-3f) + 1;
+    const int ez = (int)ceilf(f.mdx * as + f.mdz * ac + 1e-3f) + 1;
+    if (!box_clear(f, x - ex, z - ez, x + ex, z + ez))
+        return false;
+    probes += full_probes(f);
+    return true;
 }
 
 // 1: feasible without probing (isAllAngleFeasible quirk or clear shortcut),
@@ -256,6 +296,15 @@ struct KinTask {
                 last_z = lpz;
                 continue;
             }
+            if (f.sat) {
+                float sn, cs;
+                sincosf(heading, &sn, &cs);
+                if (box_feasible(f, lpx, lpz, fabsf(cs), fabsf(sn), probes)) {
+                    last_x = lpx;
+                    last_z = lpz;
+                    continue;
+                }
+            }
             pend_x = lpx;
             pend_z = lpz;
             return 1;
@@ -284,6 +333,8 @@ struct HermTask {
     float distance, t1x, t1y, t2x, t2y, nodeCost, max_curvature, pend_heading;
     int safe, ok;
     const float *intrinsic;
+    double inv_span;           // RN(1 / (numPoints - 1))
+    double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-6))^2
 
     __device__ void init(const Inst &I, const Foot &f, float max_curv, int x_, int z_,
                          float local_heading, int gx, int gz, float goal_heading, int safe_zone,
@@ -312,6 +363,11 @@ struct HermTask {
         last_z = -1;
         nodeCost = start_cost;
         trav = f.trav ? f.trav[pos] : 0;
+        inv_span = 1.0 / (double)(numPoints - 1);
+        const double khi = (double)max_curvature * (1.0 + 1e-6);
+        const double klo = (double)max_curvature * (1.0 - 1e-6);
+        kap_hi2 = khi * khi;
+        kap_lo2 = klo * klo;
         safe = safe_zone;
         i = 0;
         ok = 0;
@@ -319,8 +375,16 @@ struct HermTask {
 
     __device__ int advance(const Foot &f, unsigned long long &probes)
     {
+        const double span = (double)(numPoints - 1);
         for (; i < numPoints; ++i) {
-            const double t = ((double)0.0 + i) / (numPoints - 1);
+            // t = i / (numPoints - 1), correctly rounded, without a division
+            // per sample: with y = RN(1/b), q = RN(a y) and the exact
+            // remainder r = a - q b, RN(q + r y) is RN(a/b) (Markstein 1990);
+            // checked exhaustively for 0 <= a <= b <= 16384 against IEEE
+            // division, which covers every frame up to 4096 x 4096
+            const double ai = (double)i;
+            const double q = __dmul_rn(ai, inv_span);
+            const double t = __fma_rn(__fma_rn(-q, span, ai), inv_span, q);
             const double t2 = t * t;
             const double t3 = t2 * t;
             const double h00 = 2 * t3 - 3 * t2 + 1;
@@ -348,23 +412,27 @@ struct HermTask {
             const double t11 = 3 * t2 - 2 * t;
             const double ddx = t00 * x + t10 * t1x + t01 * goal_x + t11 * t2x;
             const double ddz = t00 * z + t10 * t1y + t01 * goal_z + t11 * t2y;
-            const float heading = atan2f(ddz, ddx) + kHalfPi;
             const double d00 = 12 * t - 6;
             const double d10 = 6 * t - 4;
             const double d01 = -12 * t + 6;
             const double d11 = 6 * t - 2;
             const double dd2x = d00 * x + d10 * t1x + d01 * goal_x + d11 * t2x;
             const double dd2z = d00 * z + d10 * t1y + d01 * goal_z + d11 * t2y;
+            const double s2 = ddx * ddx + ddz * ddz;
             if (max_curvature > 0) {
                 const double num = fabs(ddx * dd2z - ddz * dd2x);
-                const double s2 = ddx * ddx + ddz * ddz;
-                // s2 * sqrt(s2) is within a few ulp of pow(s2, 1.5); pow only
-                // decides cases inside a 1e-6 guard band around the limit
-                const double kf = num / (s2 * sqrt(s2));
+                // The reference tests (float)(num / pow(s2, 1.5)) > limit.
+                // Outside a 1e-6 relative band around the limit the answer
+                // follows from num^2 against limit^2 s2^3 (products rounded
+                // to ~1e-15); pow only decides cases inside the band.
+                // s2 == 0: num > 0 is over (num / 0 = inf), num == 0 falls
+                // through to the reference's own 0 / 0.
+                const double n2 = num * num;
+                const double s6 = s2 * s2 * s2;
                 bool over;
-                if (kf > (double)max_curvature * (1.0 + 1e-6))
+                if (n2 > kap_hi2 * s6)
                     over = true;
-                else if (kf < (double)max_curvature * (1.0 - 1e-6))
+                else if (n2 < kap_lo2 * s6)
                     over = false;
                 else {
                     const float k = num / pow(s2, 1.5);
@@ -382,7 +450,16 @@ struct HermTask {
                 continue;
             if (quick_feasible(f, last_x, last_z, probes))
                 continue;
-            pend_heading = heading;
+            // heading = atan2(ddz, ddx) + pi/2, so |cos| = |ddz| / |d| and
+            // |sin| = |ddx| / |d|
+            if (f.sat && s2 > 0.0) {
+                const float inv = rsqrtf((float)s2);
+                if (box_feasible(f, last_x, last_z, fabsf((float)ddz) * inv, fabsf((float)ddx) * inv,
+                                 probes))
+                    continue;
+            }
+            // the heading is only needed to probe the footprint
+            pend_heading = atan2f(ddz, ddx) + kHalfPi;
             ++i;
             return 1;
         }

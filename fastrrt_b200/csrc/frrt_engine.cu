@@ -148,6 +148,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         4 * (size_t)mask_words_,            // 24 clear-mask scratch
         C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
         8 * C, 8 * C, 4 * C, 4 * C,         // 27 memo key, 28 best, 29 cell, 30 seg
+        2 * (size_t)(max_w + 1) * (max_h + 1),  // 31 obstacle summed-area table
     };
     constexpr int kParts = sizeof(parts) / sizeof(parts[0]);
     size_t per_slot = 0;
@@ -205,6 +206,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         I.memo_best = (long long *)ptr[28];
         I.memo_cell = (int32_t *)ptr[29];
         I.memo_seg = (float *)ptr[30];
+        I.sat = (const uint16_t *)ptr[31];
         I.lbx = I.lbz = I.ubx = I.ubz = -1;
         I.stop_on_goal = 1;
         if (!check(cudaMemsetAsync(I.claim, 0x7F, 4 * C, stream_), "claim init"))
@@ -220,6 +222,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMalloc(&d_slots_, sizeof(int) * n_slots), "slot list") &&
               check(cudaMalloc(&d_class_costs_, sizeof(float) * kMaxClasses * n_slots), "class costs") &&
               check(cudaMalloc(&d_bad_, sizeof(int)), "flag") &&
+              check(cudaMalloc(&d_clock_, sizeof(long long)), "clock") &&
               check(cudaMallocHost(&h_small_, sizeof(int) * 64), "pinned scratch") &&
               check(cudaMalloc(&d_newcost_, sizeof(float) * kOptCap * kOptCap), "optimize scratch") &&
               check(cudaMalloc(&d_changed_, sizeof(int)), "optimize flag") &&
@@ -265,6 +268,7 @@ Engine::~Engine()
     cudaFree(d_slots_);
     cudaFree(d_class_costs_);
     cudaFree(d_bad_);
+    cudaFree(d_clock_);
     if (h_small_)
         cudaFreeHost(h_small_);
     cudaFree(d_paths_);
@@ -371,15 +375,8 @@ void Engine::set_request(int slot, const PlanRequest &r)
     I.smart = r.smart;
     I.max_iter = r.max_iter;
     I.stop_on_goal = r.stop_on_goal;
+    I.timeout_ns = r.timeout_ms > 0 ? (long long)r.timeout_ms * 1000000LL : 0;
     dirty_ = true;
-}
-
-void Engine::set_deadline(int slot, long long deadline_ns)
-{
-    h_state_[slot].deadline_ns = deadline_ns;
-    cudaMemcpyAsync(&d_state_[slot].deadline_ns, &deadline_ns, sizeof(long long),
-                    cudaMemcpyHostToDevice, stream_);
-    cudaStreamSynchronize(stream_);
 }
 
 bool Engine::set_intrinsic(int slot, const float *host_costs)
@@ -448,7 +445,7 @@ bool Engine::upload_slots_list(const std::vector<int> &slots)
                  "slot list upload");
 }
 
-bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
+bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature, bool fresh)
 {
     for (int sl : slots) {
         if (h_inst_[sl].gd_max_curvature != direct_max_curvature) {
@@ -462,7 +459,7 @@ bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
         return true;
     if (!check(cudaMemsetAsync(d_bad_, 0, sizeof(int), stream_), "flag reset"))
         return false;
-    int max_cells = 0, max_words = 0;
+    int max_cells = 0, max_words = 0, max_w = 0, max_h = 0;
     for (int s : slots) {
         const Inst &I = h_inst_[s];
         if (I.W <= 0) {
@@ -471,14 +468,16 @@ bool Engine::prepare(const std::vector<int> &slots, float direct_max_curvature)
         }
         max_cells = std::max(max_cells, I.W * I.H);
         max_words = std::max(max_words, I.mask_rw * I.H);
+        max_w = std::max(max_w, I.W);
+        max_h = std::max(max_h, I.H);
     }
     if (!upload_slots_list(slots))
         return false;
     launch_frame_masks(d_inst_, d_state_, d_slots_, (int)slots.size(), max_words, kMaxClasses, d_bad_,
-                       stream_);
+                       stream_, max_w, max_h);
     if (profiling_)
         cudaEventRecord(prof_ev_[kIterKernels + 1], stream_);
-    launch_direct_goal_reset(d_inst_, d_slots_, (int)slots.size(), max_cells, stream_);
+    launch_direct_goal_reset(d_inst_, d_slots_, (int)slots.size(), max_cells, fresh ? 1 : 0, stream_);
     if (profiling_) {
         cudaEventRecord(prof_ev_[kIterKernels + 2], stream_);
         float ms = 0;
@@ -760,6 +759,16 @@ bool Engine::grid_upload(int slot, const std::vector<int8_t> &type, const std::v
     if (ok)
         ok = set_intrinsic(slot, any_intr ? intrinsic.data() : nullptr);
     return ok && commit();
+}
+
+bool Engine::device_clock(long long &ns)
+{
+    launch_clock(d_clock_, stream_);
+    return check(cudaGetLastError(), "clock launch") &&
+           check(cudaMemcpyAsync(&h_small_[2], d_clock_, sizeof(long long), cudaMemcpyDeviceToHost,
+                                 stream_),
+                 "clock read") &&
+           sync() && (memcpy(&ns, &h_small_[2], sizeof(long long)), true);
 }
 
 bool Engine::gd_complete(int slot)

@@ -52,6 +52,7 @@ struct PlanRequest {
     int smart;
     int max_iter;
     int stop_on_goal;
+    int timeout_ms;   // > 0: the slot stops this long after search_init (device clock)
 };
 
 struct Physical {
@@ -81,13 +82,16 @@ public:
     bool copy_frame(int slot, int W, int H, const uint8_t *cls, const float *costs_host,
                     int n_classes, bool cls_on_device = false);
     void set_request(int slot, const PlanRequest &r);
-    void set_deadline(int slot, long long deadline_ns);
     // intrinsic costs: nullptr keeps them zero (the planner's default)
     bool set_intrinsic(int slot, const float *host_costs);
     bool commit();  // upload Inst table + scheduling tables
 
     // set_plan_data for listed slots: masks + goal direct-connection precompute
-    bool prepare(const std::vector<int> &slots, float direct_max_curvature = 0.8f);
+    // frame masks and the reset of the goal direct connections; `fresh` (a
+    // new request in a slot) takes the curves' start costs from a newly
+    // constructed planner (zero) instead of the slot's current grid
+    bool prepare(const std::vector<int> &slots, float direct_max_curvature = 0.8f,
+                 bool fresh = false);
     // search_init for listed slots
     // fresh = a new request: the slot starts like a newly constructed planner
     bool search_init(const std::vector<int> &slots, bool fresh);
@@ -120,6 +124,8 @@ public:
                      const std::vector<int32_t> &child, const std::vector<float> &heading,
                      const std::vector<float> &cost, const std::vector<float> &intrinsic,
                      const std::vector<float> &direct);
+    // device clock (ns) read now; the stream is synchronised
+    bool device_clock(long long &ns);
     // evaluates every goal direct connection of the slot still unknown
     bool gd_complete(int slot);
     bool gd_download(int slot, std::vector<uint8_t> &flag, std::vector<float> &heading,
@@ -186,6 +192,7 @@ private:
     float *d_newcost_ = nullptr;
     int *d_changed_ = nullptr;
     int *h_small_ = nullptr;          // pinned scratch
+    long long *d_clock_ = nullptr;    // device clock read-out
     std::vector<int> h_path_n_, h_valid_;
     std::vector<float> h_length_, h_paths_;
     bool profiling_ = false;

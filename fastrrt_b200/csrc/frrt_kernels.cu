@@ -200,8 +200,55 @@ __global__ void k_clear(const Inst *insts, const int *slots)
     }
 }
 
+// summed-area table of the obstacle mask, pass 1: prefix counts along each
+// row (row 0 and column 0 are zero)
+__global__ void k_sat_rows(const Inst *insts, const int *slots)
+{
+    const Inst &I = insts[slots[blockIdx.y]];
+    if (!I.sat)
+        return;
+    uint16_t *S = const_cast<uint16_t *>(I.sat);
+    const int w = I.W + 1;
+    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z <= I.H; z += gridDim.x * blockDim.x) {
+        uint16_t *row = S + (long)z * w;
+        row[0] = 0;
+        if (z == 0) {
+            for (int x = 1; x < w; x++)
+                row[x] = 0;
+            continue;
+        }
+        const uint32_t *m = I.blocked + (long)(z - 1) * I.mask_rw;
+        uint16_t run = 0;
+        for (int q = 0; q < I.mask_rw; q++) {
+            const uint32_t bits = m[q];
+            const int n = min(32, I.W - q * 32);
+            for (int b = 0; b < n; b++) {
+                run = (uint16_t)(run + ((bits >> b) & 1u));
+                row[q * 32 + b + 1] = run;
+            }
+        }
+    }
+}
+
+// pass 2: prefix down each column
+__global__ void k_sat_cols(const Inst *insts, const int *slots)
+{
+    const Inst &I = insts[slots[blockIdx.y]];
+    if (!I.sat)
+        return;
+    uint16_t *S = const_cast<uint16_t *>(I.sat);
+    const int w = I.W + 1;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < w; x += gridDim.x * blockDim.x) {
+        uint16_t run = 0;
+        for (int z = 1; z <= I.H; z++) {
+            run = (uint16_t)(run + S[(long)z * w + x]);
+            S[(long)z * w + x] = run;
+        }
+    }
+}
+
 void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_words,
-                        int ncls_max, int *d_bad_class, cudaStream_t st)
+                        int ncls_max, int *d_bad_class, cudaStream_t st, int max_w, int max_h)
 {
     if (n <= 0)
         return;
@@ -210,6 +257,10 @@ void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, 
     k_blocked<<<grid, 256, 0, st>>>(d_inst, d_state, d_slots, d_bad_class);
     k_rowdil<<<grid, 256, 0, st>>>(d_inst, d_slots);
     k_clear<<<grid, 256, 0, st>>>(d_inst, d_slots);
+    if (max_w > 0 && max_h > 0) {
+        k_sat_rows<<<dim3((max_h + 1 + 127) / 128, n), 128, 0, st>>>(d_inst, d_slots);
+        k_sat_cols<<<dim3((max_w + 1 + 127) / 128, n), 128, 0, st>>>(d_inst, d_slots);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -228,7 +279,7 @@ struct PrecompTask {
 // of a node it searches, so each cell is evaluated the first time such a
 // window covers it, with the same function and arguments as the eager pass
 // (graph_direct_goal_connection.cu:169-227).
-__global__ void k_gd_reset(const Inst *insts, const int *slots)
+__global__ void k_gd_reset(const Inst *insts, const int *slots, int fresh)
 {
     const Inst &I = insts[slots[blockIdx.y]];
     const long cells = (long)I.W * I.H;
@@ -241,11 +292,12 @@ __global__ void k_gd_reset(const Inst *insts, const int *slots)
         for (int q = 0; q < 16; q += 2)
             *reinterpret_cast<int4 *>(I.memo_key + base + q) = ones;
         // the eager pass starts each curve from the cell's graph cost at
-        // set_plan_data time: keep it until the cell is evaluated
+        // set_plan_data time (zero in a newly constructed planner): keep it
+        // until the cell is evaluated
 #pragma unroll
         for (int q = 0; q < 16; q += 4)
             *reinterpret_cast<int4 *>(I.gd_cost + base + q) =
-                *reinterpret_cast<const int4 *>(I.cost + base + q);
+                fresh ? make_int4(0, 0, 0, 0) : *reinterpret_cast<const int4 *>(I.cost + base + q);
     }
     for (long w = (long)blockIdx.x * blockDim.x + threadIdx.x; w < words;
          w += (long)gridDim.x * blockDim.x)
@@ -253,12 +305,12 @@ __global__ void k_gd_reset(const Inst *insts, const int *slots)
 }
 
 void launch_direct_goal_reset(const Inst *d_inst, const int *d_slots, int n, int max_cells,
-                              cudaStream_t st)
+                              int fresh, cudaStream_t st)
 {
     if (n <= 0)
         return;
     const int bx = (max_cells / 16 + 255) / 256;
-    k_gd_reset<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots);
+    k_gd_reset<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots, fresh);
 }
 
 // Evaluates the goal direct connection of cells: listed ones (list mode, one
@@ -384,6 +436,7 @@ __global__ void k_init_state(const Inst *insts, State *states, const int *slots,
     S.probes_goal = 0;
     S.start_ns = global_ns();
     S.finish_ns = 0;
+    S.deadline_ns = I.timeout_ns > 0 ? S.start_ns + I.timeout_ns : 0;
     if (reset_regions)
         for (int r = 0; r < kMaxRegions; r++)
             I.region_count[r] = 0;
@@ -913,41 +966,32 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
     }
 }
 
-__global__ void __launch_bounds__(256) k_gd_eval(const Inst *insts, State *states, Sched *sc,
-                                                 int smem_words)
+// One warp per chunk of kGdChunk listed cells, grabbed by each warp on its
+// own (curve lengths differ a lot); masks are read through L1.
+__global__ void __launch_bounds__(256) k_gd_eval(const Inst *insts, State *states, Sched *sc)
 {
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_chunk;
     const int n = sc->n_slots;
     const int total = sc->gd_start[n];
-    Stage sg{-1, false, 0u};
-    if (threadIdx.x == 0)
-        mbar_init(&bar, 1);
-    __syncthreads();
+    const int lane = threadIdx.x & 31;
     while (true) {
-        if (threadIdx.x == 0)
-            s_chunk = (int)atomicAdd(&sc->grab[2], 1u);
-        __syncthreads();
-        const int c = s_chunk;
-        __syncthreads();
+        int c = 0;
+        if (lane == 0)
+            c = (int)atomicAdd(&sc->grab[2], 1u);
+        c = __shfl_sync(kFull, c, 0);
         if (c >= total)
             break;
         const int slot = find_slot(sc->gd_start, n, c);
         const Inst &I = insts[slot];
         State &S = states[slot];
-        const uint32_t *blk, *clr;
-        stage_for(I, slot, sg, smem, smem_words, &bar, states, blk, clr);
-        const Foot f = foot_of(I, blk, clr);
-        const int idx = (c - sc->gd_start[slot]) * kGdChunk + threadIdx.x;
+        const Foot f = foot_of(I, I.blocked, I.clear);
+        const int idx = (c - sc->gd_start[slot]) * kGdChunk + lane;
         const bool has = idx < S.n_gd;
         unsigned long long probes = 0;
         gd_eval_cell(I, f, has, has ? I.gd_list[idx] : 0, probes);
         probes = warp_sum64(probes);
-        if ((threadIdx.x & 31) == 0 && probes)
+        if (lane == 0 && probes)
             atomicAdd(&S.probes_pre, probes);
     }
-    stage_drain(sg, &bar);
 }
 
 // best connection of one graph node to a precomputed goal-connected cell in
@@ -1022,34 +1066,27 @@ struct GoalLane {
     __device__ float probe_angle() const { return h.pend_heading; }
 };
 
-__global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, Sched *sc,
-                                              int smem_words)
+// One warp per listed node, grabbed one at a time by each warp: window
+// searches differ a lot in length, so no block-wide step holds warps back.
+// Masks are read through L1 (the slots of one launch are many).
+__global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, Sched *sc)
 {
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_chunk;
     const int n = sc->n_slots;
-    const int total = sc->node_start[n];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    Stage sg{-1, false, 0u};
-    if (threadIdx.x == 0)
-        mbar_init(&bar, 1);
-    __syncthreads();
+    const int total = sc->node_start[n] * kNodeChunk;
+    const int lane = threadIdx.x & 31;
     while (true) {
-        if (threadIdx.x == 0)
-            s_chunk = (int)atomicAdd(&sc->grab[1], 1u);
-        __syncthreads();
-        const int c = s_chunk;
-        __syncthreads();
-        if (c >= total)
+        int g = 0;
+        if (lane == 0)
+            g = (int)atomicAdd(&sc->grab[1], 1u);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= total)
             break;
+        const int c = g / kNodeChunk;
         const int slot = find_slot(sc->node_start, n, c);
         const Inst &I = insts[slot];
         State &S = states[slot];
-        const uint32_t *blk, *clr;
-        stage_for(I, slot, sg, smem, smem_words, &bar, states, blk, clr);
-        const Foot f = foot_of(I, blk, clr);
-        const int idx = (c - sc->node_start[slot]) * kNodeChunk + warp;
+        const Foot f = foot_of(I, I.blocked, I.clear);
+        const int idx = (c - sc->node_start[slot]) * kNodeChunk + (g - c * kNodeChunk);
         const bool has = idx < S.n_nodes;  // uniform across the warp
         unsigned long long probes = 0;
         if (has) {
@@ -1121,7 +1158,6 @@ __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, 
         if (lane == 0 && probes)
             atomicAdd(&S.probes_goal, probes);
     }
-    stage_drain(sg, &bar);
 }
 
 // among listed nodes with the minimum, the highest node cell index wins
@@ -1245,9 +1281,9 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 2);
     mark();
-    k_gd_eval<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    k_gd_eval<<<L.sms * kWarpGrabBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
-    k_goal<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    k_goal<<<L.sms * kWarpGrabBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_select<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
@@ -1825,11 +1861,14 @@ __global__ void k_feasible(const Inst *insts, int slot, int n, const int32_t *x,
         atomicAdd(probes_out, pr);
 }
 
+// the device clock that the state timestamps use (%globaltimer, ns)
+__global__ void k_clock(long long *out) { *out = global_ns(); }
+
+void launch_clock(long long *d_out, cudaStream_t st) { k_clock<<<1, 1, 0, st>>>(d_out); }
+
 void configure_kernels(int smem_bytes)
 {
     cudaFuncSetAttribute(k_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-    cudaFuncSetAttribute(k_goal, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-    cudaFuncSetAttribute(k_gd_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_candidates, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_hermite, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
 }

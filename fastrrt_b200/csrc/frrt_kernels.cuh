@@ -10,7 +10,8 @@ namespace frrt {
 constexpr int kSweepCells = 4096;   // cells per sweep chunk (256 threads x 16)
 constexpr int kCandChunk = 256;     // candidates per expansion chunk (one per thread)
 constexpr int kNodeChunk = 8;       // listed nodes per goal-search chunk (one per warp)
-constexpr int kGdChunk = 256;       // listed cells per direct-connection chunk (one per thread)
+constexpr int kGdChunk = 32;        // listed cells per direct-connection chunk (one per lane)
+constexpr int kWarpGrabBlocks = 2;  // blocks per SM of the warp-grab kernels
 constexpr int32_t kClaimFree = 0x7F7F7F7F;
 
 // Scheduling tables shared by the iteration kernels (device memory).
@@ -31,17 +32,23 @@ struct Launch {
     int smem_words;           // words per mask staged in shared memory (0 = global masks)
 };
 
+// writes the device clock of the state timestamps (ns) to *d_out
+void launch_clock(long long *d_out, cudaStream_t st);
+
 // allows `smem_bytes` of dynamic shared memory on the mask-staging kernels
 void configure_kernels(int smem_bytes);
 
-// frame preparation for listed slots: obstacle and clear masks
+// frame preparation for listed slots: obstacle and clear masks, and the
+// obstacle summed-area table of slots that have one (max_w / max_h bound the
+// listed frames; 0 skips the table)
 void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_words,
-                        int ncls_max, int *d_bad_class, cudaStream_t st);
+                        int ncls_max, int *d_bad_class, cudaStream_t st, int max_w = 0,
+                        int max_h = 0);
 // processDirectGoalConnection for the n listed slots, deferred: marks every
 // cell's goal direct connection as not evaluated; the iterations evaluate
 // the cells that goal-search windows reach
 void launch_direct_goal_reset(const Inst *d_inst, const int *d_slots, int n, int max_cells,
-                              cudaStream_t st);
+                              int fresh, cudaStream_t st);
 // evaluates every cell of the listed slots whose goal direct connection is
 // still unknown
 void launch_direct_goal_complete(const Inst *d_inst, State *d_state, const int *d_slots, int n,

@@ -183,6 +183,8 @@ typedef struct {
     int smart;
     int max_iterations;        /* 0 = unlimited */
     int class_ids_on_device;   /* class_ids points to device memory */
+    int timeout_ms;            /* > 0: the request fails this long after it starts
+                                  planning (device clock); 0 = the call's timeout */
 } fastrrt_request;
 
 void *fastrrt_batch_create(int n_slots, int max_width, int max_height);
@@ -216,6 +218,21 @@ float fastrrt_batch_last_ms(void *batch);
 int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_launches,
                        int check_every, int32_t *valid, float *length, float *latency_ms,
                        float *device_ms);
+/* Served planning with continuous batching.  Request k arrives arrival_ms[k]
+ * milliseconds after the call starts (NULL: all at once; non-decreasing). It
+ * is admitted as soon as it has arrived and a slot is free, is planned in the
+ * same graph launches as whatever else is in flight, and its slot is refilled
+ * as soon as it finishes: goal reached, loop cap, or timeout_ms after it
+ * started planning (device clock; a request's own timeout_ms wins).  Per
+ * request (any output may be NULL): valid, coarse path length, latency from
+ * arrival and from admission to finish (ms, host clock), loops run.
+ * *wall_ms = the whole call on the host clock, *device_ms = the same span
+ * between CUDA events on the planner's stream.  Returns the number of
+ * validated plans. */
+int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const double *arrival_ms,
+                        int timeout_ms, int check_every, int32_t *valid, float *length,
+                        float *latency_ms, float *service_ms, int32_t *loops, double *wall_ms,
+                        float *device_ms);
 /* kernel timing mode (1 = on): iterations launch kernels one by one between
  * CUDA events instead of replaying the CUDA graph */
 int fastrrt_batch_profile(void *batch, int on);

@@ -877,19 +877,30 @@ void orc_graph_process_direct_goal(orc_graph *g, const orc_frame *f, const orc_s
 {
     if (max_curvature < 0)
         max_curvature = (float)g->pp.max_curvature;
-    for (int z = 0; z < g->H; z++)
+    long long total = 0;
+    /* cells are independent; rows run in parallel when this is the outermost
+     * parallel region (inside orc_plan_batch's per-plan threads it is serial) */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
+#endif
+    for (int z = 0; z < g->H; z++) {
+        long long pr = 0;
         for (int x = 0; x < g->W; x++) {
             const long pos = (long)z * g->W + x;
             g->gd_flag[pos] = 0;
             const float lh = (float)orc_compute_heading(x, z, goal_x, goal_z);
             const float c = orc_direct_connection(g, f, fsp, max_curvature, x, z, lh,
-                                                  goal_x, goal_z, goal_heading, 0, probes);
+                                                  goal_x, goal_z, goal_heading, 0, &pr);
             if (c < 0)
                 continue;
             g->gd_flag[pos] = 1.0f;
             g->gd_heading[pos] = lh;
             g->gd_cost[pos] = c;
         }
+        total += pr;
+    }
+    if (probes)
+        *probes += total;
 }
 
 /* findBestGoalDirectConnection (graph_check_goal_reached.cu:17-188).  The
@@ -1469,7 +1480,7 @@ int orc_plan_batch(int n, int W, int H, const uint8_t *cls, const float *class_c
         orc_planner_set_plan_data(p, &f, &pp, min_dist_x, min_dist_z);
         orc_planner_search_init(p);
         int it = 0;
-        while (!orc_planner_goal_reached(p) && it < max_iter) {
+        while (!orc_planner_goal_reached(p) && (max_iter <= 0 || it < max_iter)) {
             if (timeout_ms > 0 && now_ms() - t0 > timeout_ms)
                 break;
             it++;

@@ -240,3 +240,44 @@ def test_batch_plan_validates_every_path(gpu, orc):
         op = orc.Planner(orc.Frame(cls, COSTS), 34.56, 34.56, 40.0, 5.4)
         op.set_plan_data(start, goal, 2.0, (22, 40), seed=k)
         assert op.validate_waypoints(B.path(k)), k
+
+
+def test_served_same_alone_and_in_the_mix(gpu):
+    """Continuous batching: requests of mixed sizes (60% 256², 30% 128², 10%
+    512²) arrive as a Poisson stream, are admitted as slots free up and
+    overlap on the device; each result (validity, loops, path length) is the
+    one the request gives served alone.  A loop cap instead of a timeout
+    keeps the comparison independent of timing."""
+    rng = np.random.default_rng(7)
+    n = 24
+    reqs = []
+    for s in range(n):
+        size = int(rng.choice([256, 128, 512], p=[0.6, 0.3, 0.1]))
+        cls, start, goal, steer, _ = synth.batch_request(2000 + s, sizes=(size,))
+        reqs.append(gpu.make_request(cls, COSTS, start, goal, max_steering_deg=steer, seed=s,
+                                     max_iterations=60))
+    arrival = np.cumsum(rng.exponential(0.5, n))
+    B = gpu.BatchPlanner(8, 512, 512)
+    mix = B.serve(reqs, arrival_ms=arrival, timeout_ms=0, check_every=2)
+    assert mix["wall_ms"] > 0 and mix["device_ms"] > 0
+    assert np.all(mix["latency_ms"] >= mix["service_ms"] - 1e-3)
+    A = gpu.BatchPlanner(1, 512, 512)
+    for k in range(n):
+        one = A.serve([reqs[k]], timeout_ms=0, check_every=2)
+        got = (int(mix["valid"][k]), int(mix["loops"][k]), float(mix["length"][k]))
+        assert got == (int(one["valid"][0]), int(one["loops"][0]), float(one["length"][0])), k
+    assert mix["valid"].sum() >= 1
+
+
+def test_served_timeout(gpu):
+    """A request whose planning runs past its timeout finishes unsolved."""
+    cls, start, goal = synth.c0_request(3)
+    far = gpu.make_request(cls, COSTS, start, goal, seed=3, timeout_ms=1)
+    B = gpu.BatchPlanner(2, W, H)
+    out = B.serve([far], timeout_ms=1, check_every=1)
+    # a 1 ms budget may or may not suffice for one loop; a finished request
+    # either validated its path or stopped at the deadline
+    assert out["loops"][0] >= 1
+    ok = gpu.make_request(cls, COSTS, start, goal, seed=3)
+    out = B.serve([ok], timeout_ms=100, check_every=1)
+    assert out["valid"][0] == 1
