@@ -221,6 +221,58 @@ __device__ inline bool probe_warp(const Foot &f, int x, int z, float angle, int 
     return true;
 }
 
+// A cheaper exact test than the full probe loop, for footprints that turn
+// out feasible.  Every probe (j, i) of the footprint at (x, z) with direction
+// (c, s) lies in the rectangle |u| <= mdx, |v| <= mdz, with u = X' c + Z' s,
+// v = -X' s + Z' c relative to the cell.  A probe in frame row zr has
+// Z' in [zr - z, zr - z + 1] (row 0 also takes Z' in (-1, 0): truncation
+// toward zero), and over that strip each constraint bounds X' by an interval
+// whose ends move linearly, so their hulls bound every probe of the row.
+// Lane k tests rows z0 + k, z0 + k + 32, ... with one cell of margin each
+// side; no obstacle bit in any interval means no probe can hit.
+__device__ inline bool rows_clear_warp(const Foot &f, int x, int z, float c, float s, int lane)
+{
+    const float ac = fabsf(c), as = fabsf(s);
+    const float ez = f.mdx * as + f.mdz * ac;
+    const int z0 = max(0, (int)floorf(z - ez) - 1);
+    const int z1 = min(f.H - 1, (int)floorf(z + ez) + 1);
+    bool hit = false;
+    for (int zr = z0 + lane; zr <= z1 && !hit; zr += 32) {
+        const float za = (float)(zr - z) - (zr == 0 ? 1.001f : 0.001f);
+        const float zb = (float)(zr - z + 1) + 0.001f;
+        float lo = -1e30f, hi = 1e30f;
+        if (ac > 1e-6f) {
+            const float a0 = (-f.mdx - za * s) / c, a1 = (f.mdx - za * s) / c;
+            const float b0 = (-f.mdx - zb * s) / c, b1 = (f.mdx - zb * s) / c;
+            lo = fmaxf(lo, fminf(fminf(a0, a1), fminf(b0, b1)));
+            hi = fminf(hi, fmaxf(fmaxf(a0, a1), fmaxf(b0, b1)));
+        }
+        if (as > 1e-6f) {
+            const float a0 = (za * c - f.mdz) / s, a1 = (za * c + f.mdz) / s;
+            const float b0 = (zb * c - f.mdz) / s, b1 = (zb * c + f.mdz) / s;
+            lo = fmaxf(lo, fminf(fminf(a0, a1), fminf(b0, b1)));
+            hi = fminf(hi, fmaxf(fmaxf(a0, a1), fmaxf(b0, b1)));
+        }
+        if (!(lo <= hi))
+            continue;
+        const int xa = max(0, (int)floorf(x + lo) - 1);
+        const int xb = min(f.W - 1, (int)floorf(x + hi) + 1);
+        if (xa > xb)
+            continue;
+        const uint32_t *row = f.blocked + (long)zr * f.rw;
+        for (int q = xa >> 5; q <= (xb >> 5); q++) {
+            const int b0 = max(xa - q * 32, 0), b1 = min(xb - q * 32, 31);
+            const uint32_t mask =
+                (b1 - b0 == 31) ? 0xffffffffu : (((1u << (b1 - b0 + 1)) - 1u) << b0);
+            if (row[q] & mask) {
+                hit = true;
+                break;
+            }
+        }
+    }
+    return !__any_sync(kFull, hit);
+}
+
 // ---------------------------------------------------------------------------
 // resumable per-lane tasks: advance() runs until a footprint needs a full
 // probe (returns 1) or the task ends (returns 0); resolve() consumes the
@@ -509,7 +561,13 @@ __device__ void run_warp(Task &t, bool has, const Foot &f, unsigned long long &p
             const int bz = __shfl_sync(kFull, pz(t), leader);
             const float ba = __shfl_sync(kFull, t.probe_angle(), leader);
             unsigned cnt = 0;
-            const bool ok = probe_warp(f, bx, bz, ba, lane, cnt);
+            bool ok;
+            if (rows_clear_warp(f, bx, bz, cosf(ba), sinf(ba), lane)) {
+                ok = true;  // feasible: the reference runs all its probes
+                cnt = full_probes(f);
+            } else {
+                ok = probe_warp(f, bx, bz, ba, lane, cnt);
+            }
             if (lane == leader) {
                 mine = ok;
                 probes += cnt;
