@@ -36,6 +36,7 @@ constexpr int kFrontierThreshold = 100;  // fastrrt.cpp:116
 constexpr long long kBigCost = 99999999999LL;
 constexpr uint8_t kGdUnknown = 0xFF;  // gd_flag of a cell not evaluated yet
 constexpr unsigned long long kMemoNone = ~0ull;  // memo_key of a cell without a result
+constexpr unsigned long long kNoConnection = ~0ull;  // node_key without a connection
 constexpr unsigned kFull = 0xffffffffu;
 
 __host__ __device__ inline int32_t pack_xz(int x, int z)
@@ -73,10 +74,8 @@ struct Inst {
     // goal search of a node is a pure function of (cell, heading, cost) for a
     // fixed frame, goal and intrinsic costs: results of complete (unpruned)
     // searches are kept per cell and reused while the node keeps that key
-    unsigned long long *memo_key;  // (heading bits << 32) | cost bits, or kMemoNone
-    long long *memo_best;
-    int32_t *memo_cell;
-    float *memo_seg;
+    unsigned long long *memo_key;     // (heading bits << 32) | cost bits, or kMemoNone
+    unsigned long long *memo_result;  // the search's result key (see node_key)
     // per-iteration scratch
     int32_t *claim;
     int32_t *cand;
@@ -84,9 +83,12 @@ struct Inst {
     float *cand_heading;
     float *cand_cost;
     int32_t *nodes;
-    long long *node_best;      // per listed node: best floor(100 * total)
-    int32_t *node_best_cell;
-    float *node_best_seg;      // per listed node: node -> cell segment cost
+    // per listed node: best connection as (floor(100 * total) << 32) |
+    // (0xffffffff - cell), so the minimum is the cheapest, ties to the highest
+    // cell; kNoConnection when none
+    unsigned long long *node_key;
+    int32_t *node_pending;     // window chunks of the node not searched yet
+    int32_t *node_pruned;      // a chunk skipped cells by the bound
     unsigned *region_count;    // [kMaxRegions] density used by the gate
     unsigned *region_new;      // [kMaxRegions] density counted after this expansion
     uint32_t *rowdil;          // mask scratch of the clear-mask dilation
@@ -101,6 +103,7 @@ struct Inst {
     double lr;                 // vehicle length / 2 (m)
     float max_curvature;       // PHYSICAL_MAX_CURVATURE as float
     float gd_max_curvature;    // curvature limit of the goal direct connections
+    int win_chunks;            // 32-cell chunks covering a node's goal-search window
     float velocity, max_path, dist_tol, heading_tol;
     int start_x, start_z;
     float start_heading;

@@ -139,7 +139,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         C, 4 * C, 4 * C,                    // 7 gd flag, 8 heading, 9 cost
         4 * C,                              // 10 claim
         4 * C, 4 * C, 4 * C, 4 * C,         // 11 cand, 12 end, 13 heading, 14 cost
-        4 * C, 8 * C, 4 * C, 4 * C,         // 15 nodes, 16 best, 17 cell, 18 seg
+        4 * C, 8 * C, 4 * C, 4 * C,         // 15 nodes, 16 best key, 17 pending, 18 pruned
         C,                                  // 19 own class ids
         4 * (size_t)mask_words_,            // 20 blocked
         4 * (size_t)mask_words_,            // 21 clear
@@ -147,8 +147,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         4 * (size_t)kMaxRegions,            // 23 region_new
         4 * (size_t)mask_words_,            // 24 clear-mask scratch
         C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
-        8 * C, 8 * C, 4 * C, 4 * C,         // 27 memo key, 28 best, 29 cell, 30 seg
-        2 * (size_t)(max_w + 1) * (max_h + 1),  // 31 obstacle summed-area table
+        8 * C, 8 * C,                       // 27 memo key, 28 memo result
+        2 * (size_t)(max_w + 1) * (max_h + 1),  // 29 obstacle summed-area table
     };
     constexpr int kParts = sizeof(parts) / sizeof(parts[0]);
     size_t per_slot = 0;
@@ -190,9 +190,9 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         I.cand_heading = (float *)ptr[13];
         I.cand_cost = (float *)ptr[14];
         I.nodes = (int32_t *)ptr[15];
-        I.node_best = (long long *)ptr[16];
-        I.node_best_cell = (int32_t *)ptr[17];
-        I.node_best_seg = (float *)ptr[18];
+        I.node_key = (unsigned long long *)ptr[16];
+        I.node_pending = (int32_t *)ptr[17];
+        I.node_pruned = (int32_t *)ptr[18];
         own_cls_[s] = (uint8_t *)ptr[19];
         I.cls = own_cls_[s];
         I.blocked = (const uint32_t *)ptr[20];
@@ -203,10 +203,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         I.gd_req = (uint32_t *)ptr[25];
         I.gd_list = (int32_t *)ptr[26];
         I.memo_key = (unsigned long long *)ptr[27];
-        I.memo_best = (long long *)ptr[28];
-        I.memo_cell = (int32_t *)ptr[29];
-        I.memo_seg = (float *)ptr[30];
-        I.sat = (const uint16_t *)ptr[31];
+        I.memo_result = (unsigned long long *)ptr[28];
+        I.sat = (const uint16_t *)ptr[29];
         I.lbx = I.lbz = I.ubx = I.ubz = -1;
         I.stop_on_goal = 1;
         if (!check(cudaMemsetAsync(I.claim, 0x7F, 4 * C, stream_), "claim init"))
@@ -217,7 +215,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMemsetAsync(d_state_, 0, sizeof(State) * n_slots, stream_), "state init") &&
               check(cudaMallocHost(&h_state_, sizeof(State) * n_slots), "pinned state") &&
               check(cudaMalloc(&d_sched_, sizeof(Sched)), "sched") &&
-              check(cudaMalloc(&d_sched_arrays_, sizeof(int) * 4 * (n_slots + 1)), "sched arrays") &&
+              check(cudaMalloc(&d_sched_arrays_, sizeof(int) * 5 * (n_slots + 1)), "sched arrays") &&
               check(cudaMalloc(&d_grab_, sizeof(unsigned) * 4), "grab counters") &&
               check(cudaMalloc(&d_slots_, sizeof(int) * n_slots), "slot list") &&
               check(cudaMalloc(&d_class_costs_, sizeof(float) * kMaxClasses * n_slots), "class costs") &&
@@ -226,7 +224,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMallocHost(&h_small_, sizeof(int) * 64), "pinned scratch") &&
               check(cudaMalloc(&d_newcost_, sizeof(float) * kOptCap * kOptCap), "optimize scratch") &&
               check(cudaMalloc(&d_changed_, sizeof(int)), "optimize flag") &&
-              check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 4 * (n_slots + 1), stream_), "sched init") &&
+              check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 5 * (n_slots + 1), stream_), "sched init") &&
               check(cudaMemsetAsync(d_grab_, 0, sizeof(unsigned) * 4, stream_), "grab init") &&
               check(cudaMemsetAsync(d_class_costs_, 0, sizeof(float) * kMaxClasses * n_slots, stream_), "costs init");
     if (!ok)
@@ -376,6 +374,9 @@ void Engine::set_request(int slot, const PlanRequest &r)
     I.max_iter = r.max_iter;
     I.stop_on_goal = r.stop_on_goal;
     I.timeout_ns = r.timeout_ms > 0 ? (long long)r.timeout_ms * 1000000LL : 0;
+    // a window spans at most (int)(2 r) + 2 cells per axis
+    const long wmax = (long)(2.0f * r.dist_tol) + 2;
+    I.win_chunks = (int)std::max(1L, (wmax * wmax + 31) / 32);
     dirty_ = true;
 }
 
@@ -401,7 +402,7 @@ bool Engine::commit()
                                cudaMemcpyHostToDevice, stream_),
                "inst upload"))
         return false;
-    std::vector<int> arrays(4 * (n_slots_ + 1), 0);
+    std::vector<int> arrays(5 * (n_slots_ + 1), 0);
     int run = 0;
     for (int s = 0; s < n_slots_; s++) {
         arrays[s] = run;
@@ -415,6 +416,7 @@ bool Engine::commit()
     h_sched_.cand_start = d_sched_arrays_ + (n_slots_ + 1);
     h_sched_.node_start = d_sched_arrays_ + 2 * (n_slots_ + 1);
     h_sched_.gd_start = d_sched_arrays_ + 3 * (n_slots_ + 1);
+    h_sched_.goal_start = d_sched_arrays_ + 4 * (n_slots_ + 1);
     h_sched_.grab = d_grab_;
     const int sweep_blocks = std::max(1, std::min(L_.sms * 8, run));
     if (sweep_blocks != L_.sweep_blocks) {

@@ -510,33 +510,41 @@ __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, 
 }
 
 // prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
-// work chunks of one slot: 0 candidates, 1 listed nodes, 2 listed cells
-__device__ __forceinline__ int chunks_of(const State &S, int which)
+// work units of one slot: 0 candidate chunks, 1 listed-node chunks, 2
+// listed-cell chunks, 3 (listed node, window chunk) pairs
+__device__ __forceinline__ long long chunks_of(const Inst &I, const State &S, int which)
 {
-    return which == 0 ? (S.n_cand + kCandChunk - 1) / kCandChunk
-           : which == 1 ? (S.n_nodes + kNodeChunk - 1) / kNodeChunk
-                        : (S.n_gd + kGdChunk - 1) / kGdChunk;
+    switch (which) {
+    case 0: return (S.n_cand + kCandChunk - 1) / kCandChunk;
+    case 1: return (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
+    case 2: return (S.n_gd + kGdChunk - 1) / kGdChunk;
+    default: return (long long)S.n_nodes * I.win_chunks;
+    }
 }
 
-__global__ void __launch_bounds__(1024) k_plan(const State *states, Sched *sc, int which)
+__global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states, Sched *sc,
+                                              int which)
 {
-    __shared__ int warp_tot[32];
+    __shared__ long long warp_tot[32];
     const int n = sc->n_slots;
-    int *out = which == 0 ? sc->cand_start : which == 1 ? sc->node_start : sc->gd_start;
+    int *out = which == 0   ? sc->cand_start
+               : which == 1 ? sc->node_start
+               : which == 2 ? sc->gd_start
+                            : sc->goal_start;
     const int per = (n + blockDim.x - 1) / blockDim.x;
     const int s0 = threadIdx.x * per;
-    int local = 0;
+    long long local = 0;
     for (int s = s0; s < s0 + per && s < n; s++) {
         const State &S = states[s];
         if (!live(S))
             continue;
-        local += chunks_of(S, which);
+        local += chunks_of(insts[s], S, which);
     }
     // block exclusive scan of `local`
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int incl = local;
+    long long incl = local;
     for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(kFull, incl, o);
+        const long long v = __shfl_up_sync(kFull, incl, o);
         if (lane >= o)
             incl += v;
     }
@@ -544,24 +552,30 @@ __global__ void __launch_bounds__(1024) k_plan(const State *states, Sched *sc, i
         warp_tot[wid] = incl;
     __syncthreads();
     if (wid == 0) {
-        int v = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        long long v = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
         for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(kFull, v, o);
+            const long long u = __shfl_up_sync(kFull, v, o);
             if (lane >= o)
                 v += u;
         }
         warp_tot[lane] = v;
     }
     __syncthreads();
-    int run = incl - local + (wid ? warp_tot[wid - 1] : 0);
+    // the work counters are 32-bit: a pass beyond 2^31 units is refused
+    // (state error 2 on every live slot) instead of wrapping
+    const bool fits = warp_tot[(blockDim.x >> 5) - 1] <= 0x7fffffffLL;
+    long long run = incl - local + (wid ? warp_tot[wid - 1] : 0);
     for (int s = s0; s < s0 + per && s < n; s++) {
-        out[s] = run;
-        const State &S = states[s];
-        if (live(S))
-            run += chunks_of(S, which);
+        out[s] = fits ? (int)run : 0;
+        State &S = states[s];
+        if (live(S)) {
+            run += chunks_of(insts[s], S, which);
+            if (!fits)
+                S.error = 2;
+        }
     }
     if (threadIdx.x == blockDim.x - 1)
-        out[n] = run;
+        out[n] = fits ? (int)run : 0;
     if (threadIdx.x == 0)
         sc->grab[which] = 0;
 }
@@ -884,7 +898,7 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
                 if (t[k] != T_NODE)
                     continue;
                 const int pos = base + k;
-                if (I.memo_key[pos] == memo_key_of(I, pos) && I.memo_best[pos] >= kBigCost) {
+                if (I.memo_key[pos] == memo_key_of(I, pos) && I.memo_result[pos] == kNoConnection) {
                     // searched before with this heading and cost and no
                     // connection found: only the goal check remains
                     goal_check_node(I, S, pos);
@@ -896,8 +910,12 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
                 *reinterpret_cast<int4 *>(I.type + base) = v;
         }
         const int at = warp_append(&S.n_nodes, cnt);
-        for (int k = 0; k < cnt; k++)
+        for (int k = 0; k < cnt; k++) {
             I.nodes[at + k] = mine[k];
+            I.node_key[at + k] = kNoConnection;
+            I.node_pending[at + k] = I.win_chunks;
+            I.node_pruned[at + k] = 0;
+        }
         temps = warp_sum(temps);
         all = warp_sum(all);
         if ((threadIdx.x & 31) == 0) {
@@ -999,14 +1017,13 @@ __global__ void __launch_bounds__(256) k_gd_eval(const Inst *insts, State *state
 // the node (graph_best_node.cu:181-222)
 struct GoalLane {
     HermTask h;
-    int w, wtotal, nx, zlo, xlo;
+    int w, wend, nx, zlo, xlo;
     bool in_task;
     int x, z;
     float heading, cost, gd_cost_cur;
     int cell_cur;
     long long best;
     int best_cell;
-    float best_seg;
     const Inst *I;
     const volatile long long *global_best;
     bool prune;
@@ -1016,7 +1033,7 @@ struct GoalLane {
     {
         while (true) {
             if (!in_task) {
-                if (w >= wtotal)
+                if (w >= wend)
                     return 0;
                 const int zp = zlo + w / nx, xp = xlo + w % nx;
                 w += 32;
@@ -1025,7 +1042,7 @@ struct GoalLane {
                 if (xp < 0 || xp >= I->W)
                     continue;
                 const int cell = zp * I->W + xp;
-                if (!(I->gd_flag[cell] > 0))
+                if (!(I->gd_flag[cell] == 1))
                     continue;
                 const float gdc = I->gd_cost[cell];
                 if (prune) {
@@ -1046,13 +1063,11 @@ struct GoalLane {
                 return 1;
             in_task = false;
             if (h.ok) {
-                const float c = h.nodeCost;
-                const float total = c + gd_cost_cur;
+                const float total = h.nodeCost + gd_cost_cur;
                 const long long lc = __float2ll_rd(100 * total);
                 if (lc <= best) {
                     best = lc;
                     best_cell = cell_cur;
-                    best_seg = c;
                 }
             }
         }
@@ -1066,97 +1081,98 @@ struct GoalLane {
     __device__ float probe_angle() const { return h.pend_heading; }
 };
 
-// One warp per listed node, grabbed one at a time by each warp: window
-// searches differ a lot in length, so no block-wide step holds warps back.
-// Masks are read through L1 (the slots of one launch are many).
+__device__ __forceinline__ unsigned long long connection_key(long long lc, int cell)
+{
+    return ((unsigned long long)lc << 32) | (unsigned long long)(0xffffffffu - (unsigned)cell);
+}
+
+// Goal search, one warp per (listed node, 32-cell chunk of its window), each
+// warp grabbing units on its own: a node's window is spread over many warps,
+// so a few nodes with busy windows do not hold a launch back.  The last
+// chunk of a node to finish keeps the node's result when no chunk skipped a
+// cell by the bound.  Masks are read through L1.
 __global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, Sched *sc)
 {
     const int n = sc->n_slots;
-    const int total = sc->node_start[n] * kNodeChunk;
+    const int total = sc->goal_start[n];
     const int lane = threadIdx.x & 31;
     while (true) {
         int g = 0;
         if (lane == 0)
-            g = (int)atomicAdd(&sc->grab[1], 1u);
+            g = (int)atomicAdd(&sc->grab[3], 1u);
         g = __shfl_sync(kFull, g, 0);
         if (g >= total)
             break;
-        const int c = g / kNodeChunk;
-        const int slot = find_slot(sc->node_start, n, c);
+        const int slot = find_slot(sc->goal_start, n, g);
         const Inst &I = insts[slot];
         State &S = states[slot];
-        const Foot f = foot_of(I, I.blocked, I.clear);
-        const int idx = (c - sc->node_start[slot]) * kNodeChunk + (g - c * kNodeChunk);
-        const bool has = idx < S.n_nodes;  // uniform across the warp
-        unsigned long long probes = 0;
-        if (has) {
-            const int pos = I.nodes[idx];
-            if (lane == 0)
+        const int local = g - sc->goal_start[slot];
+        const int idx = local / I.win_chunks;
+        const int wc = local - idx * I.win_chunks;
+        const int pos = I.nodes[idx];
+        const unsigned long long key = memo_key_of(I, pos);
+        if (I.memo_key[pos] == key) {
+            // a complete search with this heading and cost was kept
+            if (wc == 0 && lane == 0) {
                 goal_check_node(I, S, pos);
-            const unsigned long long key = memo_key_of(I, pos);
-            if (I.memo_key[pos] == key) {
-                // a complete search with this heading and cost was kept
-                if (lane == 0) {
-                    const long long b = I.memo_best[pos];
-                    I.node_best[idx] = b;
-                    I.node_best_cell[idx] = I.memo_cell[pos];
-                    I.node_best_seg[idx] = I.memo_seg[pos];
-                    if (b < kBigCost)
-                        atomicMin(&S.best, b);
-                }
-                continue;
+                const unsigned long long r = I.memo_result[pos];
+                I.node_key[idx] = r;
+                if (r != kNoConnection)
+                    atomicMin(&S.best, (long long)(r >> 32));
             }
-            GoalLane g;
-            g.I = &I;
-            g.z = pos / I.W;
-            g.x = pos - g.z * I.W;
-            g.heading = I.heading[pos];
-            g.cost = I.cost[pos];
-            const int nz = window_count(g.z, I.dist_tol, g.zlo);
-            g.nx = window_count(g.x, I.dist_tol, g.xlo);
-            g.wtotal = g.nx > 0 ? nz * g.nx : 0;
-            g.w = lane;
-            g.in_task = false;
-            g.best = kBigCost;
-            g.best_cell = -1;
-            g.best_seg = 0.0f;
-            g.global_best = &S.best;
-            g.prune = I.intrinsic == nullptr;
-            g.pruned = false;
-            run_warp(g, true, f, probes, [](const GoalLane &q) { return q.h.last_x; },
-                     [](const GoalLane &q) { return q.h.last_z; });
-            // warp minimum of best, ties to the highest cell index
-            long long b = g.best;
-            int bc = g.best_cell;
-            float bs = g.best_seg;
-            for (int o = 16; o; o >>= 1) {
-                const long long ob = __shfl_xor_sync(kFull, b, o);
-                const int oc = __shfl_xor_sync(kFull, bc, o);
-                const float os = __shfl_xor_sync(kFull, bs, o);
-                if (ob < b || (ob == b && oc > bc)) {
-                    b = ob;
-                    bc = oc;
-                    bs = os;
-                }
+            continue;
+        }
+        if (wc == 0 && lane == 0)
+            goal_check_node(I, S, pos);
+        const Foot f = foot_of(I, I.blocked, I.clear);
+        GoalLane gl;
+        gl.I = &I;
+        gl.z = pos / I.W;
+        gl.x = pos - gl.z * I.W;
+        gl.heading = I.heading[pos];
+        gl.cost = I.cost[pos];
+        const int nz = window_count(gl.z, I.dist_tol, gl.zlo);
+        gl.nx = window_count(gl.x, I.dist_tol, gl.xlo);
+        const int wtotal = gl.nx > 0 ? nz * gl.nx : 0;
+        gl.w = wc * 32 + lane;
+        gl.wend = min(wtotal, (wc + 1) * 32);
+        gl.in_task = false;
+        gl.best = kBigCost;
+        gl.best_cell = -1;
+        gl.global_best = &S.best;
+        gl.prune = I.intrinsic == nullptr;
+        gl.pruned = false;
+        unsigned long long probes = 0;
+        run_warp(gl, true, f, probes, [](const GoalLane &q) { return q.h.last_x; },
+                 [](const GoalLane &q) { return q.h.last_z; });
+        // warp minimum, ties to the highest cell index
+        unsigned long long k = gl.best < kBigCost ? connection_key(gl.best, gl.best_cell) : kNoConnection;
+        for (int o = 16; o; o >>= 1) {
+            const unsigned long long ok = __shfl_xor_sync(kFull, k, o);
+            k = ok < k ? ok : k;
+        }
+        const bool pruned = __any_sync(kFull, gl.pruned);
+        probes = warp_sum64(probes);
+        if (lane == 0) {
+            if (probes)
+                atomicAdd(&S.probes_goal, probes);
+            if (k != kNoConnection) {
+                atomicMin(&I.node_key[idx], k);
+                atomicMin(&S.best, (long long)(k >> 32));
             }
-            const bool complete = !__any_sync(kFull, g.pruned);
-            if (lane == 0) {
-                I.node_best[idx] = b;
-                I.node_best_cell[idx] = bc;
-                I.node_best_seg[idx] = bs;
-                if (b < kBigCost)
-                    atomicMin(&S.best, b);
-                if (complete) {
-                    I.memo_best[pos] = b;
-                    I.memo_cell[pos] = bc;
-                    I.memo_seg[pos] = bs;
+            if (pruned)
+                atomicOr(&I.node_pruned[idx], 1);
+            __threadfence();
+            if (atomicSub(&I.node_pending[idx], 1) == 1) {
+                // every chunk of the node is done
+                __threadfence();
+                const unsigned long long r = atomicAdd(&I.node_key[idx], 0ull);
+                if (!atomicAdd(&I.node_pruned[idx], 0)) {
+                    I.memo_result[pos] = r;
                     I.memo_key[pos] = key;
                 }
             }
         }
-        probes = warp_sum64(probes);
-        if (lane == 0 && probes)
-            atomicAdd(&S.probes_goal, probes);
     }
 }
 
@@ -1174,7 +1190,8 @@ __global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states
         const int idx = (chunk - sc->node_start[slot]) * kNodeChunk + (int)(e % kNodeChunk);
         if (idx >= S.n_nodes || S.best >= kBigCost)
             continue;
-        if (I.node_best[idx] == S.best) {
+        const unsigned long long nk = I.node_key[idx];
+        if (nk != kNoConnection && (long long)(nk >> 32) == S.best) {
             const unsigned long long key =
                 ((unsigned long long)(unsigned)I.nodes[idx] << 32) | (unsigned)idx;
             atomicMax(&S.winner, key);
@@ -1182,16 +1199,53 @@ __global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states
     }
 }
 
-// the host-side tail of FastRRT::loop, per slot
+struct SegLane {
+    HermTask h;
+    __device__ int advance(const Foot &f, unsigned long long &p) { return h.advance(f, p); }
+    __device__ bool resolve(bool ok) { return h.resolve(ok); }
+    __device__ float probe_angle() const { return h.pend_heading; }
+};
+
+// The cost of the curve from node ppos to the goal-connected cell, as the goal
+// search computed it: the same task, on lane 0 of the calling warp, with the
+// warp's help for full footprint probes (graph_direct_goal_connection.cu:
+// 16-167 from the node).  Every lane of the warp calls it.
+__device__ float connection_segment_cost(const Inst &I, int ppos, int cell, int lane)
+{
+    const Foot f = foot_of(I, I.blocked, I.clear);
+    const int pz = ppos / I.W, px = ppos - pz * I.W;
+    const int cz = cell / I.W, cx = cell - cz * I.W;
+    SegLane t;
+    if (lane == 0)
+        t.h.init(I, f, I.max_curvature, px, pz, I.heading[ppos], cx, cz, I.gd_heading[cell], 1,
+                 I.cost[ppos]);
+    unsigned long long unused = 0;
+    run_warp(t, lane == 0, f, unused, [](const SegLane &q) { return q.h.last_x; },
+             [](const SegLane &q) { return q.h.last_z; });
+    return __shfl_sync(kFull, t.h.nodeCost, 0);
+}
+
+// the host-side tail of FastRRT::loop, one warp per slot (the warp helps
+// lane 0 re-run the winning connection's curve)
 __global__ void k_finish(const Inst *insts, State *states, int n)
 {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int slot = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (slot >= n)
-        return;
+        return;  // uniform across the warp
     State &S = states[slot];
     if (!live(S))
-        return;
+        return;  // uniform across the warp
     const Inst &I = insts[slot];
+    const bool connect = !(S.temp_count == 0 && S.all_count == 0) && S.best < kBigCost;
+    float seg = 0.0f;
+    if (connect) {
+        const int widx = (int)(S.winner & 0xffffffffu);
+        const int wcell = (int)(0xffffffffu - (unsigned)(I.node_key[widx] & 0xffffffffu));
+        seg = connection_segment_cost(I, I.nodes[widx], wcell, lane);
+    }
+    if (lane != 0)
+        return;
     S.last_expanded = S.temp_count;
     if (S.temp_count == 0 && S.all_count == 0) {
         // empty graph: the start is added again (fastrrt.cpp:132-139)
@@ -1201,11 +1255,11 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
         const int idx = (int)(S.winner & 0xffffffffu);
         const int ppos = I.nodes[idx];
         const int pz = ppos / I.W, px = ppos - pz * I.W;
-        const int cell = I.node_best_cell[idx];
+        const int cell = (int)(0xffffffffu - (unsigned)(I.node_key[idx] & 0xffffffffu));
         const int cz = cell / I.W, cx = cell - cz * I.W;
         const float base = I.cost[ppos];
         const float child_heading = I.gd_heading[cell];
-        grid_add(I, cx, cz, child_heading, px, pz, I.node_best_seg[idx] + base);
+        grid_add(I, cx, cz, child_heading, px, pz, seg + base);
         const float child_cost = child_heading + base;
         grid_add(I, I.goal_x, I.goal_z, I.goal_heading, cx, cz, child_cost);
         if (I.goal_x >= 0 && I.goal_x < I.W && I.goal_z >= 0 && I.goal_z < I.H &&
@@ -1246,7 +1300,7 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
 const char *const kIterKernelNames[kIterKernels] = {
     "k_scan", "k_plan(cand)", "k_expand", "k_apply", "k_post", "k_erase",
     "k_setnodes", "k_accept", "k_plan(nodes)", "k_gd_demand", "k_plan(cells)", "k_gd_eval",
-    "k_goal", "k_select", "k_finish"};
+    "k_plan(windows)", "k_goal", "k_select", "k_finish"};
 
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
                       const Launch &L, cudaStream_t st, cudaEvent_t *ev)
@@ -1261,7 +1315,7 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     k_scan<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 0);
+    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 0);
     mark();
     k_expand<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
     mark();
@@ -1275,19 +1329,21 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     k_accept<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 1);
+    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 1);
     mark();
     k_gd_demand<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_state, d_sched, 2);
+    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 2);
     mark();
     k_gd_eval<<<L.sms * kWarpGrabBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    mark();
+    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 3);
     mark();
     k_goal<<<L.sms * kWarpGrabBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_select<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
-    k_finish<<<(n_slots + 127) / 128, 128, 0, st>>>(d_inst, d_state, n_slots);
+    k_finish<<<(n_slots * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_state, n_slots);
     mark();
 }
 

@@ -22,6 +22,7 @@ struct Sched {
     int *cand_start;          // [n_slots + 1] prefix of candidate chunks per slot
     int *node_start;          // [n_slots + 1] prefix of node chunks per slot
     int *gd_start;            // [n_slots + 1] prefix of direct-connection chunks per slot
+    int *goal_start;          // [n_slots + 1] prefix of (node, window chunk) units per slot
     unsigned *grab;           // [4] dynamic work counters
 };
 
@@ -61,7 +62,7 @@ void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, 
 // one planning iteration (loop()) over all active slots; with `ev` (an array
 // of kIterKernels + 1 events) an event is recorded before each kernel and
 // after the last one
-constexpr int kIterKernels = 15;
+constexpr int kIterKernels = 16;
 extern const char *const kIterKernelNames[kIterKernels];
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
                       const Launch &L, cudaStream_t st, cudaEvent_t *ev = nullptr);
