@@ -119,17 +119,18 @@ __device__ __forceinline__ bool box_clear(const Foot &f, int x0, int z0, int x1,
 
 // The footprint at heading direction (|cos|, |sin|) = (ac, as) probes only
 // cells within its axis-aligned bounding box: offsets j c - i s and j s + i c
-// with |j| <= mdx, |i| <= mdz, truncated toward zero, plus one cell for the
-// truncation and the rounding of the reference's cosf / sinf.  An empty box
-// means every probe misses, so the footprint is feasible and the reference
-// runs all its probes.
+// with |j| <= mdx, |i| <= mdz are at most e = mdx ac + mdz as (resp.
+// mdx as + mdz ac) away, so the truncated cells lie within ceil(e + 1e-3)
+// (the slack covers the rounding of the reference's cosf / sinf and float
+// arithmetic).  An empty box means every probe misses, so the footprint is
+// feasible and the reference runs all its probes.
 __device__ __forceinline__ bool box_feasible(const Foot &f, int x, int z, float ac, float as,
                                              unsigned long long &probes)
 {
     if (!f.sat || !(ac <= 1.5f) || !(as <= 1.5f))
         return false;
-    const int ex = (int)ceilf(f.mdx * ac + f.mdz * as + 1e-3f) + 1;
-    const int ez = (int)ceilf(f.mdx * as + f.mdz * ac + 1e-3f) + 1;
+    const int ex = (int)ceilf(f.mdx * ac + f.mdz * as + 1e-3f);
+    const int ez = (int)ceilf(f.mdx * as + f.mdz * ac + 1e-3f);
     if (!box_clear(f, x - ex, z - ez, x + ex, z + ez))
         return false;
     probes += full_probes(f);
@@ -224,39 +225,43 @@ __device__ inline bool probe_warp(const Foot &f, int x, int z, float angle, int 
 // A cheaper exact test than the full probe loop, for footprints that turn
 // out feasible.  Every probe (j, i) of the footprint at (x, z) with direction
 // (c, s) lies in the rectangle |u| <= mdx, |v| <= mdz, with u = X' c + Z' s,
-// v = -X' s + Z' c relative to the cell.  A probe in frame row zr has
-// Z' in [zr - z, zr - z + 1] (row 0 also takes Z' in (-1, 0): truncation
+// v = -X' s + Z' c relative to the cell.  A probe lands in frame row zr when
+// Z' is in [zr - z, zr - z + 1) (row 0 also takes Z' in (-1, 0): truncation
 // toward zero), and over that strip each constraint bounds X' by an interval
-// whose ends move linearly, so their hulls bound every probe of the row.
-// Lane k tests rows z0 + k, z0 + k + 32, ... with one cell of margin each
-// side; no obstacle bit in any interval means no probe can hit.
+// whose ends move linearly, so their hulls bound every probe of the row; the
+// probe's column is the truncation of x + X'.  Lane k tests rows z0 + k,
+// z0 + k + 32, ...; 1e-3 of slack covers the rounding of the reference's
+// float probe arithmetic.  No obstacle bit in any interval means no probe can
+// hit.
 __device__ inline bool rows_clear_warp(const Foot &f, int x, int z, float c, float s, int lane)
 {
     const float ac = fabsf(c), as = fabsf(s);
     const float ez = f.mdx * as + f.mdz * ac;
     const int z0 = max(0, (int)floorf(z - ez) - 1);
     const int z1 = min(f.H - 1, (int)floorf(z + ez) + 1);
+    const bool use1 = ac > 1e-6f, use2 = as > 1e-6f;
+    const float ic = use1 ? 1.0f / c : 0.0f, is = use2 ? 1.0f / s : 0.0f;
+    const float h1 = f.mdx * fabsf(ic), h2 = f.mdz * fabsf(is);
+    const float sic = s * ic, cis = c * is;
     bool hit = false;
     for (int zr = z0 + lane; zr <= z1 && !hit; zr += 32) {
         const float za = (float)(zr - z) - (zr == 0 ? 1.001f : 0.001f);
         const float zb = (float)(zr - z + 1) + 0.001f;
         float lo = -1e30f, hi = 1e30f;
-        if (ac > 1e-6f) {
-            const float a0 = (-f.mdx - za * s) / c, a1 = (f.mdx - za * s) / c;
-            const float b0 = (-f.mdx - zb * s) / c, b1 = (f.mdx - zb * s) / c;
-            lo = fmaxf(lo, fminf(fminf(a0, a1), fminf(b0, b1)));
-            hi = fminf(hi, fmaxf(fmaxf(a0, a1), fmaxf(b0, b1)));
+        if (use1) {  // X' = (+-mdx - Z' s) / c
+            const float pa = -za * sic, pb = -zb * sic;
+            lo = fmaxf(lo, fminf(pa, pb) - h1);
+            hi = fminf(hi, fmaxf(pa, pb) + h1);
         }
-        if (as > 1e-6f) {
-            const float a0 = (za * c - f.mdz) / s, a1 = (za * c + f.mdz) / s;
-            const float b0 = (zb * c - f.mdz) / s, b1 = (zb * c + f.mdz) / s;
-            lo = fmaxf(lo, fminf(fminf(a0, a1), fminf(b0, b1)));
-            hi = fminf(hi, fmaxf(fmaxf(a0, a1), fmaxf(b0, b1)));
+        if (use2) {  // X' = (Z' c +- mdz) / s
+            const float qa = za * cis, qb = zb * cis;
+            lo = fmaxf(lo, fminf(qa, qb) - h2);
+            hi = fminf(hi, fmaxf(qa, qb) + h2);
         }
         if (!(lo <= hi))
             continue;
-        const int xa = max(0, (int)floorf(x + lo) - 1);
-        const int xb = min(f.W - 1, (int)floorf(x + hi) + 1);
+        const int xa = max(0, (int)floorf(x + lo - 1e-3f));
+        const int xb = min(f.W - 1, (int)(x + hi + 1e-3f));
         if (xa > xb)
             continue;
         const uint32_t *row = f.blocked + (long)zr * f.rw;
