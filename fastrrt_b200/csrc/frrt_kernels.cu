@@ -313,9 +313,8 @@ void launch_direct_goal_reset(const Inst *d_inst, const int *d_slots, int n, int
     k_gd_reset<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots, fresh);
 }
 
-// Evaluates the goal direct connection of cells: listed ones (list mode, one
-// chunk of kGdChunk list entries per grab) or, without a list, every cell of
-// the slots in `slots` still unknown (one chunk of kGdChunk cells per grab).
+// Evaluates the goal direct connection of one cell per lane (has = the lane
+// holds a cell); the warp answers full footprint probes together.
 __device__ void gd_eval_cell(const Inst &I, const Foot &f, bool has, int pos,
                              unsigned long long &probes)
 {
@@ -511,13 +510,13 @@ __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, 
 
 // prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
 // work units of one slot: 0 candidate chunks, 1 listed-node chunks, 2
-// listed-cell chunks, 3 (listed node, window chunk) pairs
+// listed cells, 3 (listed node, window chunk) pairs
 __device__ __forceinline__ long long chunks_of(const Inst &I, const State &S, int which)
 {
     switch (which) {
     case 0: return (S.n_cand + kCandChunk - 1) / kCandChunk;
     case 1: return (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
-    case 2: return (S.n_gd + kGdChunk - 1) / kGdChunk;
+    case 2: return S.n_gd;
     default: return (long long)S.n_nodes * I.win_chunks;
     }
 }
@@ -984,31 +983,112 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
     }
 }
 
-// One warp per chunk of kGdChunk listed cells, grabbed by each warp on its
-// own (curve lengths differ a lot); masks are read through L1.
-__global__ void __launch_bounds__(256) k_gd_eval(const Inst *insts, State *states, Sched *sc)
+// A full footprint probe for lane `leader`, answered by the whole warp; the
+// leader's footprint may belong to another slot than the other lanes' tasks.
+__device__ inline bool coop_probe(const Foot &mine, int leader, int lane, int x, int z, float angle,
+                                  unsigned &cnt)
+{
+    Foot f;
+    f.W = __shfl_sync(kFull, mine.W, leader);
+    f.H = __shfl_sync(kFull, mine.H, leader);
+    f.mdx = __shfl_sync(kFull, mine.mdx, leader);
+    f.mdz = __shfl_sync(kFull, mine.mdz, leader);
+    f.lbx = __shfl_sync(kFull, mine.lbx, leader);
+    f.lbz = __shfl_sync(kFull, mine.lbz, leader);
+    f.ubx = __shfl_sync(kFull, mine.ubx, leader);
+    f.ubz = __shfl_sync(kFull, mine.ubz, leader);
+    f.rw = __shfl_sync(kFull, mine.rw, leader);
+    f.blocked = reinterpret_cast<const uint32_t *>(
+        __shfl_sync(kFull, reinterpret_cast<unsigned long long>(mine.blocked), leader));
+    f.clear = nullptr;
+    f.trav = nullptr;
+    f.sat = nullptr;
+    const int bx = __shfl_sync(kFull, x, leader);
+    const int bz = __shfl_sync(kFull, z, leader);
+    const float ba = __shfl_sync(kFull, angle, leader);
+    if (rows_clear_warp(f, bx, bz, cosf(ba), sinf(ba), lane)) {
+        cnt = full_probes(f);  // feasible: the reference runs all its probes
+        return true;
+    }
+    return probe_warp(f, bx, bz, ba, lane, cnt);
+}
+
+// Listed cells are handed to lanes one by one: a lane whose curve ended
+// takes the next cell (of any slot) at the start of the warp's next step, so
+// lanes stay busy although curve lengths differ a lot.  Full footprint
+// probes are answered by the whole warp.  Masks are read through L1.
+__global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts, State *states, Sched *sc)
 {
     const int n = sc->n_slots;
     const int total = sc->gd_start[n];
     const int lane = threadIdx.x & 31;
+    const unsigned lower = (1u << lane) - 1u;
+    PrecompTask t;
+    Foot f{};
+    const Inst *I = nullptr;
+    int slot = 0, pos = 0;
+    float lh = 0.0f;
+    bool active = false, exhausted = false;
+    unsigned long long probes = 0;
+    auto finish = [&]() {
+        if (t.h.ok) {
+            I->gd_heading[pos] = lh;
+            I->gd_cost[pos] = t.h.nodeCost;
+        }
+        I->gd_flag[pos] = t.h.ok ? 1 : 0;
+        if (probes)
+            atomicAdd(&states[slot].probes_pre, probes);
+        probes = 0;
+        active = false;
+    };
     while (true) {
-        int c = 0;
-        if (lane == 0)
-            c = (int)atomicAdd(&sc->grab[2], 1u);
-        c = __shfl_sync(kFull, c, 0);
-        if (c >= total)
+        if (!exhausted) {
+            const unsigned idle = __ballot_sync(kFull, !active);
+            if (idle) {
+                int base = 0;
+                if (lane == 0)
+                    base = (int)atomicAdd(&sc->grab[2], (unsigned)__popc(idle));
+                base = __shfl_sync(kFull, base, 0);
+                if (base + __popc(idle) >= total)
+                    exhausted = true;
+                const int e = base + __popc(idle & lower);
+                if (!active && e < total) {
+                    slot = find_slot(sc->gd_start, n, e);
+                    I = &insts[slot];
+                    pos = I->gd_list[e - sc->gd_start[slot]];
+                    f = foot_of(*I, I->blocked, I->clear);
+                    const int z = pos / I->W;
+                    const int x = pos - z * I->W;
+                    lh = compute_heading(x, z, I->goal_x, I->goal_z);
+                    t.h.init(*I, f, I->gd_max_curvature, x, z, lh, I->goal_x, I->goal_z,
+                             I->goal_heading, 0, I->gd_cost[pos]);
+                    active = true;
+                }
+            }
+        }
+        if (!__any_sync(kFull, active))
             break;
-        const int slot = find_slot(sc->gd_start, n, c);
-        const Inst &I = insts[slot];
-        State &S = states[slot];
-        const Foot f = foot_of(I, I.blocked, I.clear);
-        const int idx = (c - sc->gd_start[slot]) * kGdChunk + lane;
-        const bool has = idx < S.n_gd;
-        unsigned long long probes = 0;
-        gd_eval_cell(I, f, has, has ? I.gd_list[idx] : 0, probes);
-        probes = warp_sum64(probes);
-        if (lane == 0 && probes)
-            atomicAdd(&S.probes_pre, probes);
+        bool need = false;
+        if (active) {
+            if (t.advance(f, probes))
+                need = true;
+            else
+                finish();
+        }
+        unsigned m = __ballot_sync(kFull, need);
+        bool ok_mine = true;
+        while (m) {
+            const int leader = __ffs(m) - 1;
+            m &= m - 1;
+            unsigned cnt = 0;
+            const bool ok = coop_probe(f, leader, lane, t.h.last_x, t.h.last_z, t.probe_angle(), cnt);
+            if (lane == leader) {
+                ok_mine = ok;
+                probes += cnt;
+            }
+        }
+        if (need && !t.resolve(ok_mine))
+            finish();
     }
 }
 
@@ -1091,7 +1171,7 @@ __device__ __forceinline__ unsigned long long connection_key(long long lc, int c
 // so a few nodes with busy windows do not hold a launch back.  The last
 // chunk of a node to finish keeps the node's result when no chunk skipped a
 // cell by the bound.  Masks are read through L1.
-__global__ void __launch_bounds__(256) k_goal(const Inst *insts, State *states, Sched *sc)
+__global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, State *states, Sched *sc)
 {
     const int n = sc->n_slots;
     const int total = sc->goal_start[n];
@@ -1335,11 +1415,11 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 2);
     mark();
-    k_gd_eval<<<L.sms * kWarpGrabBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_gd_eval<<<L.sms * kEvalBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 3);
     mark();
-    k_goal<<<L.sms * kWarpGrabBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    k_goal<<<L.sms * kGoalBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_select<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();

@@ -10,8 +10,10 @@ namespace frrt {
 constexpr int kSweepCells = 4096;   // cells per sweep chunk (256 threads x 16)
 constexpr int kCandChunk = 256;     // candidates per expansion chunk (one per thread)
 constexpr int kNodeChunk = 8;       // listed nodes per goal-search chunk (one per warp)
-constexpr int kGdChunk = 32;        // listed cells per direct-connection chunk (one per lane)
-constexpr int kWarpGrabBlocks = 2;  // blocks per SM of the warp-grab kernels
+// resident blocks per SM of the warp-grab kernels (register budgets: measured
+// best on B200, 2 for the cell evaluation, 3 for the goal search)
+constexpr int kEvalBlocks = 2;
+constexpr int kGoalBlocks = 3;
 constexpr int32_t kClaimFree = 0x7F7F7F7F;
 
 // Scheduling tables shared by the iteration kernels (device memory).
@@ -21,7 +23,7 @@ struct Sched {
     int *sweep_start;         // [n_slots + 1] prefix of sweep chunks per slot
     int *cand_start;          // [n_slots + 1] prefix of candidate chunks per slot
     int *node_start;          // [n_slots + 1] prefix of node chunks per slot
-    int *gd_start;            // [n_slots + 1] prefix of direct-connection chunks per slot
+    int *gd_start;            // [n_slots + 1] prefix of listed direct-connection cells per slot
     int *goal_start;          // [n_slots + 1] prefix of (node, window chunk) units per slot
     unsigned *grab;           // [4] dynamic work counters
 };
