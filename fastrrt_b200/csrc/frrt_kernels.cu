@@ -200,47 +200,65 @@ __global__ void k_clear(const Inst *insts, const int *slots)
     }
 }
 
-// summed-area table of the obstacle mask, pass 1: prefix counts along each
-// row (row 0 and column 0 are zero)
-__global__ void k_sat_rows(const Inst *insts, const int *slots)
+// Summed-area table of the obstacle mask, one block per slot: each warp scans
+// rows (lanes over 32-pixel words, popcount prefix across the warp), then each
+// thread runs down columns.  Row 0 and column 0 are zero; counts wrap mod 2^16.
+__global__ void __launch_bounds__(256) k_sat(const Inst *insts, const int *slots)
 {
-    const Inst &I = insts[slots[blockIdx.y]];
+    const Inst &I = insts[slots[blockIdx.x]];
     if (!I.sat)
         return;
     uint16_t *S = const_cast<uint16_t *>(I.sat);
     const int w = I.W + 1;
-    for (int z = blockIdx.x * blockDim.x + threadIdx.x; z <= I.H; z += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int z = warp; z <= I.H; z += nwarps) {
         uint16_t *row = S + (long)z * w;
-        row[0] = 0;
         if (z == 0) {
-            for (int x = 1; x < w; x++)
+            for (int x = lane; x < w; x += 32)
                 row[x] = 0;
             continue;
         }
+        if (lane == 0)
+            row[0] = 0;
         const uint32_t *m = I.blocked + (long)(z - 1) * I.mask_rw;
-        uint16_t run = 0;
-        for (int q = 0; q < I.mask_rw; q++) {
-            const uint32_t bits = m[q];
-            const int n = min(32, I.W - q * 32);
-            for (int b = 0; b < n; b++) {
-                run = (uint16_t)(run + ((bits >> b) & 1u));
-                row[q * 32 + b + 1] = run;
+        unsigned carry = 0;
+        for (int q0 = 0; q0 < I.mask_rw; q0 += 32) {
+            const int q = q0 + lane;
+            const uint32_t bits = q < I.mask_rw ? m[q] : 0u;
+            const int c = __popc(bits);
+            int incl = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o)
+                    incl += v;
             }
+            if (q < I.mask_rw) {
+                unsigned run = carry + (unsigned)(incl - c);
+                const int nb = min(32, I.W - q * 32);
+                for (int b = 0; b < nb; b++) {
+                    run += (bits >> b) & 1u;
+                    row[q * 32 + b + 1] = (uint16_t)run;
+                }
+            }
+            carry += (unsigned)__shfl_sync(kFull, incl, 31);
         }
     }
-}
-
-// pass 2: prefix down each column
-__global__ void k_sat_cols(const Inst *insts, const int *slots)
-{
-    const Inst &I = insts[slots[blockIdx.y]];
-    if (!I.sat)
-        return;
-    uint16_t *S = const_cast<uint16_t *>(I.sat);
-    const int w = I.W + 1;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < w; x += gridDim.x * blockDim.x) {
+    __syncthreads();
+    for (int x = threadIdx.x; x < w; x += blockDim.x) {
         uint16_t run = 0;
-        for (int z = 1; z <= I.H; z++) {
+        int z = 1;
+        for (; z + 7 <= I.H; z += 8) {
+            uint16_t v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                v[k] = S[(long)(z + k) * w + x];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                run = (uint16_t)(run + v[k]);
+                S[(long)(z + k) * w + x] = run;
+            }
+        }
+        for (; z <= I.H; z++) {
             run = (uint16_t)(run + S[(long)z * w + x]);
             S[(long)z * w + x] = run;
         }
@@ -257,10 +275,8 @@ void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, 
     k_blocked<<<grid, 256, 0, st>>>(d_inst, d_state, d_slots, d_bad_class);
     k_rowdil<<<grid, 256, 0, st>>>(d_inst, d_slots);
     k_clear<<<grid, 256, 0, st>>>(d_inst, d_slots);
-    if (max_w > 0 && max_h > 0) {
-        k_sat_rows<<<dim3((max_h + 1 + 127) / 128, n), 128, 0, st>>>(d_inst, d_slots);
-        k_sat_cols<<<dim3((max_w + 1 + 127) / 128, n), 128, 0, st>>>(d_inst, d_slots);
-    }
+    if (max_w > 0 && max_h > 0)
+        k_sat<<<n, 256, 0, st>>>(d_inst, d_slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -384,6 +400,12 @@ __global__ void k_clear_types(const Inst *insts, const int *slots, int fresh)
     const Inst &I = insts[slots[blockIdx.y]];
     const long cells = (long)I.W * I.H;
     const int4 zero = make_int4(0, 0, 0, 0);
+    if (blockIdx.x == 0)
+        for (int r = threadIdx.x; r < kMaxRegions; r += blockDim.x) {
+            if (fresh)
+                I.region_count[r] = 0;
+            I.region_new[r] = 0;
+        }
     for (long base = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < cells;
          base += (long)gridDim.x * blockDim.x * 16) {
         *reinterpret_cast<int4 *>(I.type + base) = zero;
@@ -436,11 +458,7 @@ __global__ void k_init_state(const Inst *insts, State *states, const int *slots,
     S.start_ns = global_ns();
     S.finish_ns = 0;
     S.deadline_ns = I.timeout_ns > 0 ? S.start_ns + I.timeout_ns : 0;
-    if (reset_regions)
-        for (int r = 0; r < kMaxRegions; r++)
-            I.region_count[r] = 0;
-    for (int r = 0; r < kMaxRegions; r++)
-        I.region_new[r] = 0;
+    (void)reset_regions;  // region counters are reset by k_clear_types
 }
 
 void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, int n,
@@ -1772,18 +1790,26 @@ __device__ __forceinline__ float wrap_pi(float a)
 }
 
 // per-path checks, one thread per slot (the path is short)
-__global__ void k_path_check(const Inst *insts, const int *slots, int n, const float *paths,
-                             const int *path_n, int cap, int *valid, float *length)
+// The validator on one path per warp: lane k checks waypoints k, k + 32, ...
+// (cell in the frame, parent link, no repeated cell, heading change within
+// the curvature bound, footprint feasible outside the ego box); footprints
+// the quick tests cannot clear are probed by the whole warp.
+__global__ void __launch_bounds__(128) k_path_check(const Inst *insts, const int *slots, int n,
+                                                    const float *paths, const int *path_n, int cap,
+                                                    int *valid, float *length)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (k >= n)
-        return;
+        return;  // uniform across the warp
     const Inst &I = insts[slots[k]];
     const float *p = paths + (long)k * cap * 3;
     const int m = path_n[k];
-    length[k] = 0.0f;
     if (m < 2 || (int)p[0] != I.start_x || (int)p[1] != I.start_z) {
-        valid[k] = 0;
+        if (lane == 0) {
+            valid[k] = 0;
+            length[k] = 0.0f;
+        }
         return;
     }
     const Foot f = foot_of(I, I.blocked, I.clear);
@@ -1794,49 +1820,64 @@ __global__ void k_path_check(const Inst *insts, const int *slots, int n, const f
     if (0.8 > kappa)
         kappa = 0.8;
     float len = 0.0f;
-    bool ok = true;
-    for (int i = 0; i < m && ok; i++) {
-        const int x = (int)p[3 * i], z = (int)p[3 * i + 1];
-        const float h = p[3 * i + 2];
-        if (x < 0 || x >= I.W || z < 0 || z >= I.H) {
-            ok = false;
-            break;
+    bool bad = false;
+    for (int i0 = 0; i0 < m; i0 += 32) {
+        const int i = i0 + lane;
+        bool need = false;
+        int x = 0, z = 0;
+        float h = 0.0f;
+        if (i < m) {
+            x = (int)p[3 * i];
+            z = (int)p[3 * i + 1];
+            h = p[3 * i + 2];
+            if (x < 0 || x >= I.W || z < 0 || z >= I.H) {
+                bad = true;
+            } else {
+                const bool in_ego = x >= I.lbx && x <= I.ubx && z >= I.ubz && z <= I.lbz;
+                unsigned long long pr = 0;
+                if (!in_ego && !quick_feasible(f, x, z, pr)) {
+                    float sn, cs;
+                    sincosf(h, &sn, &cs);
+                    need = !box_feasible(f, x, z, fabsf(cs), fabsf(sn), pr);
+                }
+                if (i > 0) {
+                    const int px = (int)p[3 * (i - 1)], pz = (int)p[3 * (i - 1) + 1];
+                    const int32_t par = I.parent[(long)z * I.W + x];
+                    const double chord =
+                        sqrt((double)(x - px) * (x - px) + (double)(z - pz) * (z - pz));
+                    const float dh = wrap_pi(h - p[3 * (i - 1) + 2]);
+                    if ((px == x && pz == z) || I.type[(long)z * I.W + x] == T_NULL ||
+                        unpack_x(par) != px || unpack_z(par) != pz ||
+                        fabs(dh) > (kPi / 2) * kappa * chord + 1e-3)
+                        bad = true;
+                    len += sqrtf((float)((x - px) * (x - px) + (z - pz) * (z - pz)));
+                }
+            }
         }
-        const bool in_ego = x >= I.lbx && x <= I.ubx && z >= I.ubz && z <= I.lbz;
-        unsigned long long pr = 0;
-        if (!in_ego && !feasible_scalar(f, x, z, h, pr)) {
-            ok = false;
-            break;
-        }
-        if (i > 0) {
-            const int px = (int)p[3 * (i - 1)], pz = (int)p[3 * (i - 1) + 1];
-            if (px == x && pz == z) {
-                ok = false;
-                break;
-            }
-            const int32_t par = I.parent[(long)z * I.W + x];
-            if (I.type[(long)z * I.W + x] == T_NULL || unpack_x(par) != px || unpack_z(par) != pz) {
-                ok = false;
-                break;
-            }
-            const double chord = sqrt((double)(x - px) * (x - px) + (double)(z - pz) * (z - pz));
-            const float dh = wrap_pi(h - p[3 * (i - 1) + 2]);
-            if (fabs(dh) > (kPi / 2) * kappa * chord + 1e-3) {
-                ok = false;
-                break;
-            }
-            len += sqrtf((float)((x - px) * (x - px) + (z - pz) * (z - pz)));
+        unsigned mm = __ballot_sync(kFull, need);
+        while (mm) {
+            const int leader = __ffs(mm) - 1;
+            mm &= mm - 1;
+            unsigned cnt = 0;
+            const bool ok = coop_probe(f, leader, lane, x, z, h, cnt);
+            if (lane == leader && !ok)
+                bad = true;
         }
     }
-    if (ok) {
+    bad = __any_sync(kFull, bad);
+    for (int o = 16; o; o >>= 1)
+        len += __shfl_xor_sync(kFull, len, o);
+    if (lane != 0)
+        return;
+    if (!bad) {
         const int lx = (int)p[3 * (m - 1)], lz = (int)p[3 * (m - 1) + 1];
         const double gdx = lx - I.goal_x, gdz = lz - I.goal_z;
         if (sqrt(gdx * gdx + gdz * gdz) > I.dist_tol)
-            ok = false;
+            bad = true;
         if (fabsf(p[3 * (m - 1) + 2] - I.goal_heading) > I.heading_tol)
-            ok = false;
+            bad = true;
     }
-    if (!ok)
+    if (bad)
         valid[k] = 0;
     length[k] = len;
 }
@@ -1858,8 +1899,8 @@ void launch_validate(const Inst *d_inst, State *d_state, const int *d_slots, int
     k_fill_int<<<(n + 255) / 256, 256, 0, st>>>(d_valid, n, 1);
     launch_count(d_inst, d_slots, n, max_cells, T_NODE, d_counts, st);
     k_dag<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, d_counts, d_valid);
-    k_path_check<<<(n + 63) / 64, 64, 0, st>>>(d_inst, d_slots, n, d_paths, d_path_n, cap, d_valid,
-                                               d_length);
+    k_path_check<<<(n * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_slots, n, d_paths, d_path_n, cap,
+                                                       d_valid, d_length);
 }
 
 // ---------------------------------------------------------------------------
