@@ -58,6 +58,9 @@ EXPORTS = [
     "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
     "fastrrt_batch_kernel_times", "fastrrt_kernel_count", "fastrrt_kernel_name",
     "fastrrt_batch_probes", "fastrrt_batch_serve",
+    # learned expansion proposal
+    "fastrrt_mlp_create", "fastrrt_mlp_destroy", "fastrrt_mlp_get_weights",
+    "fastrrt_mlp_set_weights", "fastrrt_mlp_forward", "fastrrt_mlp_gradients", "fastrrt_mlp_train",
 ]
 
 
@@ -142,6 +145,14 @@ def lib():
         "fastrrt_kernel_count": (C.c_int, []),
         "fastrrt_kernel_name": (C.c_char_p, [C.c_int]),
         "fastrrt_batch_probes": (C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+        "fastrrt_mlp_create": (vp, [C.c_uint64, C.c_int]),
+        "fastrrt_mlp_destroy": (None, [vp]),
+        "fastrrt_mlp_get_weights": (C.c_int, [vp] + [f32p] * 6),
+        "fastrrt_mlp_set_weights": (C.c_int, [vp] + [f32p] * 6),
+        "fastrrt_mlp_forward": (C.c_int, [vp, C.c_int, f32p, f32p]),
+        "fastrrt_mlp_gradients": (C.c_int, [vp, C.c_int, f32p, i32p] + [f32p] * 6 + [P(C.c_float)]),
+        "fastrrt_mlp_train": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                                        P(C.c_float)]),
         "fastrrt_batch_serve": (C.c_int, [vp, C.c_int, P(Request), vp, C.c_int, C.c_int, i32p, f32p,
                                           f32p, f32p, i32p, P(C.c_double), P(C.c_float)]),
     }

@@ -1,0 +1,85 @@
+// frrt_mlp.cuh -- the learned expansion proposal: a BF16 MLP (1030 -> 256 ->
+// 256 -> 128, ReLU, FP32 accumulation) with hand-written tensor-core GEMMs
+// (mma.sync m16n8k16 bf16), its training kernels, and the planner-side
+// feature extraction and proposal sampling.
+#pragma once
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "frrt_common.cuh"
+
+namespace frrt {
+
+constexpr int kMlpPatch = 32;                     // patch side (samples)
+constexpr int kMlpPatchStride = 2;                // pixels between patch samples
+constexpr int kMlpScalars = 6;                    // goal (u, v), distance, sin h, cos h, steer limit
+constexpr int kMlpIn = kMlpPatch * kMlpPatch + kMlpScalars;  // 1030
+constexpr int kMlpInPad = 1040;                   // K of layer 1, a multiple of 16
+constexpr int kMlpHidden = 256;
+constexpr int kSteerBins = 16;
+constexpr int kLenBins = 8;
+constexpr int kMlpOut = kSteerBins * kLenBins;    // 128
+
+// Weights of the three layers: W[l] is out x in (row-major, bf16), b[l] f32.
+struct MlpWeights {
+    const __nv_bfloat16 *w1, *w2, *w3;
+    const float *b1, *b2, *b3;
+};
+
+// C(M x N) = epilogue(sum_k A(m, k) B(k, n)).  A(m, k) = A[m * lda + k], or
+// A[k * lda + m] with transA; B(k, n) = B[n * ldb + k] (a weight matrix, out
+// x in), or B[k * ldb + n] with transB.  Epilogue: + bias[n] when bias,
+// ReLU when relu, times (mask[m * ldm + n] > 0) when mask (ReLU backward);
+// the result is written as f32 (cf) or bf16 (cb), row-major with ldc.
+struct GemmArgs {
+    int M, N, K;
+    const int *dM;             // device row count capping M, or nullptr
+    const __nv_bfloat16 *A;
+    int lda, transA;
+    const __nv_bfloat16 *B;
+    int ldb, transB;
+    const float *bias;
+    int relu;
+    const __nv_bfloat16 *mask;
+    int ldm;
+    float *cf;
+    __nv_bfloat16 *cb;
+    int ldc;
+};
+void launch_gemm(const GemmArgs &g, cudaStream_t st);
+
+// softmax cross-entropy over rows of logits (M x 128, f32): per-row loss
+// (f32, summed into *loss), d logits = (softmax - onehot) * scale as bf16
+void launch_softmax_xent(const float *logits, const int32_t *labels, int M, float scale,
+                         __nv_bfloat16 *dlogits, float *loss, cudaStream_t st);
+// db[n] = sum_m dY[m * ld + n] (bf16 in, f32 out)
+void launch_bias_grad(const __nv_bfloat16 *dY, int M, int N, int ld, float *db, cudaStream_t st);
+// Adam on f32 master weights; refreshes the bf16 copy
+void launch_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *w16, int n, float lr,
+                 float b1, float b2, float eps, int step, cudaStream_t st);
+void launch_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n, cudaStream_t st);
+// X rows and labels of a minibatch gathered by index
+void launch_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int32_t *idx, int n,
+                        __nv_bfloat16 *Xb, int32_t *lb, cudaStream_t st);
+
+// Features of expansion candidates: for candidate k of the listed ones, the
+// 32 x 32 obstacle patch around its parent cell in the parent's heading frame
+// (stride 2 px, forward = heading), the goal in that frame, the distance to
+// the goal, sin / cos of the heading and the steering limit; bf16, rows of
+// kMlpInPad (zero padded).  cells[k] / slots[k] name the parent.
+void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *slot_of, int n,
+                     __nv_bfloat16 *X, cudaStream_t st);
+
+// The (steering, length) bin of a draw, the training label
+__host__ __device__ inline int proposal_bin(float steer, float len, float max_steer, float max_path)
+{
+    int sb = (int)floorf((steer + max_steer) / (2.0f * max_steer) * kSteerBins);
+    sb = sb < 0 ? 0 : (sb >= kSteerBins ? kSteerBins - 1 : sb);
+    const float lo = 5.0f, hi = max_path > 5.0f ? max_path : 5.0f + 1e-3f;
+    int lb = (int)floorf((len - lo) / (hi - lo) * kLenBins);
+    lb = lb < 0 ? 0 : (lb >= kLenBins ? kLenBins - 1 : lb);
+    return sb * kLenBins + lb;
+}
+
+}  // namespace frrt

@@ -1,0 +1,70 @@
+"""The learned expansion proposal: a BF16 MLP (1030 -> 256 -> 256 -> 128)
+trained with the library's own kernels on expansions the planner accepted on
+its solution paths (fastrrt_mlp_* in the C ABI)."""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+N_IN = 1030
+N_IN_PAD = 1040
+HIDDEN = 256
+N_OUT = 128
+STEER_BINS = 16
+LEN_BINS = 8
+SHAPES = [(HIDDEN, N_IN_PAD), (HIDDEN,), (HIDDEN, HIDDEN), (HIDDEN,), (N_OUT, HIDDEN), (N_OUT,)]
+
+
+class ProposalNet:
+    def __init__(self, seed=0, max_batch=4096):
+        h = _lib.lib().fastrrt_mlp_create(int(seed), int(max_batch))
+        if not h:
+            raise _lib.FastRRTError("mlp_create: " + _lib.last_error())
+        self._h = h
+        self.max_batch = max_batch
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib._lib is not None:
+            _lib.lib().fastrrt_mlp_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_weights(self):
+        ws = [np.zeros(s, np.float32) for s in SHAPES]
+        _lib.check(_lib.lib().fastrrt_mlp_get_weights(self._h, *[w.reshape(-1) for w in ws]),
+                   "mlp_get_weights")
+        return ws
+
+    def set_weights(self, ws):
+        ws = [np.ascontiguousarray(w, np.float32).reshape(-1) for w in ws]
+        _lib.check(_lib.lib().fastrrt_mlp_set_weights(self._h, *ws), "mlp_set_weights")
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, N_IN)
+        out = np.zeros((len(X), N_OUT), np.float32)
+        _lib.check(_lib.lib().fastrrt_mlp_forward(self._h, len(X), X.reshape(-1), out.reshape(-1)),
+                   "mlp_forward")
+        return out
+
+    def gradients(self, X, labels):
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, N_IN)
+        labels = np.ascontiguousarray(labels, np.int32)
+        gs = [np.zeros(s, np.float32) for s in SHAPES]
+        loss = C.c_float(0)
+        _lib.check(_lib.lib().fastrrt_mlp_gradients(self._h, len(X), X.reshape(-1), labels,
+                                                     *[g.reshape(-1) for g in gs], C.byref(loss)),
+                   "mlp_gradients")
+        return gs, loss.value
+
+    def train(self, X_dev, labels_dev, n, epochs=4, batch=1024, lr=1e-3, seed=0):
+        """Adam on a device dataset (X_dev: n x 1040 bf16, labels_dev: n int32,
+        e.g. torch tensors); returns the mean loss of the last batch."""
+        loss = C.c_float(0)
+        _lib.check(_lib.lib().fastrrt_mlp_train(self._h, X_dev.data_ptr(), labels_dev.data_ptr(), int(n),
+                                                int(epochs), int(batch), float(lr), int(seed),
+                                                C.byref(loss)), "mlp_train")
+        return loss.value

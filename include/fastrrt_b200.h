@@ -247,6 +247,30 @@ int fastrrt_kernel_count(void);
 int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute);
 const char *fastrrt_kernel_name(int k);
 
+/* ---- part 5: the learned expansion proposal ------------------------------
+ * No counterpart in the reference.  A BF16 MLP (1030 -> 256 -> 256 -> 128,
+ * ReLU, FP32 accumulation, mma.sync tensor-core GEMMs) that proposes the
+ * (steering, length) bin of an expansion from a 32 x 32 obstacle patch around
+ * the parent (its heading frame, 2 px stride), the goal in that frame, the
+ * distance to the goal, sin / cos of the heading and the steering limit.
+ * Weights: w1 256 x 1040 (inputs 1030..1039 are padding), b1 256, w2
+ * 256 x 256, b2 256, w3 128 x 256, b3 128; all f32 on the host. */
+void *fastrrt_mlp_create(uint64_t seed, int max_batch);
+void fastrrt_mlp_destroy(void *mlp);
+int fastrrt_mlp_get_weights(void *mlp, float *w1, float *b1, float *w2, float *b2, float *w3,
+                            float *b3);
+int fastrrt_mlp_set_weights(void *mlp, const float *w1, const float *b1, const float *w2,
+                            const float *b2, const float *w3, const float *b3);
+/* logits (n x 128) of n host feature rows of 1030 floats */
+int fastrrt_mlp_forward(void *mlp, int n, const float *X, float *logits);
+/* mean cross-entropy gradients of a host batch (labels in 0..127) */
+int fastrrt_mlp_gradients(void *mlp, int n, const float *X, const int32_t *labels, float *gw1,
+                          float *gb1, float *gw2, float *gb2, float *gw3, float *gb3, float *loss);
+/* Adam training on a device dataset: X_bf16 n x 1040 bf16 rows, labels n
+ * int32 (device pointers); *last_loss = mean loss of the last batch */
+int fastrrt_mlp_train(void *mlp, const void *X_bf16, const int32_t *labels, int n, int epochs,
+                      int batch, float lr, uint64_t seed, float *last_loss);
+
 #ifdef __cplusplus
 }
 #endif
