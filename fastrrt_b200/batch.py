@@ -67,9 +67,12 @@ class BatchPlanner:
         self.n_slots = n_slots
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib._lib is not None:
-            _lib.lib().fastrrt_batch_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None) and _lib._lib is not None:
+                _lib.lib().fastrrt_batch_destroy(self._h)
+                self._h = None
+        except (AttributeError, TypeError):
+            pass  # interpreter shutdown
 
     def admit_many(self, requests, timeout_ms=0):
         arr = (_lib.Request * len(requests))(*requests)
@@ -148,6 +151,20 @@ class BatchPlanner:
         out["wall_ms"] = wall.value
         out["device_ms"] = dev.value
         return out
+
+    def set_proposal(self, net, mix=0.5, cap=131072):
+        """attach a ProposalNet (None detaches): each candidate's expansion is
+        sampled from the network with probability mix, uniformly otherwise"""
+        self._net = net
+        _lib.check(_lib.lib().fastrrt_batch_set_proposal(self._h, net.handle if net else None,
+                                                         float(mix), int(cap)), "batch_set_proposal")
+
+    def log_paths(self, X_dev, labels_dev, offset, cap):
+        """training rows of the last collected list's valid paths into device
+        tensors (X: rows of 1040 bf16, labels: int32); returns rows written"""
+        return _lib.check(_lib.lib().fastrrt_batch_log_paths(self._h, X_dev.data_ptr(),
+                                                             labels_dev.data_ptr(), int(offset),
+                                                             int(cap)), "batch_log_paths")
 
     def profile(self, on=True):
         _lib.check(_lib.lib().fastrrt_batch_profile(self._h, int(on)), "batch_profile")

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "frrt_engine.h"
+#include "frrt_mlp.h"
 
 using namespace frrt;
 
@@ -1127,6 +1128,29 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
     if (device_ms)
         *device_ms = ms;
     return good;
+}
+
+int fastrrt_batch_set_proposal(void *batch, void *mlp, float mix, int cap)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || (mlp && (cap <= 0 || !(mix >= 0.0f && mix <= 1.0f)))) {
+        set_error("batch set_proposal: bad arguments");
+        return -1;
+    }
+    if (!mlp)
+        return b->eng->set_proposal(nullptr, 0.0f, 0) ? 0 : -1;
+    const MlpWeights w = static_cast<Mlp *>(mlp)->weights();
+    return b->eng->set_proposal(&w, mix, cap) ? 0 : -1;
+}
+
+int fastrrt_batch_log_paths(void *batch, void *X_bf16, int32_t *labels, int offset, int cap)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || !X_bf16 || !labels || offset < 0 || cap < offset) {
+        set_error("batch log_paths: bad arguments");
+        return -1;
+    }
+    return b->eng->log_paths(static_cast<__nv_bfloat16 *>(X_bf16), labels, offset, cap);
 }
 
 int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute)

@@ -82,6 +82,10 @@ struct Inst {
     int32_t *cand_end;
     float *cand_heading;
     float *cand_cost;
+    float *cand_steer, *cand_len;  // per candidate: the draw it was integrated with
+    int32_t *prop_row;             // per candidate: row of the learned proposal, or -1
+    float *prop_steer, *prop_len;  // per candidate: the proposal (prop_len < 0: uniform)
+    float *exp_steer, *exp_len;    // per cell: the draw of the expansion that made the node
     int32_t *nodes;
     // per listed node: best connection as (floor(100 * total) << 32) |
     // (0xffffffff - cell), so the minimum is the cheapest, ties to the highest
@@ -113,6 +117,7 @@ struct Inst {
     int smart;
     int max_iter;              // 0 = unlimited
     int stop_on_goal;          // batched planning stops a slot at its goal
+    int proposal;              // expansions may come from the learned proposal
     long long timeout_ns;      // > 0: deadline after search_init (device clock)
 };
 

@@ -149,6 +149,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
         8 * C, 8 * C,                       // 27 memo key, 28 memo result
         2 * (size_t)(max_w + 1) * (max_h + 1),  // 29 obstacle summed-area table
+        4 * C, 4 * C, 4 * C, 4 * C, 4 * C,  // 30 cand steer, 31 cand len, 32 prop row, 33/34 prop
+        4 * C, 4 * C,                       // 35 exp steer, 36 exp len
     };
     constexpr int kParts = sizeof(parts) / sizeof(parts[0]);
     size_t per_slot = 0;
@@ -205,6 +207,13 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         I.memo_key = (unsigned long long *)ptr[27];
         I.memo_result = (unsigned long long *)ptr[28];
         I.sat = (const uint16_t *)ptr[29];
+        I.cand_steer = (float *)ptr[30];
+        I.cand_len = (float *)ptr[31];
+        I.prop_row = (int32_t *)ptr[32];
+        I.prop_steer = (float *)ptr[33];
+        I.prop_len = (float *)ptr[34];
+        I.exp_steer = (float *)ptr[35];
+        I.exp_len = (float *)ptr[36];
         I.lbx = I.lbz = I.ubx = I.ubz = -1;
         I.stop_on_goal = 1;
         if (!check(cudaMemsetAsync(I.claim, 0x7F, 4 * C, stream_), "claim init"))
@@ -267,6 +276,17 @@ Engine::~Engine()
     cudaFree(d_class_costs_);
     cudaFree(d_bad_);
     cudaFree(d_clock_);
+    cudaFree(pb_.cells);
+    cudaFree(pb_.slot_of);
+    cudaFree(pb_.idx);
+    cudaFree(pb_.count);
+    cudaFree(pb_.X);
+    cudaFree(pb_.h1);
+    cudaFree(pb_.h2);
+    cudaFree(pb_.logits);
+    cudaFree(d_log_cells_);
+    cudaFree(d_log_slots_);
+    cudaFree(d_log_count_);
     if (h_small_)
         cudaFreeHost(h_small_);
     cudaFree(d_paths_);
@@ -523,7 +543,8 @@ bool Engine::ensure_graph()
         return true;
     if (!check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture"))
         return false;
-    launch_iteration(d_inst_, d_state_, d_sched_, n_slots_, L_, stream_);
+    launch_iteration(d_inst_, d_state_, d_sched_, n_slots_, L_, stream_, nullptr,
+                     use_proposal_ ? &pb_ : nullptr);
     const cudaError_t launch_err = cudaGetLastError();
     const cudaError_t end_err = cudaStreamEndCapture(stream_, &graph_);
     if (!check(launch_err, "iteration capture") || !check(end_err, "graph capture end"))
@@ -552,7 +573,8 @@ bool Engine::iterate()
     if (dirty_ && !commit())
         return false;
     if (profiling_) {
-        launch_iteration(d_inst_, d_state_, d_sched_, n_slots_, L_, stream_, prof_ev_.data());
+        launch_iteration(d_inst_, d_state_, d_sched_, n_slots_, L_, stream_, prof_ev_.data(),
+                         use_proposal_ ? &pb_ : nullptr);
         if (!check(cudaGetLastError(), "iteration launch") || !sync())
             return false;
         for (int k = 0; k < kIterKernels; k++) {
@@ -761,6 +783,82 @@ bool Engine::grid_upload(int slot, const std::vector<int8_t> &type, const std::v
     if (ok)
         ok = set_intrinsic(slot, any_intr ? intrinsic.data() : nullptr);
     return ok && commit();
+}
+
+bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
+{
+    if (w && cap > 0 && cap != pb_.cap) {
+        cudaFree(pb_.cells);
+        cudaFree(pb_.slot_of);
+        cudaFree(pb_.idx);
+        cudaFree(pb_.count);
+        cudaFree(pb_.X);
+        cudaFree(pb_.h1);
+        cudaFree(pb_.h2);
+        cudaFree(pb_.logits);
+        pb_ = ProposalBufs{};
+        const size_t c = (size_t)cap;
+        if (!check(cudaMalloc(&pb_.cells, 4 * c), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.slot_of, 4 * c), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.idx, 4 * c), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.count, sizeof(int)), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.X, 2 * c * kMlpInPad), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.h1, 2 * c * kMlpHidden), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.h2, 2 * c * kMlpHidden), "proposal buffers") ||
+            !check(cudaMalloc(&pb_.logits, 4 * c * kMlpOut), "proposal buffers"))
+            return false;
+        pb_.cap = cap;
+    }
+    use_proposal_ = w != nullptr && pb_.cap > 0;
+    if (use_proposal_) {
+        pb_.w = *w;
+        pb_.mix = mix;
+    }
+    for (auto &I : h_inst_)
+        I.proposal = use_proposal_ ? 1 : 0;
+    dirty_ = true;
+    // the iteration graph changes
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    if (graph_) {
+        cudaGraphDestroy(graph_);
+        graph_ = nullptr;
+    }
+    return commit();
+}
+
+int Engine::log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap)
+{
+    const int n = (int)h_path_n_.size();
+    if (n == 0 || cap <= offset)
+        return 0;
+    const int rows_max = cap - offset;
+    if (rows_max > log_cap_) {
+        cudaFree(d_log_cells_);
+        cudaFree(d_log_slots_);
+        if (!d_log_count_ && !check(cudaMalloc(&d_log_count_, sizeof(int)), "log counter"))
+            return -1;
+        if (!check(cudaMalloc(&d_log_cells_, 4 * (size_t)rows_max), "log rows") ||
+            !check(cudaMalloc(&d_log_slots_, 4 * (size_t)rows_max), "log rows"))
+            return -1;
+        log_cap_ = rows_max;
+    }
+    if (!check(cudaMemsetAsync(d_log_count_, 0, sizeof(int), stream_), "log counter"))
+        return -1;
+    launch_log_paths(d_inst_, d_state_, d_slots_, n, d_paths_, d_path_n_, d_valid_, cap_, d_log_cells_,
+                     d_log_slots_, labels + offset, d_log_count_, rows_max, stream_);
+    int rows = 0;
+    if (!check(cudaMemcpyAsync(&h_small_[4], d_log_count_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+               "log counter") ||
+        !sync())
+        return -1;
+    rows = std::min(h_small_[4], rows_max);
+    launch_features(d_inst_, d_log_cells_, d_log_slots_, rows, X + (size_t)offset * kMlpInPad, stream_);
+    if (!check(cudaGetLastError(), "log features") || !sync())
+        return -1;
+    return rows;
 }
 
 bool Engine::device_clock(long long &ns)

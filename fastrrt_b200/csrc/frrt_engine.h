@@ -14,6 +14,7 @@
 
 #include "frrt_common.cuh"
 #include "frrt_kernels.cuh"
+#include "frrt_mlp.cuh"
 
 namespace frrt {
 
@@ -136,6 +137,14 @@ public:
 
     // batched extraction + validation of listed slots
     bool extract_and_validate(const std::vector<int> &slots, int cap);
+    // learned expansion proposal: network weights (device), the probability
+    // of sampling from it, rows per iteration; w == nullptr detaches it
+    bool set_proposal(const MlpWeights *w, float mix, int cap);
+    // training rows of the last extracted list: for each valid path, one row
+    // per expansion on it (features of the parent, the bin of the draw that
+    // made the child) appended at X[offset..], labels[offset..] (device, at
+    // most cap rows in all); returns the rows added or -1
+    int log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap);
     const std::vector<int> &paths_n() const { return h_path_n_; }
     const std::vector<int> &valid() const { return h_valid_; }
     const std::vector<float> &lengths() const { return h_length_; }
@@ -155,6 +164,11 @@ public:
     State *d_state() const { return d_state_; }
 
 private:
+    ProposalBufs pb_{};
+    bool use_proposal_ = false;
+    int32_t *d_log_cells_ = nullptr, *d_log_slots_ = nullptr;
+    int *d_log_count_ = nullptr;
+    int log_cap_ = 0;
     bool check(cudaError_t e, const char *what);
     bool ensure_graph();
     bool upload_slots_list(const std::vector<int> &slots);

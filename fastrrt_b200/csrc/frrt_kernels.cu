@@ -33,6 +33,7 @@
 
 #include "frrt_device.cuh"
 #include "frrt_kernels.cuh"
+#include "frrt_mlp.cuh"
 
 namespace frrt {
 
@@ -682,7 +683,15 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
             pos = I.cand[idx];
             const int z = pos / I.W, x = pos - z * I.W;
             float steer, len;
-            draw_expansion(I.seed, (uint32_t)pos, S.iter, (float)I.max_steer, I.max_path, steer, len);
+            if (I.proposal && I.prop_row[idx] >= 0 && I.prop_len[idx] >= 0.0f) {
+                steer = I.prop_steer[idx];
+                len = I.prop_len[idx];
+            } else {
+                draw_expansion(I.seed, (uint32_t)pos, S.iter, (float)I.max_steer, I.max_path, steer,
+                               len);
+            }
+            I.cand_steer[idx] = steer;
+            I.cand_len[idx] = len;
             t.k.init(I, x, z, steer, len, I.velocity, I.heading[pos], I.cost[pos]);
         }
         run_warp(t, has, f, probes, [](const KinLane &q) { return q.k.pend_x; },
@@ -744,6 +753,8 @@ __global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states,
         I.parent[end] = pack_xz(x, z);
         I.heading[end] = I.cand_heading[idx];
         I.cost[end] = I.cand_cost[idx];
+        I.exp_steer[end] = I.cand_steer[idx];
+        I.exp_len[end] = I.cand_len[idx];
     }
 }
 
@@ -1396,12 +1407,129 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
 }
 
 const char *const kIterKernelNames[kIterKernels] = {
-    "k_scan", "k_plan(cand)", "k_expand", "k_apply", "k_post", "k_erase",
+    "k_scan", "k_plan(cand)", "k_propose(mlp)", "k_expand", "k_apply", "k_post", "k_erase",
     "k_setnodes", "k_accept", "k_plan(nodes)", "k_gd_demand", "k_plan(cells)", "k_gd_eval",
     "k_plan(windows)", "k_goal", "k_select", "k_finish"};
 
+// ---------------------------------------------------------------------------
+// learned expansion proposal inside an iteration
+// ---------------------------------------------------------------------------
+
+// lists the candidates of slots that use the proposal (up to pb.cap rows)
+__global__ void __launch_bounds__(256) k_prop_list(const Inst *insts, const State *states,
+                                                   const Sched *sc, ProposalBufs pb)
+{
+    const int n = sc->n_slots;
+    const int total = sc->cand_start[n];
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        const int slot = find_slot(sc->cand_start, n, c);
+        const Inst &I = insts[slot];
+        const State &S = states[slot];
+        const int idx = (c - sc->cand_start[slot]) * kCandChunk + threadIdx.x;
+        if (idx >= S.n_cand || !I.proposal)
+            continue;
+        int row = atomicAdd(pb.count, 1);
+        if (row >= pb.cap) {
+            row = -1;
+        } else {
+            pb.cells[row] = I.cand[idx];
+            pb.slot_of[row] = slot;
+            pb.idx[row] = idx;
+        }
+        I.prop_row[idx] = row;
+    }
+}
+
+// One warp per listed candidate: with probability mix (the third Philox word
+// of the candidate's draw) the (steering, length) bin is sampled from the
+// softmax of the network's logits (fourth word, inverse CDF) and the value
+// uniformly inside the bin (first two words); otherwise prop_len = -1 and
+// the expansion draws uniformly as without the network.
+__global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const State *states,
+                                                     ProposalBufs pb)
+{
+    const int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int rows = min(*pb.count, pb.cap);
+    if (r >= rows)
+        return;
+    const int slot = pb.slot_of[r], idx = pb.idx[r], pos = pb.cells[r];
+    const Inst &I = insts[slot];
+    const State &S = states[slot];
+    uint32_t w[4];
+    philox4x32((uint32_t)pos, S.iter, kRngTag, 0u, (uint32_t)I.seed, (uint32_t)(I.seed >> 32), w);
+    if (!(u01(w[2]) < pb.mix)) {
+        if (lane == 0)
+            I.prop_len[idx] = -1.0f;
+        return;
+    }
+    const float *l = pb.logits + (long)r * kMlpOut;
+    float v[kMlpOut / 32];
+    float mx = -1e30f;
+#pragma unroll
+    for (int q = 0; q < kMlpOut / 32; q++) {
+        v[q] = l[lane * (kMlpOut / 32) + q];  // lane owns bins lane*4 .. lane*4+3
+        mx = fmaxf(mx, v[q]);
+    }
+    for (int o = 16; o; o >>= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+    float mine = 0.0f;
+#pragma unroll
+    for (int q = 0; q < kMlpOut / 32; q++) {
+        v[q] = __expf(v[q] - mx);
+        mine += v[q];
+    }
+    float incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const float t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += t;
+    }
+    const float total = __shfl_sync(kFull, incl, 31);
+    const float target = u01(w[3]) * total;
+    // the first bin whose cumulative mass reaches the target
+    const float before = incl - mine;
+    int bin = -1;
+    if (target < incl && target >= before) {
+        float run = before;
+        bin = lane * (kMlpOut / 32) + kMlpOut / 32 - 1;
+#pragma unroll
+        for (int q = 0; q < kMlpOut / 32; q++) {
+            run += v[q];
+            if (target < run) {
+                bin = lane * (kMlpOut / 32) + q;
+                break;
+            }
+        }
+    }
+    const unsigned found = __ballot_sync(kFull, bin >= 0);
+    const int owner = found ? __ffs(found) - 1 : 31;
+    bin = __shfl_sync(kFull, bin, owner);
+    if (bin < 0)
+        bin = kMlpOut - 1;
+    if (lane != 0)
+        return;
+    const float ms = (float)I.max_steer;
+    const int sb = bin / kLenBins, lb = bin - sb * kLenBins;
+    const float sw = 2.0f * ms / kSteerBins;
+    const float lo = 5.0f, hi = fmaxf(I.max_path, 5.0f);
+    const float lw = (hi - lo) / kLenBins;
+    I.prop_steer[idx] = -ms + (sb + u01(w[0])) * sw;
+    I.prop_len[idx] = fmaxf(5.0f, lo + (lb + u01(w[1])) * lw);
+}
+
+void launch_proposal(const Inst *d_inst, State *d_state, const Sched *d_sched, const ProposalBufs &pb,
+                     const Launch &L, cudaStream_t st)
+{
+    cudaMemsetAsync(pb.count, 0, sizeof(int), st);
+    k_prop_list<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched, pb);
+    launch_features(d_inst, pb.cells, pb.slot_of, pb.cap, pb.X, st, pb.count);
+    launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, pb.h1, pb.h2, pb.logits, st);
+    k_prop_sample<<<(pb.cap * 32 + 255) / 256, 256, 0, st>>>(d_inst, d_state, pb);
+}
+
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
-                      const Launch &L, cudaStream_t st, cudaEvent_t *ev)
+                      const Launch &L, cudaStream_t st, cudaEvent_t *ev, const ProposalBufs *pb)
 {
     const size_t smem = (size_t)L.smem_words * 2 * 4;
     int k = 0;
@@ -1414,6 +1542,9 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     k_scan<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 0);
+    mark();
+    if (pb)
+        launch_proposal(d_inst, d_state, d_sched, *pb, L, st);
     mark();
     k_expand<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
     mark();
@@ -1880,6 +2011,50 @@ __global__ void __launch_bounds__(128) k_path_check(const Inst *insts, const int
     if (bad)
         valid[k] = 0;
     length[k] = len;
+}
+
+// Training rows of valid paths: one per expansion on the path (waypoints 1 ..
+// m - 3; the last two are the goal connection and the goal): the parent cell,
+// its slot, and the bin of the draw that made the child.  One warp per path.
+__global__ void __launch_bounds__(128) k_log_list(const Inst *insts, const State *states,
+                                                  const int *slots, int n, const float *paths,
+                                                  const int *path_n, const int *valid, int cap,
+                                                  int32_t *cells, int32_t *slot_of, int32_t *labels,
+                                                  int *count, int cap_rows)
+{
+    const int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= n)
+        return;
+    const int slot = slots[k];
+    const Inst &I = insts[slot];
+    if (!valid[k] || !states[slot].goal_reached)
+        return;
+    const float *p = paths + (long)k * cap * 3;
+    const int m = path_n[k];
+    for (int i = 1 + lane; i <= m - 3; i += 32) {
+        const int cx = (int)p[3 * i], cz = (int)p[3 * i + 1];
+        const int px = (int)p[3 * (i - 1)], pz = (int)p[3 * (i - 1) + 1];
+        const int child = cz * I.W + cx;
+        const int row = atomicAdd(count, 1);
+        if (row >= cap_rows)
+            continue;
+        cells[row] = pz * I.W + px;
+        slot_of[row] = slot;
+        labels[row] = proposal_bin(I.exp_steer[child], I.exp_len[child], (float)I.max_steer, I.max_path);
+    }
+}
+
+void launch_log_paths(const Inst *d_inst, const State *d_state, const int *d_slots, int n,
+                      const float *d_paths, const int *d_path_n, const int *d_valid, int cap,
+                      int32_t *cells, int32_t *slot_of, int32_t *labels, int *count, int cap_rows,
+                      cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_log_list<<<(n * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_state, d_slots, n, d_paths, d_path_n,
+                                                      d_valid, cap, cells, slot_of, labels, count,
+                                                      cap_rows);
 }
 
 __global__ void k_fill_int(int *v, int n, int value)

@@ -64,10 +64,14 @@ void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, 
 // one planning iteration (loop()) over all active slots; with `ev` (an array
 // of kIterKernels + 1 events) an event is recorded before each kernel and
 // after the last one
-constexpr int kIterKernels = 16;
+constexpr int kIterKernels = 17;
 extern const char *const kIterKernelNames[kIterKernels];
+struct ProposalBufs;
+// with `pb`, candidates of slots that use the learned proposal get their
+// (steering, length) from the network before the expansion
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
-                      const Launch &L, cudaStream_t st, cudaEvent_t *ev = nullptr);
+                      const Launch &L, cudaStream_t st, cudaEvent_t *ev = nullptr,
+                      const ProposalBufs *pb = nullptr);
 // standalone goal check (checkGoalReached) for listed slots
 void launch_goal_check(const Inst *d_inst, State *d_state, const int *d_slots, int n,
                        int max_cells, cudaStream_t st);
@@ -83,6 +87,12 @@ void launch_optimize(const Inst *d_inst, int slot, int cells, float *d_path, int
 void launch_validate(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_cells,
                      const float *d_paths, const int *d_path_n, int cap, unsigned *d_counts,
                      int *d_valid, float *d_length, cudaStream_t st);
+// training rows (parent cell, slot, label) of the valid paths of the last
+// extraction, appended through *count (at most cap_rows)
+void launch_log_paths(const Inst *d_inst, const State *d_state, const int *d_slots, int n,
+                      const float *d_paths, const int *d_path_n, const int *d_valid, int cap,
+                      int32_t *cells, int32_t *slot_of, int32_t *labels, int *count, int cap_rows,
+                      cudaStream_t st);
 // count cells of `type` (type < 0: all non-NULL) for listed slots into d_out[k]
 void launch_count(const Inst *d_inst, const int *d_slots, int n, int max_cells, int type,
                   unsigned *d_out, cudaStream_t st);

@@ -219,10 +219,12 @@ __global__ void k_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, con
 
 // one warp per candidate; lanes over the 1024 patch samples
 __global__ void k_features(const Inst *insts, const int32_t *cells, const int32_t *slot_of, int n,
-                           __nv_bfloat16 *X)
+                           __nv_bfloat16 *X, const int *d_count)
 {
     const int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
+    if (d_count && *d_count < n)
+        n = *d_count;
     if (k >= n)
         return;
     const Inst &I = insts[slot_of[k]];
@@ -305,11 +307,47 @@ void launch_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int
 }
 
 void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *slot_of, int n,
-                     __nv_bfloat16 *X, cudaStream_t st)
+                     __nv_bfloat16 *X, cudaStream_t st, const int *d_count)
 {
     if (n <= 0)
         return;
-    k_features<<<(n * 32 + 255) / 256, 256, 0, st>>>(d_inst, cells, slot_of, n, X);
+    k_features<<<(n * 32 + 255) / 256, 256, 0, st>>>(d_inst, cells, slot_of, n, X, d_count);
+}
+
+void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
+                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st)
+{
+    GemmArgs g{};
+    g.M = n;
+    g.dM = d_count;
+    g.N = kMlpHidden;
+    g.K = kMlpInPad;
+    g.A = X;
+    g.lda = kMlpInPad;
+    g.B = w.w1;
+    g.ldb = kMlpInPad;
+    g.bias = w.b1;
+    g.relu = 1;
+    g.cb = h1;
+    g.ldc = kMlpHidden;
+    launch_gemm(g, st);
+    g.K = kMlpHidden;
+    g.A = h1;
+    g.lda = kMlpHidden;
+    g.B = w.w2;
+    g.ldb = kMlpHidden;
+    g.bias = w.b2;
+    g.cb = h2;
+    launch_gemm(g, st);
+    g.N = kMlpOut;
+    g.A = h2;
+    g.B = w.w3;
+    g.bias = w.b3;
+    g.relu = 0;
+    g.cb = nullptr;
+    g.cf = logits;
+    g.ldc = kMlpOut;
+    launch_gemm(g, st);
 }
 
 }  // namespace frrt

@@ -63,13 +63,29 @@ void launch_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n, cudaStream_
 void launch_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int32_t *idx, int n,
                         __nv_bfloat16 *Xb, int32_t *lb, cudaStream_t st);
 
+// the network's forward pass: logits (n x 128, f32) of X (n x kMlpInPad);
+// d_count, when given, caps n on the device
+void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
+                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st);
+
+// Buffers of the proposal step inside a planning iteration (cap rows).
+struct ProposalBufs {
+    int cap;                   // candidates the network proposes for per iteration
+    float mix;                 // probability of sampling from the network (else uniform)
+    int32_t *cells, *slot_of, *idx;
+    int *count;                // candidates listed this iteration (may exceed cap)
+    __nv_bfloat16 *X, *h1, *h2;
+    float *logits;
+    MlpWeights w;
+};
+
 // Features of expansion candidates: for candidate k of the listed ones, the
 // 32 x 32 obstacle patch around its parent cell in the parent's heading frame
 // (stride 2 px, forward = heading), the goal in that frame, the distance to
 // the goal, sin / cos of the heading and the steering limit; bf16, rows of
 // kMlpInPad (zero padded).  cells[k] / slots[k] name the parent.
 void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *slot_of, int n,
-                     __nv_bfloat16 *X, cudaStream_t st);
+                     __nv_bfloat16 *X, cudaStream_t st, const int *d_count = nullptr);
 
 // The (steering, length) bin of a draw, the training label
 __host__ __device__ inline int proposal_bin(float steer, float len, float max_steer, float max_path)

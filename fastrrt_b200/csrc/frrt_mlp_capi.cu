@@ -121,37 +121,7 @@ MlpWeights Mlp::weights() const
 void Mlp::forward(const __nv_bfloat16 *X, int n, cudaStream_t st, float *logits,
                   __nv_bfloat16 *h1, __nv_bfloat16 *h2, const int *d_count) const
 {
-    GemmArgs g{};
-    g.M = n;
-    g.dM = d_count;
-    g.N = kMlpHidden;
-    g.K = kMlpInPad;
-    g.A = X;
-    g.lda = kMlpInPad;
-    g.B = w16_[0];
-    g.ldb = kMlpInPad;
-    g.bias = w_[1];
-    g.relu = 1;
-    g.cb = h1;
-    g.ldc = kMlpHidden;
-    launch_gemm(g, st);
-    g.K = kMlpHidden;
-    g.A = h1;
-    g.lda = kMlpHidden;
-    g.B = w16_[1];
-    g.ldb = kMlpHidden;
-    g.bias = w_[3];
-    g.cb = h2;
-    launch_gemm(g, st);
-    g.N = kMlpOut;
-    g.A = h2;
-    g.B = w16_[2];
-    g.bias = w_[5];
-    g.relu = 0;
-    g.cb = nullptr;
-    g.cf = logits;
-    g.ldc = kMlpOut;
-    launch_gemm(g, st);
+    launch_mlp_forward(weights(), X, n, d_count, h1, h2, logits, st);
 }
 
 // forward + backward of a batch in x_ / labels_; gradients into g_

@@ -25,9 +25,12 @@ class Candidates:
         self._h = h
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib._lib is not None:
-            _lib.lib().fastrrt_candidates_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None) and _lib._lib is not None:
+                _lib.lib().fastrrt_candidates_destroy(self._h)
+                self._h = None
+        except (AttributeError, TypeError):
+            pass  # interpreter shutdown
 
     def kinematic(self, sx, sz, steer, length, velocity):
         n = len(sx)

@@ -25,9 +25,12 @@ class ProposalNet:
         self.max_batch = max_batch
 
     def __del__(self):
-        if getattr(self, "_h", None) and _lib._lib is not None:
-            _lib.lib().fastrrt_mlp_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None) and _lib._lib is not None:
+                _lib.lib().fastrrt_mlp_destroy(self._h)
+                self._h = None
+        except (AttributeError, TypeError):
+            pass  # interpreter shutdown
 
     @property
     def handle(self):
@@ -68,3 +71,58 @@ class ProposalNet:
                                                 int(epochs), int(batch), float(lr), int(seed),
                                                 C.byref(loss)), "mlp_train")
         return loss.value
+
+
+def collect_dataset(n_plans, seed0=500_000, max_rows=200_000, slots=256, max_iterations=100,
+                    sizes=(128, 256, 512)):
+    """Training rows from the planner's own solves of seeded batched requests
+    (mixed frame sizes, 5-30% obstacles): one row per expansion on every
+    validated path.  Returns device tensors (X: rows x 1040 bf16, labels:
+    int32) and the number of plans solved."""
+    import torch
+
+    from . import synth
+    from .batch import BatchPlanner, make_request
+    size_max = max(sizes)
+    planner = BatchPlanner(slots, size_max, size_max)
+    X = torch.zeros((max_rows, N_IN_PAD), dtype=torch.bfloat16, device="cuda")
+    labels = torch.zeros(max_rows, dtype=torch.int32, device="cuda")
+    rows = solved = 0
+    for b0 in range(0, n_plans, slots):
+        reqs = []
+        for k in range(b0, min(n_plans, b0 + slots)):
+            cls, start, goal, steer, _ = synth.batch_request(seed0 + k, sizes=sizes)
+            reqs.append(make_request(cls, synth.CLASS_COSTS, start, goal, max_steering_deg=steer,
+                                     seed=seed0 + k, max_iterations=max_iterations))
+        valid, _, _, _ = planner.plan(reqs, max_launches=max_iterations + 8, check_every=4)
+        solved += int(valid.sum())
+        rows += planner.log_paths(X, labels, rows, max_rows)
+        if rows >= max_rows:
+            break
+    return X[:rows], labels[:rows], solved
+
+
+def evaluate(net, n_plans, seed0, mix=0.5, slots=256, max_iterations=60, sizes=(128, 256, 512)):
+    """Solve seeded requests with and without the network attached; returns
+    per-request validity and loop counts for both."""
+    from . import synth
+    from .batch import BatchPlanner, make_request
+    size_max = max(sizes)
+    out = {}
+    for name, use in (("uniform", False), ("learned", True)):
+        planner = BatchPlanner(slots, size_max, size_max)
+        if use:
+            planner.set_proposal(net, mix=mix)
+        valid, loops = [], []
+        for b0 in range(0, n_plans, slots):
+            reqs = []
+            for k in range(b0, min(n_plans, b0 + slots)):
+                cls, start, goal, steer, _ = synth.batch_request(seed0 + k, sizes=sizes)
+                reqs.append(make_request(cls, synth.CLASS_COSTS, start, goal, max_steering_deg=steer,
+                                         seed=seed0 + k, max_iterations=max_iterations))
+            v, _, _, _ = planner.plan(reqs, max_launches=max_iterations + 8, check_every=4)
+            _, _, lp = planner.status()
+            valid.extend(v.tolist())
+            loops.extend(lp[:len(reqs)].tolist())
+        out[name] = {"valid": np.array(valid), "loops": np.array(loops)}
+    return out

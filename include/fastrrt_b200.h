@@ -266,6 +266,20 @@ int fastrrt_mlp_forward(void *mlp, int n, const float *X, float *logits);
 /* mean cross-entropy gradients of a host batch (labels in 0..127) */
 int fastrrt_mlp_gradients(void *mlp, int n, const float *X, const int32_t *labels, float *gw1,
                           float *gb1, float *gw2, float *gb2, float *gw3, float *gb3, float *loss);
+/* Planner side.  With a network attached, each iteration lists up to cap
+ * expansion candidates, computes their features and logits, and with
+ * probability mix samples the (steering, length) of a candidate from the
+ * network's softmax (the value uniform inside the bin); otherwise, and for
+ * candidates beyond cap, the uniform draw of the reference.  The
+ * kinematic and collision checks judge every expansion as before.
+ * mlp == NULL detaches. */
+int fastrrt_batch_set_proposal(void *batch, void *mlp, float mix, int cap);
+/* After fastrrt_batch_collect / fastrrt_batch_plan: training rows of the
+ * valid paths of that list, one per expansion on a path (features of the
+ * parent, label = the bin of the draw that made the child), written at rows
+ * offset.. of the device arrays X_bf16 (rows of 1040 bf16) and labels (int32),
+ * at most cap rows in all.  Returns the rows written. */
+int fastrrt_batch_log_paths(void *batch, void *X_bf16, int32_t *labels, int offset, int cap);
 /* Adam training on a device dataset: X_bf16 n x 1040 bf16 rows, labels n
  * int32 (device pointers); *last_loss = mean loss of the last batch */
 int fastrrt_mlp_train(void *mlp, const void *X_bf16, const int32_t *labels, int n, int epochs,
