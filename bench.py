@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--check-every", type=int, default=2)
     ap.add_argument("--rates", default="200,1000,5000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--rate-requests", type=int, default=600)
+    ap.add_argument("--mix", type=float, default=0.8, help="learned-proposal sampling probability")
+    ap.add_argument("--candidates", type=int, default=1 << 20, help="per-candidate microbench size")
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", type=int, default=16, help="plans of the plain single-instance loop")
@@ -267,6 +269,67 @@ def plain_loop(n, rank):
                     "the 100 ms timeout, per plan through the reference API, host wall clock"}
 
 
+def candidate_microbench(n, cpu=True):
+    """Per-candidate kernels on 256x256 C0-generator frames at 5/15/30%
+    obstacles: n kinematic candidates (parent uniform, heading U(-pi, pi),
+    steering U(-40, 40) deg, length U(5, 40) px) and 65,536 Hermite pairs of
+    64 samples, through the device entry points (device clock, synchronised);
+    the CPU restatement on a bounded sample beside them."""
+    import torch
+
+    import fastrrt_b200 as F
+    from fastrrt_b200 import synth
+    from oracle import oracle as O
+    res = {}
+    ms = math.radians(40.0)
+    for cov in (0.05, 0.15, 0.30):
+        cls = synth.make_frame(11, SIZE, coverage=cov)
+        heading, sx, sz, steer, seg = synth.candidates(n, SIZE, SIZE, 1)
+        fr = F.SearchFrame(class_ids=cls, class_costs=synth.CLASS_COSTS)
+        ctx = F.Candidates(fr, min_dist=(22, 40), max_steering_rad=ms, lr_m=2.7, heading_grid=heading)
+        d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (sx, sz, steer, seg)]
+        out = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+        pr = torch.zeros(1, dtype=torch.int64, device="cuda")
+        ctx.kinematic_device(*d, 2.0, out, pr)
+        torch.cuda.synchronize()
+        reps = 3
+        pr.zero_()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ctx.kinematic_device(*d, 2.0, out, pr)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / reps
+        entry = {"candidates_per_s": n / dt, "reference_probes_per_s": float(pr.item()) / reps / dt,
+                 "feasible_fraction": float((out[:, 0] >= 0).float().mean().item())}
+        if cpu:
+            m = min(n, 20000)
+            g = O.Graph(SIZE, SIZE, SIZE * M_PER_PX, SIZE * M_PER_PX, 40.0, 5.4, -1.0, (22, 40))
+            g.g.pp.lr, g.g.pp.max_steer_rad = 2.7, ms
+            g.heading[:] = heading
+            t0 = time.perf_counter()
+            g.kinematic_batch(O.Frame(cls, synth.CLASS_COSTS), sx[:m], sz[:m], steer[:m], seg[:m], 2.0)
+            entry["cpu_candidates_per_s"] = m / (time.perf_counter() - t0)
+            entry["cpu_cores"] = os.cpu_count()
+        res[f"kinematic_{int(cov * 100)}pct"] = entry
+    cls = synth.make_frame(11, SIZE, coverage=0.15)
+    x, z, lh, gx, gz, gh = synth.hermite_pairs(65536, SIZE, SIZE, 5, num_points=64)
+    fr = F.SearchFrame(class_ids=cls, class_costs=synth.CLASS_COSTS)
+    ctx = F.Candidates(fr, min_dist=(22, 40), max_steering_rad=ms, lr_m=2.7)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (x, z, lh, gx, gz, gh)]
+    out = torch.zeros(65536, dtype=torch.float32, device="cuda")
+    pr = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ctx.hermite_device(*d, 0.8, out, pr)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        ctx.hermite_device(*d, 0.8, out, pr)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / 3
+    res["hermite_64_samples"] = {"pairs_per_s": 65536 / dt,
+                                 "connected_fraction": float((out >= 0).float().mean().item())}
+    return res
+
+
 def pct(a, q):
     return float(np.percentile(a, q)) if len(a) else None
 
@@ -361,6 +424,29 @@ def run_mine(args, rank, world, local):
             "success_rate": float(v.mean()),
             "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
 
+    # the same served workload with the learned expansion proposal attached
+    learned = None
+    from fastrrt_b200 import proposal as P
+    from fastrrt_b200 import train_proposal as TP
+    net = P.ProposalNet(seed=0, max_batch=512)
+    if TP.load(net):
+        planner.set_proposal(net, mix=args.mix)
+        serve(reqs_dev[0])
+        l_ms, l_valid, l_service = 0.0, 0, []
+        for s in range(args.warmup, total_steps):
+            out = serve(reqs_dev[s])
+            l_ms += out["device_ms"]
+            v = out["valid"] > 0
+            l_valid += int(v.sum())
+            l_service.extend(out["service_ms"][v].tolist())
+        planner.set_proposal(None)
+        l_t = max_over_ranks(l_ms, world)
+        learned = {"value": sum_over_ranks(l_valid, world) / (l_t / 1e3), "unit": "plans/s",
+                   "mix": args.mix, "success_rate": l_valid / float(R * args.steps),
+                   "service_p50_ms": pct(l_service, 50), "service_p99_ms": pct(l_service, 99),
+                   "note": "same requests, network weights trained on the planner's own solves of "
+                           "held-out mixed-size requests (fastrrt_b200/train_proposal.py)"}
+
     # kernel timing replay of one step (same inputs, kernels launched one by one)
     planner.profile(True)
     serve(reqs_dev[args.warmup])
@@ -384,6 +470,7 @@ def run_mine(args, rank, world, local):
     if rank == 0:
         plain = plain_loop(args.plain, rank)
         cpu = None if args.no_cpu_baseline else cpu_baseline()
+        micro = candidate_microbench(args.candidates, cpu=not args.no_cpu_baseline)
         line = {
             "metric": METRIC, "value": value, "unit": "plans/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -401,6 +488,8 @@ def run_mine(args, rank, world, local):
             "mean_loops": float(np.mean(loops)) if loops else None,
             "mean_path_len_px": float(np.mean(lengths)) if lengths else None,
             "serving": serving,
+            "learned_proposal": learned,
+            "candidate_kernels": micro,
             "plain_gpu_loop": plain,
             "served_over_plain": value / plain["plans_per_s"] if plain["plans_per_s"] else None,
             "e2e": {"value": e2e_plans / (e2e_t / 1e3), "unit": "plans/s",
