@@ -57,8 +57,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--requests", type=int, default=1024, help="requests per step and GPU")
-    ap.add_argument("--slots", type=int, default=512, help="planning slots per GPU")
-    ap.add_argument("--check-every", type=int, default=2)
+    ap.add_argument("--slots", type=int, default=None,
+                    help="planning slots per GPU (default: the autotuned value, else 512)")
+    ap.add_argument("--check-every", type=int, default=None,
+                    help="graph launches between harvests (default: autotuned, else 2)")
     ap.add_argument("--rates", default="200,1000,5000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--rate-requests", type=int, default=600)
     ap.add_argument("--mix", type=float, default=0.8, help="learned-proposal sampling probability")
@@ -338,15 +340,24 @@ def run_mine(args, rank, world, local):
     import torch
 
     import fastrrt_b200 as F
-    from fastrrt_b200 import synth
+    from fastrrt_b200 import autotune, synth
     F._lib.require_cuda()
     torch.cuda.set_device(local)
+    tuned = autotune.load()
+    if tuned and args.slots is None:
+        args.slots = tuned["slots"]
+    if tuned and args.check_every is None:
+        args.check_every = tuned["check_every"]
+    args.slots = args.slots or 512
+    args.check_every = args.check_every or 2
     R = args.requests
     total_steps = args.warmup + args.steps
     t_gen = time.time()
     work = [workload(rank, s, R) for s in range(total_steps)]
     gen_s = time.time() - t_gen
     planner = F.BatchPlanner(args.slots, SIZE, SIZE)
+    if tuned:
+        planner.set_launch(tuned["sweep_blocks_per_sm"], tuned["work_blocks_per_sm"])
     costs = synth.CLASS_COSTS
 
     def requests(frames, starts, goals, seeds, device_frames=None):
@@ -480,6 +491,9 @@ def run_mine(args, rank, world, local):
                                    f"frames per step and GPU, continuous batching over "
                                    f"{args.slots} slots, {TIMEOUT_MS} ms timeout per request",
                        "requests_per_step_per_gpu": R, "slots_per_gpu": args.slots,
+                       "check_every": args.check_every,
+                       "launch_shape": ({k: tuned[k] for k in ("sweep_blocks_per_sm", "work_blocks_per_sm")}
+                                        if tuned else "default"),
                        "frame": f"{SIZE}x{SIZE} @ {M_PER_PX} m/px",
                        "parallelism": f"request sharding x{world}",
                        "l2": "fresh frames every step; per-step working set > L2"},

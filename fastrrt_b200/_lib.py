@@ -61,7 +61,7 @@ EXPORTS = [
     # learned expansion proposal
     "fastrrt_mlp_create", "fastrrt_mlp_destroy", "fastrrt_mlp_get_weights",
     "fastrrt_mlp_set_weights", "fastrrt_mlp_forward", "fastrrt_mlp_gradients", "fastrrt_mlp_train",
-    "fastrrt_batch_set_proposal", "fastrrt_batch_log_paths",
+    "fastrrt_batch_set_proposal", "fastrrt_batch_log_paths", "fastrrt_batch_set_launch",
 ]
 
 
@@ -155,6 +155,7 @@ def lib():
         "fastrrt_mlp_train": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64,
                                         P(C.c_float)]),
         "fastrrt_batch_set_proposal": (C.c_int, [vp, vp, C.c_float, C.c_int]),
+        "fastrrt_batch_set_launch": (C.c_int, [vp, C.c_int, C.c_int]),
         "fastrrt_batch_log_paths": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
         "fastrrt_batch_serve": (C.c_int, [vp, C.c_int, P(Request), vp, C.c_int, C.c_int, i32p, f32p,
                                           f32p, f32p, i32p, P(C.c_double), P(C.c_float)]),

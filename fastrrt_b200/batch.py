@@ -152,6 +152,10 @@ class BatchPlanner:
         out["device_ms"] = dev.value
         return out
 
+    def set_launch(self, sweep_blocks_per_sm=8, work_blocks_per_sm=2):
+        _lib.check(_lib.lib().fastrrt_batch_set_launch(self._h, int(sweep_blocks_per_sm),
+                                                       int(work_blocks_per_sm)), "batch_set_launch")
+
     def set_proposal(self, net, mix=0.5, cap=131072):
         """attach a ProposalNet (None detaches): each candidate's expansion is
         sampled from the network with probability mix, uniformly otherwise"""

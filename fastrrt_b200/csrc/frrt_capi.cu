@@ -1130,6 +1130,16 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
     return good;
 }
 
+int fastrrt_batch_set_launch(void *batch, int sweep_blocks_per_sm, int work_blocks_per_sm)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b) {
+        set_error("batch set_launch: bad arguments");
+        return -1;
+    }
+    return b->eng->set_launch(sweep_blocks_per_sm, work_blocks_per_sm) ? 0 : -1;
+}
+
 int fastrrt_batch_set_proposal(void *batch, void *mlp, float mix, int cap)
 {
     auto *b = static_cast<Batch *>(batch);

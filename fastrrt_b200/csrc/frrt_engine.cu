@@ -250,8 +250,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
         if (!check(cudaGetLastError(), "kernel attributes"))
             return;
     }
-    L_.work_blocks = sms * 2;
-    L_.sweep_blocks = sms * 8;
+    L_.work_blocks = sms * work_per_sm_;
+    L_.sweep_blocks = sms * sweep_per_sm_;
     ok_ = true;
     ok_ = commit();
 }
@@ -438,7 +438,7 @@ bool Engine::commit()
     h_sched_.gd_start = d_sched_arrays_ + 3 * (n_slots_ + 1);
     h_sched_.goal_start = d_sched_arrays_ + 4 * (n_slots_ + 1);
     h_sched_.grab = d_grab_;
-    const int sweep_blocks = std::max(1, std::min(L_.sms * 8, run));
+    const int sweep_blocks = std::max(1, std::min(L_.sms * sweep_per_sm_, run));
     if (sweep_blocks != L_.sweep_blocks) {
         L_.sweep_blocks = sweep_blocks;
         if (graph_exec_) {
@@ -783,6 +783,28 @@ bool Engine::grid_upload(int slot, const std::vector<int8_t> &type, const std::v
     if (ok)
         ok = set_intrinsic(slot, any_intr ? intrinsic.data() : nullptr);
     return ok && commit();
+}
+
+bool Engine::set_launch(int sweep_per_sm, int work_per_sm)
+{
+    if (sweep_per_sm < 1 || sweep_per_sm > 64 || work_per_sm < 1 || work_per_sm > 8) {
+        set_error("launch shape out of range (sweep 1..64, work 1..8 blocks per SM)");
+        return false;
+    }
+    sweep_per_sm_ = sweep_per_sm;
+    work_per_sm_ = work_per_sm;
+    L_.work_blocks = L_.sms * work_per_sm;
+    L_.sweep_blocks = -1;  // recomputed (and the graph recaptured) by commit()
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    if (graph_) {
+        cudaGraphDestroy(graph_);
+        graph_ = nullptr;
+    }
+    dirty_ = true;
+    return commit();
 }
 
 bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)

@@ -140,6 +140,9 @@ public:
     // learned expansion proposal: network weights (device), the probability
     // of sampling from it, rows per iteration; w == nullptr detaches it
     bool set_proposal(const MlpWeights *w, float mix, int cap);
+    // launch shape: blocks per SM of the sweep kernels and of the persistent
+    // expansion kernel (the autotuner's knobs)
+    bool set_launch(int sweep_per_sm, int work_per_sm);
     // training rows of the last extracted list: for each valid path, one row
     // per expansion on it (features of the parent, the bin of the draw that
     // made the child) appended at X[offset..], labels[offset..] (device, at
@@ -165,6 +168,7 @@ public:
 
 private:
     ProposalBufs pb_{};
+    int sweep_per_sm_ = 8, work_per_sm_ = 2;
     bool use_proposal_ = false;
     int32_t *d_log_cells_ = nullptr, *d_log_slots_ = nullptr;
     int *d_log_count_ = nullptr;

@@ -233,6 +233,10 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                         int timeout_ms, int check_every, int32_t *valid, float *length,
                         float *latency_ms, float *service_ms, int32_t *loops, double *wall_ms,
                         float *device_ms);
+/* launch shape of the iteration: blocks per SM of the sweep kernels (1..64,
+ * default 8) and of the persistent expansion kernel (1..8, default 2); the
+ * autotuner (fastrrt_b200/autotune.py) picks them */
+int fastrrt_batch_set_launch(void *batch, int sweep_blocks_per_sm, int work_blocks_per_sm);
 /* kernel timing mode (1 = on): iterations launch kernels one by one between
  * CUDA events instead of replaying the CUDA graph */
 int fastrrt_batch_profile(void *batch, int on);
@@ -271,7 +275,7 @@ int fastrrt_mlp_gradients(void *mlp, int n, const float *X, const int32_t *label
  * probability mix samples the (steering, length) of a candidate from the
  * network's softmax (the value uniform inside the bin); otherwise, and for
  * candidates beyond cap, the uniform draw of the reference.  The
- * kinematic and collision checks judge every expansion as before.
+ * kinematic and collision checks decide every expansion as before.
  * mlp == NULL detaches. */
 int fastrrt_batch_set_proposal(void *batch, void *mlp, float mix, int cap);
 /* After fastrrt_batch_collect / fastrrt_batch_plan: training rows of the
