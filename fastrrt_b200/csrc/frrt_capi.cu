@@ -1093,7 +1093,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                 list.push_back(s);
         if (list.empty())
             continue;
-        if (!e.extract_and_validate(list, 1024))
+        if (!e.extract_and_validate(list, 1024, false))
             return -1;
         for (size_t k = 0; k < list.size(); k++) {
             const int s = list[k];

@@ -231,6 +231,8 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMalloc(&d_bad_, sizeof(int)), "flag") &&
               check(cudaMalloc(&d_clock_, sizeof(long long)), "clock") &&
               check(cudaMallocHost(&h_small_, sizeof(int) * 64), "pinned scratch") &&
+              check(cudaMallocHost(&h_costs_pin_, sizeof(float) * kMaxClasses * n_slots), "pinned costs") &&
+              check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "staging event") &&
               check(cudaMalloc(&d_newcost_, sizeof(float) * kOptCap * kOptCap), "optimize scratch") &&
               check(cudaMalloc(&d_changed_, sizeof(int)), "optimize flag") &&
               check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 5 * (n_slots + 1), stream_), "sched init") &&
@@ -289,6 +291,12 @@ Engine::~Engine()
     cudaFree(d_log_count_);
     if (h_small_)
         cudaFreeHost(h_small_);
+    if (h_costs_pin_)
+        cudaFreeHost(h_costs_pin_);
+    if (h_stage_)
+        cudaFreeHost(h_stage_);
+    if (stage_ev_)
+        cudaEventDestroy(stage_ev_);
     cudaFree(d_paths_);
     cudaFree(d_path_n_);
     cudaFree(d_keys_);
@@ -366,9 +374,11 @@ bool Engine::copy_frame(int slot, int W, int H, const uint8_t *cls, const float 
                                  cls_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                  stream_),
                  "frame upload") &&
-           check(cudaMemcpyAsync(d_class_costs_ + (size_t)slot * kMaxClasses, costs_host,
-                                 sizeof(float) * n_classes, cudaMemcpyHostToDevice, stream_),
-                 "class costs");
+           (memcpy(h_costs_pin_ + (size_t)slot * kMaxClasses, costs_host, sizeof(float) * n_classes),
+            check(cudaMemcpyAsync(d_class_costs_ + (size_t)slot * kMaxClasses,
+                                  h_costs_pin_ + (size_t)slot * kMaxClasses, sizeof(float) * n_classes,
+                                  cudaMemcpyHostToDevice, stream_),
+                  "class costs"));
 }
 
 void Engine::set_request(int slot, const PlanRequest &r)
@@ -418,11 +428,7 @@ bool Engine::commit()
 {
     if (!ok_)
         return false;
-    if (!check(cudaMemcpyAsync(d_inst_, h_inst_.data(), sizeof(Inst) * n_slots_,
-                               cudaMemcpyHostToDevice, stream_),
-               "inst upload"))
-        return false;
-    std::vector<int> arrays(5 * (n_slots_ + 1), 0);
+    std::vector<int> arrays(n_slots_ + 1, 0);
     int run = 0;
     for (int s = 0; s < n_slots_; s++) {
         arrays[s] = run;
@@ -450,12 +456,33 @@ bool Engine::commit()
             graph_ = nullptr;
         }
     }
-    bool ok = check(cudaMemcpyAsync(d_sched_arrays_, arrays.data(), sizeof(int) * (n_slots_ + 1),
-                                    cudaMemcpyHostToDevice, stream_),
-                    "sched upload") &&
-              check(cudaMemcpyAsync(d_sched_, &h_sched_, sizeof(Sched), cudaMemcpyHostToDevice, stream_),
-                    "sched upload") &&
-              check(cudaStreamSynchronize(stream_), "commit sync");
+    // stage the three tables in pinned memory (the previous upload from it
+    // has to be done first) and upload them without waiting for the stream
+    const size_t inst_b = sizeof(Inst) * n_slots_, arr_b = sizeof(int) * (n_slots_ + 1);
+    const size_t need = inst_b + arr_b + sizeof(Sched);
+    if (need > stage_bytes_) {
+        if (h_stage_ && !check(cudaEventSynchronize(stage_ev_), "staging wait"))
+            return false;
+        if (h_stage_)
+            cudaFreeHost(h_stage_);
+        h_stage_ = nullptr;
+        if (!check(cudaMallocHost(&h_stage_, need), "pinned staging"))
+            return false;
+        stage_bytes_ = need;
+    } else if (!check(cudaEventSynchronize(stage_ev_), "staging wait")) {
+        return false;
+    }
+    memcpy(h_stage_, h_inst_.data(), inst_b);
+    memcpy(h_stage_ + inst_b, arrays.data(), arr_b);
+    memcpy(h_stage_ + inst_b + arr_b, &h_sched_, sizeof(Sched));
+    const bool ok =
+        check(cudaMemcpyAsync(d_inst_, h_stage_, inst_b, cudaMemcpyHostToDevice, stream_), "inst upload") &&
+        check(cudaMemcpyAsync(d_sched_arrays_, h_stage_ + inst_b, arr_b, cudaMemcpyHostToDevice, stream_),
+              "sched upload") &&
+        check(cudaMemcpyAsync(d_sched_, h_stage_ + inst_b + arr_b, sizeof(Sched), cudaMemcpyHostToDevice,
+                              stream_),
+              "sched upload") &&
+        check(cudaEventRecord(stage_ev_, stream_), "staging event");
     dirty_ = !ok;
     return ok;
 }
@@ -633,7 +660,7 @@ int Engine::count(int slot, int type)
     return h_small_[0];
 }
 
-bool Engine::extract_and_validate(const std::vector<int> &slots, int cap)
+bool Engine::extract_and_validate(const std::vector<int> &slots, int cap, bool copy_paths)
 {
     const int n = (int)slots.size();
     if (cap > cap_ || !d_paths_) {
@@ -666,7 +693,8 @@ bool Engine::extract_and_validate(const std::vector<int> &slots, int cap)
     h_path_n_.resize(n);
     h_valid_.resize(n);
     h_length_.resize(n);
-    h_paths_.resize((size_t)3 * cap_ * n);
+    if (copy_paths)
+        h_paths_.resize((size_t)3 * cap_ * n);
     return check(cudaGetLastError(), "extract launch") &&
            check(cudaMemcpyAsync(h_path_n_.data(), d_path_n_, sizeof(int) * n, cudaMemcpyDeviceToHost,
                                  stream_), "path counts") &&
@@ -674,8 +702,9 @@ bool Engine::extract_and_validate(const std::vector<int> &slots, int cap)
                                  stream_), "valid flags") &&
            check(cudaMemcpyAsync(h_length_.data(), d_length_, sizeof(float) * n, cudaMemcpyDeviceToHost,
                                  stream_), "lengths") &&
-           check(cudaMemcpyAsync(h_paths_.data(), d_paths_, sizeof(float) * 3 * (size_t)cap_ * n,
-                                 cudaMemcpyDeviceToHost, stream_), "paths") &&
+           (!copy_paths ||
+            check(cudaMemcpyAsync(h_paths_.data(), d_paths_, sizeof(float) * 3 * (size_t)cap_ * n,
+                                  cudaMemcpyDeviceToHost, stream_), "paths")) &&
            sync();
 }
 

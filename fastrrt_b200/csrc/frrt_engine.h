@@ -136,7 +136,9 @@ public:
     bool clear_goal_flag(int slot);
 
     // batched extraction + validation of listed slots
-    bool extract_and_validate(const std::vector<int> &slots, int cap);
+    // copy_paths = false leaves the paths on the device (counts, validity and
+    // lengths still come to the host)
+    bool extract_and_validate(const std::vector<int> &slots, int cap, bool copy_paths = true);
     // learned expansion proposal: network weights (device), the probability
     // of sampling from it, rows per iteration; w == nullptr detaches it
     bool set_proposal(const MlpWeights *w, float mix, int cap);
@@ -190,6 +192,12 @@ private:
     State *d_state_ = nullptr;
     State *h_state_ = nullptr;  // pinned
     Sched h_sched_{};
+    // pinned staging of the tables commit() uploads and of class costs, so
+    // the uploads do not wait for the stream (pageable copies would)
+    unsigned char *h_stage_ = nullptr;
+    size_t stage_bytes_ = 0;
+    cudaEvent_t stage_ev_ = nullptr;
+    float *h_costs_pin_ = nullptr;
     Sched *d_sched_ = nullptr;
     int *d_sched_arrays_ = nullptr;
     unsigned *d_grab_ = nullptr;

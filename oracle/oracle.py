@@ -365,6 +365,7 @@ class Planner:
         self.px = np.ctypeslib.as_array(g.px, (n,))
         self.pz = np.ctypeslib.as_array(g.pz, (n,))
         self.child = np.ctypeslib.as_array(g.child, (n,))
+        self.intrinsic = np.ctypeslib.as_array(g.intrinsic, (n,))
         self.gd_flag = np.ctypeslib.as_array(g.gd_flag, (n,))
         self.gd_heading = np.ctypeslib.as_array(g.gd_heading, (n,))
         self.gd_cost = np.ctypeslib.as_array(g.gd_cost, (n,))

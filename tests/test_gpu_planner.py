@@ -281,3 +281,54 @@ def test_served_timeout(gpu):
     ok = gpu.make_request(cls, COSTS, start, goal, seed=3)
     out = B.serve([ok], timeout_ms=100, check_every=1)
     assert out["valid"][0] == 1
+
+
+def test_loaded_intrinsic_costs_match_oracle(gpu, dev_orc, tmp_path):
+    """A graph dump with intrinsic costs loaded mid-plan (load_graph_state):
+    the goal direct connections keep the costs of set_plan_data time, the
+    expansion and goal search use the loaded ones, and the plan continues
+    exactly like the oracle's from the same state."""
+    orc = dev_orc
+    seed = 5
+    cls, start, goal = synth.c0_request(seed)
+    p, fr = gpu_planner(gpu, cls, seed)
+    p.set_plan_data(fr, start, goal, 2.0)
+    p.search_init()
+    for _ in range(3):
+        p.loop(False)
+    assert not p.goal_reached()
+    f = str(tmp_path / "g.txt")
+    p.save_current_graph_state(f)
+    rows = np.loadtxt(f)
+    rng = np.random.default_rng(3)
+    band = np.zeros(W * H, bool)
+    band[(W * 20):(W * 120)] = True  # rows 20..119
+    rows[band, 6] = np.round(rng.uniform(0.0, 3.0, band.sum()), 3)
+    f2 = str(tmp_path / "g2.txt")
+    np.savetxt(f2, rows, fmt="%d %d %d %d %f %f %f %f")
+    q, fr2 = gpu_planner(gpu, cls, seed)
+    q.set_plan_data(fr2, start, goal, 2.0)
+    q.search_init()
+    q.load_graph_state(f2)
+    op = orc.Planner(orc.Frame(cls, COSTS), 34.56, 34.56, 40.0, 5.4)
+    op.set_plan_data(start, goal, 2.0, (22, 40), seed=seed)
+    op.search_init()
+    op.px[:] = rows[:, 0]
+    op.pz[:] = rows[:, 1]
+    op.type[:] = rows[:, 2]
+    op.child[:] = rows[:, 3]
+    op.heading[:] = rows[:, 4].astype(np.float32)
+    op.cost[:] = rows[:, 5].astype(np.float32)
+    op.intrinsic[:] = rows[:, 6].astype(np.float32)
+    op.p.contents.last_expanded = int((rows[:, 2] == 2).sum())
+    n = m = 0
+    while not q.goal_reached() and n < 60:
+        n += 1
+        q.loop(False)
+    while not op.goal_reached() and m < 60:
+        m += 1
+        op.loop(False)
+    assert n == m
+    assert np.array_equal(grid_types(q.export_graph_nodes()), op.type.reshape(H, W))
+    if q.goal_reached():
+        assert np.array_equal(q.get_planned_path_array()[:, :2], op.path()[:, :2])
