@@ -648,76 +648,6 @@ __device__ inline void stage_drain(Stage &sg, uint64_t *bar)
 
 // expand_node (graph_expansion.cu:103-145): every listed NODE cell draws a
 // steering angle and a length, integrates, and claims its end cell
-__global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states, Sched *sc,
-                                                int smem_words)
-{
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ int s_chunk;
-    const int n = sc->n_slots;
-    const int total = sc->cand_start[n];
-    Stage sg{-1, false, 0u};
-    if (threadIdx.x == 0)
-        mbar_init(&bar, 1);
-    __syncthreads();
-    while (true) {
-        if (threadIdx.x == 0)
-            s_chunk = (int)atomicAdd(&sc->grab[0], 1u);
-        __syncthreads();
-        const int c = s_chunk;
-        __syncthreads();
-        if (c >= total)
-            break;
-        const int slot = find_slot(sc->cand_start, n, c);
-        const Inst &I = insts[slot];
-        State &S = states[slot];
-        const uint32_t *blk, *clr;
-        stage_for(I, slot, sg, smem, smem_words, &bar, states, blk, clr);
-        const Foot f = foot_of(I, blk, clr);
-        const int idx = (c - sc->cand_start[slot]) * kCandChunk + threadIdx.x;
-        const bool has = idx < S.n_cand;
-        KinLane t;
-        int pos = 0;
-        unsigned long long probes = 0;
-        if (has) {
-            pos = I.cand[idx];
-            const int z = pos / I.W, x = pos - z * I.W;
-            float steer, len;
-            if (I.proposal && I.prop_row[idx] >= 0 && I.prop_len[idx] >= 0.0f) {
-                steer = I.prop_steer[idx];
-                len = I.prop_len[idx];
-            } else {
-                draw_expansion(I.seed, (uint32_t)pos, S.iter, (float)I.max_steer, I.max_path, steer,
-                               len);
-            }
-            I.cand_steer[idx] = steer;
-            I.cand_len[idx] = len;
-            t.k.init(I, x, z, steer, len, I.velocity, I.heading[pos], I.cost[pos]);
-        }
-        run_warp(t, has, f, probes, [](const KinLane &q) { return q.k.pend_x; },
-                 [](const KinLane &q) { return q.k.pend_z; });
-        if (has) {
-            int end = -1;
-            if (t.k.ok) {
-                const int ex = t.k.last_x, ez = t.k.last_z;
-                if (!(ex == I.og_x && ez == I.og_z)) {
-                    const int ep = ez * I.W + ex;
-                    if (ep != pos)
-                        end = ep;
-                }
-            }
-            I.cand_end[idx] = end;
-            I.cand_heading[idx] = t.k.heading;
-            I.cand_cost[idx] = t.k.nodeCost;
-            if (end >= 0)
-                atomicMin(&I.claim[end], pos);
-        }
-        probes = warp_sum64(probes);
-        if ((threadIdx.x & 31) == 0 && probes)
-            atomicAdd(&S.probes, probes);
-    }
-    stage_drain(sg, &bar);
-}
 
 // the winner of each claimed cell applies expand_node's transitions
 __global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states, const Sched *sc)
@@ -1111,6 +1041,110 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
             m &= m - 1;
             unsigned cnt = 0;
             const bool ok = coop_probe(f, leader, lane, t.h.last_x, t.h.last_z, t.probe_angle(), cnt);
+            if (lane == leader) {
+                ok_mine = ok;
+                probes += cnt;
+            }
+        }
+        if (need && !t.resolve(ok_mine))
+            finish();
+    }
+}
+
+// Expansion: candidates are handed to lanes one by one over all slots (the
+// padded space of 256-candidate chunks): a lane whose integration ended takes
+// the next candidate at the start of the warp's next step, so lanes stay busy
+// although path lengths differ.  Full footprint probes are answered by the
+// whole warp; masks are read through L1.
+__global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states, Sched *sc)
+{
+    const int n = sc->n_slots;
+    const int total = sc->cand_start[n] * kCandChunk;
+    const int lane = threadIdx.x & 31;
+    const unsigned lower = (1u << lane) - 1u;
+    KinLane t;
+    Foot f{};
+    const Inst *I = nullptr;
+    int slot = 0, idx = 0, pos = 0;
+    bool active = false, exhausted = false;
+    unsigned long long probes = 0;
+    auto finish = [&]() {
+        int end = -1;
+        if (t.k.ok) {
+            const int ex = t.k.last_x, ez = t.k.last_z;
+            if (!(ex == I->og_x && ez == I->og_z)) {
+                const int ep = ez * I->W + ex;
+                if (ep != pos)
+                    end = ep;
+            }
+        }
+        I->cand_end[idx] = end;
+        I->cand_heading[idx] = t.k.heading;
+        I->cand_cost[idx] = t.k.nodeCost;
+        if (end >= 0)
+            atomicMin(&I->claim[end], pos);
+        if (probes)
+            atomicAdd(&states[slot].probes, probes);
+        probes = 0;
+        active = false;
+    };
+    while (true) {
+        if (!exhausted) {
+            const unsigned idle = __ballot_sync(kFull, !active);
+            if (idle) {
+                int base = 0;
+                if (lane == 0)
+                    base = (int)atomicAdd(&sc->grab[0], (unsigned)__popc(idle));
+                base = __shfl_sync(kFull, base, 0);
+                if (base + __popc(idle) >= total)
+                    exhausted = true;
+                const int e = base + __popc(idle & lower);
+                if (!active && e < total) {
+                    const int c = e / kCandChunk;
+                    const int s = find_slot(sc->cand_start, n, c);
+                    const int k = (c - sc->cand_start[s]) * kCandChunk + (e - c * kCandChunk);
+                    if (k < states[s].n_cand) {
+                        slot = s;
+                        idx = k;
+                        I = &insts[s];
+                        f = foot_of(*I, I->blocked, I->clear);
+                        pos = I->cand[idx];
+                        const int z = pos / I->W, x = pos - z * I->W;
+                        float steer, len;
+                        if (I->proposal && I->prop_row[idx] >= 0 && I->prop_len[idx] >= 0.0f) {
+                            steer = I->prop_steer[idx];
+                            len = I->prop_len[idx];
+                        } else {
+                            draw_expansion(I->seed, (uint32_t)pos, states[s].iter, (float)I->max_steer,
+                                           I->max_path, steer, len);
+                        }
+                        I->cand_steer[idx] = steer;
+                        I->cand_len[idx] = len;
+                        t.k.init(*I, x, z, steer, len, I->velocity, I->heading[pos], I->cost[pos]);
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(kFull, active)) {
+            if (exhausted)
+                break;
+            continue;
+        }
+        bool need = false;
+        if (active) {
+            if (t.advance(f, probes))
+                need = true;
+            else
+                finish();
+        }
+        unsigned m = __ballot_sync(kFull, need);
+        bool ok_mine = true;
+        while (m) {
+            const int leader = __ffs(m) - 1;
+            m &= m - 1;
+            unsigned cnt = 0;
+            const bool ok = coop_probe(f, leader, lane, t.k.pend_x, t.k.pend_z, t.probe_angle(), cnt);
             if (lane == leader) {
                 ok_mine = ok;
                 probes += cnt;
@@ -1546,7 +1580,7 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     if (pb)
         launch_proposal(d_inst, d_state, d_sched, *pb, L, st);
     mark();
-    k_expand<<<L.work_blocks, 256, smem, st>>>(d_inst, d_state, d_sched, L.smem_words);
+    k_expand<<<L.work_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_apply<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
@@ -2220,7 +2254,6 @@ void launch_clock(long long *d_out, cudaStream_t st) { k_clock<<<1, 1, 0, st>>>(
 
 void configure_kernels(int smem_bytes)
 {
-    cudaFuncSetAttribute(k_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_candidates, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
     cudaFuncSetAttribute(k_hermite, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
 }
