@@ -942,6 +942,16 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
     }
 }
 
+// Lanes of a warp that take tasks: all 32 when there is work for every lane
+// of the grid, fewer when there is little (a warp answers its lanes' full
+// probes one after another, so a lightly loaded launch finishes sooner with
+// tasks spread over more warps); the other lanes only help with probes.
+__device__ __forceinline__ unsigned lanes_in_use(int total, int warps)
+{
+    const int per = min(32, max(1, (total + warps - 1) / max(warps, 1)));
+    return per >= 32 ? kFull : ((1u << per) - 1u);
+}
+
 // A full footprint probe for lane `leader`, answered by the whole warp; the
 // leader's footprint may belong to another slot than the other lanes' tasks.
 __device__ inline bool coop_probe(const Foot &mine, int leader, int lane, int x, int z, float angle,
@@ -982,6 +992,7 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
     const int total = sc->gd_start[n];
     const int lane = threadIdx.x & 31;
     const unsigned lower = (1u << lane) - 1u;
+    const unsigned lanes = lanes_in_use(total, gridDim.x * (blockDim.x >> 5));
     PrecompTask t;
     Foot f{};
     const Inst *I = nullptr;
@@ -1002,7 +1013,7 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
     };
     while (true) {
         if (!exhausted) {
-            const unsigned idle = __ballot_sync(kFull, !active);
+            const unsigned idle = __ballot_sync(kFull, !active) & lanes;
             if (idle) {
                 int base = 0;
                 if (lane == 0)
@@ -1011,7 +1022,7 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
                 if (base + __popc(idle) >= total)
                     exhausted = true;
                 const int e = base + __popc(idle & lower);
-                if (!active && e < total) {
+                if (((idle >> lane) & 1u) && e < total) {
                     slot = find_slot(sc->gd_start, n, e);
                     I = &insts[slot];
                     pos = I->gd_list[e - sc->gd_start[slot]];
@@ -1062,6 +1073,7 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
     const int total = sc->cand_start[n] * kCandChunk;
     const int lane = threadIdx.x & 31;
     const unsigned lower = (1u << lane) - 1u;
+    const unsigned lanes = lanes_in_use(total, gridDim.x * (blockDim.x >> 5));
     KinLane t;
     Foot f{};
     const Inst *I = nullptr;
@@ -1090,7 +1102,7 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
     };
     while (true) {
         if (!exhausted) {
-            const unsigned idle = __ballot_sync(kFull, !active);
+            const unsigned idle = __ballot_sync(kFull, !active) & lanes;
             if (idle) {
                 int base = 0;
                 if (lane == 0)
@@ -1099,7 +1111,7 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
                 if (base + __popc(idle) >= total)
                     exhausted = true;
                 const int e = base + __popc(idle & lower);
-                if (!active && e < total) {
+                if (((idle >> lane) & 1u) && e < total) {
                     const int c = e / kCandChunk;
                     const int s = find_slot(sc->cand_start, n, c);
                     const int k = (c - sc->cand_start[s]) * kCandChunk + (e - c * kCandChunk);
