@@ -280,10 +280,25 @@ __device__ inline bool rows_clear_warp(const Foot &f, int x, int z, float c, flo
 
 // ---------------------------------------------------------------------------
 // resumable per-lane tasks: advance() runs until a footprint needs a full
-// probe (returns 1) or the task ends (returns 0); resolve() consumes the
-// probe result.  run_warp() drives 32 tasks and answers their probes with
-// probe_warp, so lanes never probe 943 cells serially.
+// probe (returns kTaskProbe), the task ends (kTaskDone) or `budget` steps
+// have run (kTaskPaused); resolve() consumes the probe result.  run_warp()
+// drives 32 tasks and answers their probes with probe_warp, so lanes never
+// probe 943 cells serially.  A budget keeps the lanes of a warp in step: a
+// lane that needs a probe soon does not wait for a lane with a long clean
+// stretch, and the two resume together after the probe.
 // ---------------------------------------------------------------------------
+
+constexpr int kTaskDone = 0, kTaskProbe = 1, kTaskPaused = 2;
+constexpr int kNoBudget = 1 << 30;
+#ifndef FRRT_STEP_SAMPLES
+#define FRRT_STEP_SAMPLES 8
+#endif
+// curve samples / integration steps a lane runs per warp step in the
+// lane-refilling kernels
+constexpr int kStepSamples = FRRT_STEP_SAMPLES;
+#ifndef FRRT_HERMITE_POLY
+#define FRRT_HERMITE_POLY 0
+#endif
 
 // check_kinematic_new_path (kinematics.cu:123-231)
 struct KinTask {
@@ -328,9 +343,11 @@ struct KinTask {
         ok = 0;
     }
 
-    __device__ int advance(const Foot &f, unsigned long long &probes)
+    __device__ int advance(const Foot &f, unsigned long long &probes, int budget = kNoBudget)
     {
         while (size < maxSize) {
+            if (budget-- <= 0)
+                return kTaskPaused;
             if (loop_count++ > loop_max)
                 break;
             x += ds * cosf(heading + beta);
@@ -364,10 +381,10 @@ struct KinTask {
             }
             pend_x = lpx;
             pend_z = lpz;
-            return 1;
+            return kTaskProbe;
         }
         ok = size >= 1;
-        return 0;
+        return kTaskDone;
     }
     // returns false when the task ended (infeasible footprint)
     __device__ bool resolve(bool feasible)
@@ -391,7 +408,14 @@ struct HermTask {
     int safe, ok;
     const float *intrinsic;
     double inv_span;           // RN(1 / (numPoints - 1))
+#if FRRT_HERMITE_POLY
+    double c3x, c2x, c3z, c2z; // cubic coefficients of t^3 and t^2
+    double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-5))^2
+    double kap_s2min;          // |d|^2 below which the reference's values decide
+    static constexpr double kEdge = 1e-7;
+#else
     double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-6))^2
+#endif
 
     __device__ void init(const Inst &I, const Foot &f, float max_curv, int x_, int z_,
                          float local_heading, int gx, int gz, float goal_heading, int safe_zone,
@@ -421,41 +445,130 @@ struct HermTask {
         nodeCost = start_cost;
         trav = f.trav ? f.trav[pos] : 0;
         inv_span = 1.0 / (double)(numPoints - 1);
+#if FRRT_HERMITE_POLY
+        c3x = 2.0 * x + (double)t1x - 2.0 * goal_x + (double)t2x;
+        c2x = -3.0 * x - 2.0 * (double)t1x + 3.0 * goal_x - (double)t2x;
+        c3z = 2.0 * z + (double)t1y - 2.0 * goal_z + (double)t2y;
+        c2z = -3.0 * z - 2.0 * (double)t1y + 3.0 * goal_z - (double)t2y;
+        const double khi = (double)max_curvature * (1.0 + 1e-5);
+        const double klo = (double)max_curvature * (1.0 - 1e-5);
+        kap_hi2 = khi * khi;
+        kap_lo2 = klo * klo;
+        // scale of the derivative's terms; |d| under 1e-4 of it is a cusp
+        const double sc = fabs(c3x) + fabs(c2x) + fabs(c3z) + fabs(c2z) + fabs((double)t1x) +
+                          fabs((double)t1y) + 1.0;
+        kap_s2min = 1e-8 * sc * sc;
+#else
         const double khi = (double)max_curvature * (1.0 + 1e-6);
         const double klo = (double)max_curvature * (1.0 - 1e-6);
         kap_hi2 = khi * khi;
         kap_lo2 = klo * klo;
+#endif
         safe = safe_zone;
         i = 0;
         ok = 0;
     }
 
-    __device__ int advance(const Foot &f, unsigned long long &probes)
+    // the reference's evaluation of the curve at t: position, first and
+    // second derivative, in its order of operations
+    __device__ __forceinline__ void ref_pos(double t, double &px, double &pz) const
+    {
+        const double t2 = t * t;
+        const double t3 = t2 * t;
+        const double h00 = 2 * t3 - 3 * t2 + 1;
+        const double h10 = t3 - 2 * t2 + t;
+        const double h01 = -2 * t3 + 3 * t2;
+        const double h11 = t3 - t2;
+        px = h00 * x + h10 * t1x + h01 * goal_x + h11 * t2x;
+        pz = h00 * z + h10 * t1y + h01 * goal_z + h11 * t2y;
+    }
+    __device__ __forceinline__ void ref_deriv(double t, double &ddx, double &ddz, double &dd2x,
+                                              double &dd2z) const
+    {
+        const double t2 = t * t;
+        const double t00 = 6 * t2 - 6 * t;
+        const double t10 = 3 * t2 - 4 * t + 1;
+        const double t01 = -6 * t2 + 6 * t;
+        const double t11 = 3 * t2 - 2 * t;
+        ddx = t00 * x + t10 * t1x + t01 * goal_x + t11 * t2x;
+        ddz = t00 * z + t10 * t1y + t01 * goal_z + t11 * t2y;
+        const double d00 = 12 * t - 6;
+        const double d10 = 6 * t - 4;
+        const double d01 = -12 * t + 6;
+        const double d11 = 6 * t - 2;
+        dd2x = d00 * x + d10 * t1x + d01 * goal_x + d11 * t2x;
+        dd2z = d00 * z + d10 * t1y + d01 * goal_z + d11 * t2y;
+    }
+    // The reference tests (float)(num / pow(s2, 1.5)) > limit.  Outside a
+    // 1e-6 relative band around the limit (hi2 / lo2: the band's squared
+    // ends) the answer follows from num^2 against limit^2 s2^3 (products
+    // rounded to ~1e-15); pow only decides cases inside the band.  s2 == 0:
+    // num > 0 is over (num / 0 = inf), num == 0 falls through to the
+    // reference's own 0 / 0.
+    __device__ __forceinline__ bool ref_over(double ddx, double ddz, double dd2x, double dd2z,
+                                             double hi2, double lo2) const
+    {
+        const double s2 = ddx * ddx + ddz * ddz;
+        const double num = fabs(ddx * dd2z - ddz * dd2x);
+        const double n2 = num * num;
+        const double s6 = s2 * s2 * s2;
+        if (n2 > hi2 * s6)
+            return true;
+        if (n2 < lo2 * s6)
+            return false;
+        const float k = num / pow(s2, 1.5);
+        return k > max_curvature;
+    }
+    // t = i / (numPoints - 1), correctly rounded, without a division per
+    // sample: with y = RN(1/b), q = RN(a y) and the exact remainder
+    // r = a - q b, RN(q + r y) is RN(a/b) (Markstein 1990); checked
+    // exhaustively for 0 <= a <= b <= 16384 against IEEE division, which
+    // covers every frame up to 4096 x 4096
+    __device__ __forceinline__ double sample_t(int k) const
     {
         const double span = (double)(numPoints - 1);
-        for (; i < numPoints; ++i) {
-            // t = i / (numPoints - 1), correctly rounded, without a division
-            // per sample: with y = RN(1/b), q = RN(a y) and the exact
-            // remainder r = a - q b, RN(q + r y) is RN(a/b) (Markstein 1990);
-            // checked exhaustively for 0 <= a <= b <= 16384 against IEEE
-            // division, which covers every frame up to 4096 x 4096
-            const double ai = (double)i;
-            const double q = __dmul_rn(ai, inv_span);
-            const double t = __fma_rn(__fma_rn(-q, span, ai), inv_span, q);
-            const double t2 = t * t;
-            const double t3 = t2 * t;
-            const double h00 = 2 * t3 - 3 * t2 + 1;
-            const double h10 = t3 - 2 * t2 + t;
-            const double h01 = -2 * t3 + 3 * t2;
-            const double h11 = t3 - t2;
-            const double px = h00 * x + h10 * t1x + h01 * goal_x + h11 * t2x;
-            const double pz = h00 * z + h10 * t1y + h01 * goal_z + h11 * t2y;
+        const double ak = (double)k;
+        const double q = __dmul_rn(ak, inv_span);
+        return __fma_rn(__fma_rn(-q, span, ak), inv_span, q);
+    }
+
+    __device__ int advance(const Foot &f, unsigned long long &probes, int budget = kNoBudget)
+    {
+        const int stop = numPoints - i > budget ? i + budget : numPoints;
+        for (; i < stop; ++i) {
+            const double t = sample_t(i);
+#if FRRT_HERMITE_POLY
+            // The curve as a cubic in t (exact coefficients, Horner) lands
+            // within ~1e-12 px of the reference's basis-function sum; a cell
+            // whose fractional offsets are further than kEdge from an edge is
+            // the reference's cell, and the bounds tests follow from it.
+            // Closer to an edge the reference's sum decides.
+            double px = fma(fma(fma(c3x, t, c2x), t, (double)t1x), t, (double)x);
+            double pz = fma(fma(fma(c3z, t, c2z), t, (double)t1y), t, (double)z);
+            int cx = __double2int_rd(px);
+            int cz = __double2int_rd(pz);
+            {
+                const double rx = px - (double)cx, rz = pz - (double)cz;
+                if (rx < kEdge || rx > 1.0 - kEdge || rz < kEdge || rz > 1.0 - kEdge) {
+                    ref_pos(t, px, pz);
+                    if (px < 0 || px >= W)
+                        continue;
+                    if (pz < 0 || pz >= H)
+                        continue;
+                    cx = (int)(px);
+                    cz = (int)(pz);
+                }
+            }
+#else
+            double px, pz;
+            ref_pos(t, px, pz);
             if (px < 0 || px >= W)
                 continue;
             if (pz < 0 || pz >= H)
                 continue;
             const int cx = (int)(px);
             const int cz = (int)(pz);
+#endif
             if (cx == last_x && cz == last_z)
                 continue;
             if (cx < 0 || cx >= W)
@@ -463,44 +576,48 @@ struct HermTask {
             if (cz < 0 || cz >= H)
                 continue;
             nodeCost += (intrinsic ? intrinsic[(long)cz * W + cx] : 0.0f) + 1;
-            const double t00 = 6 * t2 - 6 * t;
-            const double t10 = 3 * t2 - 4 * t + 1;
-            const double t01 = -6 * t2 + 6 * t;
-            const double t11 = 3 * t2 - 2 * t;
-            const double ddx = t00 * x + t10 * t1x + t01 * goal_x + t11 * t2x;
-            const double ddz = t00 * z + t10 * t1y + t01 * goal_z + t11 * t2y;
-            const double d00 = 12 * t - 6;
-            const double d10 = 6 * t - 4;
-            const double d01 = -12 * t + 6;
-            const double d11 = 6 * t - 2;
-            const double dd2x = d00 * x + d10 * t1x + d01 * goal_x + d11 * t2x;
-            const double dd2z = d00 * z + d10 * t1y + d01 * goal_z + d11 * t2y;
+#if FRRT_HERMITE_POLY
+            // derivatives of the cubic; the curvature test decides from them
+            // outside a 1e-5 band around the limit (their relative error is
+            // ~1e-14 of the curve's scale), the reference's values inside it
+            const double e3x = 3.0 * c3x, e3z = 3.0 * c3z;
+            const double ddx = fma(fma(e3x, t, 2.0 * c2x), t, (double)t1x);
+            const double ddz = fma(fma(e3z, t, 2.0 * c2z), t, (double)t1y);
             const double s2 = ddx * ddx + ddz * ddz;
             if (max_curvature > 0) {
+                const double dd2x = fma(2.0 * e3x, t, 2.0 * c2x);
+                const double dd2z = fma(2.0 * e3z, t, 2.0 * c2z);
                 const double num = fabs(ddx * dd2z - ddz * dd2x);
-                // The reference tests (float)(num / pow(s2, 1.5)) > limit.
-                // Outside a 1e-6 relative band around the limit the answer
-                // follows from num^2 against limit^2 s2^3 (products rounded
-                // to ~1e-15); pow only decides cases inside the band.
-                // s2 == 0: num > 0 is over (num / 0 = inf), num == 0 falls
-                // through to the reference's own 0 / 0.
                 const double n2 = num * num;
                 const double s6 = s2 * s2 * s2;
                 bool over;
-                if (n2 > kap_hi2 * s6)
+                if (s2 > kap_s2min && n2 > kap_hi2 * s6)
                     over = true;
-                else if (n2 < kap_lo2 * s6)
+                else if (s2 > kap_s2min && n2 < kap_lo2 * s6)
                     over = false;
                 else {
-                    const float k = num / pow(s2, 1.5);
-                    over = k > max_curvature;
+                    double rdx, rdz, rd2x, rd2z;
+                    ref_deriv(t, rdx, rdz, rd2x, rd2z);
+                    const double khi = (double)max_curvature * (1.0 + 1e-6);
+                    const double klo = (double)max_curvature * (1.0 - 1e-6);
+                    over = ref_over(rdx, rdz, rd2x, rd2z, khi * khi, klo * klo);
                 }
                 if (over) {
                     ok = 0;
                     i = numPoints;
-                    return 0;
+                    return kTaskDone;
                 }
             }
+#else
+            double ddx, ddz, dd2x, dd2z;
+            ref_deriv(t, ddx, ddz, dd2x, dd2z);
+            const double s2 = ddx * ddx + ddz * ddz;
+            if (max_curvature > 0 && ref_over(ddx, ddz, dd2x, dd2z, kap_hi2, kap_lo2)) {
+                ok = 0;
+                i = numPoints;
+                return kTaskDone;
+            }
+#endif
             last_x = cx;
             last_z = cz;
             if (safe && (trav & 0x100))
@@ -515,16 +632,27 @@ struct HermTask {
                                  probes))
                     continue;
             }
-            // the heading is only needed to probe the footprint
+            // the heading is only needed to probe the footprint: the
+            // reference's derivative, rounded to float as it does
+#if FRRT_HERMITE_POLY
+            {
+                double rdx, rdz, rd2x, rd2z;
+                ref_deriv(t, rdx, rdz, rd2x, rd2z);
+                pend_heading = atan2f(rdz, rdx) + kHalfPi;
+            }
+#else
             pend_heading = atan2f(ddz, ddx) + kHalfPi;
+#endif
             ++i;
-            return 1;
+            return kTaskProbe;
         }
+        if (i < numPoints)
+            return kTaskPaused;
         if (numPoints <= 0 || (last_x != goal_x && last_z != goal_z))
             ok = 0;
         else
             ok = 1;
-        return 0;
+        return kTaskDone;
     }
     __device__ bool resolve(bool feasible)
     {
@@ -545,16 +673,18 @@ struct HermTask {
 // Drives one task per lane.  `has` says whether the lane holds a task.
 // Probes needing a full footprint scan are answered cooperatively.
 template <class Task, class PX, class PZ>
-__device__ void run_warp(Task &t, bool has, const Foot &f, unsigned long long &probes, PX px, PZ pz)
+__device__ void run_warp(Task &t, bool has, const Foot &f, unsigned long long &probes, PX px, PZ pz,
+                         int budget = kNoBudget)
 {
     const int lane = threadIdx.x & 31;
     bool active = has;
     while (__any_sync(kFull, active)) {
         bool need = false;
         if (active) {
-            if (t.advance(f, probes))
+            const int r = t.advance(f, probes, budget);
+            if (r == kTaskProbe)
                 need = true;
-            else
+            else if (r == kTaskDone)
                 active = false;
         }
         unsigned m = __ballot_sync(kFull, need);

@@ -286,7 +286,10 @@ void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, 
 
 struct PrecompTask {
     HermTask h;
-    __device__ int advance(const Foot &f, unsigned long long &p) { return h.advance(f, p); }
+    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
+    {
+        return h.advance(f, p, budget);
+    }
     __device__ bool resolve(bool ok) { return h.resolve(ok); }
     __device__ float probe_angle() const { return h.pend_heading; }
 };
@@ -600,7 +603,10 @@ __global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states,
 
 struct KinLane {
     KinTask k;
-    __device__ int advance(const Foot &f, unsigned long long &p) { return k.advance(f, p); }
+    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
+    {
+        return k.advance(f, p, budget);
+    }
     __device__ bool resolve(bool ok) { return k.resolve(ok); }
     __device__ float probe_angle() const { return k.heading; }
 };
@@ -1040,9 +1046,10 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
             break;
         bool need = false;
         if (active) {
-            if (t.advance(f, probes))
+            const int r = t.advance(f, probes, kStepSamples);
+            if (r == kTaskProbe)
                 need = true;
-            else
+            else if (r == kTaskDone)
                 finish();
         }
         unsigned m = __ballot_sync(kFull, need);
@@ -1145,9 +1152,10 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
         }
         bool need = false;
         if (active) {
-            if (t.advance(f, probes))
+            const int r = t.advance(f, probes, kStepSamples);
+            if (r == kTaskProbe)
                 need = true;
-            else
+            else if (r == kTaskDone)
                 finish();
         }
         unsigned m = __ballot_sync(kFull, need);
@@ -1184,12 +1192,12 @@ struct GoalLane {
     bool prune;
     bool pruned;               // a window cell was skipped by the bound
 
-    __device__ int advance(const Foot &f, unsigned long long &probes)
+    __device__ int advance(const Foot &f, unsigned long long &probes, int budget)
     {
         while (true) {
             if (!in_task) {
                 if (w >= wend)
-                    return 0;
+                    return kTaskDone;
                 const int zp = zlo + w / nx, xp = xlo + w % nx;
                 w += 32;
                 if (zp < 0 || zp >= I->H)
@@ -1214,8 +1222,9 @@ struct GoalLane {
                 gd_cost_cur = gdc;
                 in_task = true;
             }
-            if (h.advance(f, probes))
-                return 1;
+            const int r = h.advance(f, probes, budget);
+            if (r != kTaskDone)
+                return r;
             in_task = false;
             if (h.ok) {
                 const float total = h.nodeCost + gd_cost_cur;
@@ -1299,7 +1308,7 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
         gl.pruned = false;
         unsigned long long probes = 0;
         run_warp(gl, true, f, probes, [](const GoalLane &q) { return q.h.last_x; },
-                 [](const GoalLane &q) { return q.h.last_z; });
+                 [](const GoalLane &q) { return q.h.last_z; }, kStepSamples);
         // warp minimum, ties to the highest cell index
         unsigned long long k = gl.best < kBigCost ? connection_key(gl.best, gl.best_cell) : kNoConnection;
         for (int o = 16; o; o >>= 1) {
@@ -1356,7 +1365,10 @@ __global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states
 
 struct SegLane {
     HermTask h;
-    __device__ int advance(const Foot &f, unsigned long long &p) { return h.advance(f, p); }
+    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
+    {
+        return h.advance(f, p, budget);
+    }
     __device__ bool resolve(bool ok) { return h.resolve(ok); }
     __device__ float probe_angle() const { return h.pend_heading; }
 };
@@ -1760,7 +1772,10 @@ void launch_extract_paths(const Inst *d_inst, State *d_state, const int *d_slots
 // j >= i + 2, of path waypoints is tested with checkDirectConnectionToGoal
 struct PairLane {
     HermTask h;
-    __device__ int advance(const Foot &f, unsigned long long &p) { return h.advance(f, p); }
+    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
+    {
+        return h.advance(f, p, budget);
+    }
     __device__ bool resolve(bool ok) { return h.resolve(ok); }
     __device__ float probe_angle() const { return h.pend_heading; }
 };
