@@ -142,11 +142,14 @@ __device__ __forceinline__ bool box_feasible(const Foot &f, int x, int z, float 
 __device__ __forceinline__ int quick_feasible(const Foot &f, int x, int z, unsigned long long &probes)
 {
     const long pos = (long)z * f.W + x;
+    // both words are loaded before either is tested: one memory round trip
+    const int tv = f.trav ? f.trav[pos] : 0;
+    const bool clear = bit_xz(f.clear, f.rw, x, z);
     // isAllAngleFeasible (path_feasible.cu:13-16): `TO_INT(z) & 256 > 0` == bit 0
-    if (f.trav && (f.trav[pos] & 1))
+    if (tv & 1)
         return 1;
     // no obstacle within the Chebyshev radius that bounds every probe
-    if (bit_xz(f.clear, f.rw, x, z)) {
+    if (clear) {
         probes += full_probes(f);
         return 1;
     }
@@ -290,20 +293,16 @@ __device__ inline bool rows_clear_warp(const Foot &f, int x, int z, float c, flo
 
 constexpr int kTaskDone = 0, kTaskProbe = 1, kTaskPaused = 2;
 constexpr int kNoBudget = 1 << 30;
-#ifndef FRRT_STEP_SAMPLES
-#define FRRT_STEP_SAMPLES 8
-#endif
 // curve samples / integration steps a lane runs per warp step in the
-// lane-refilling kernels
-constexpr int kStepSamples = FRRT_STEP_SAMPLES;
-#ifndef FRRT_HERMITE_POLY
-#define FRRT_HERMITE_POLY 0
-#endif
+// lane-refilling kernels (8 measured best of 8, 16 and unbounded on served
+// 256 x 256 planning)
+constexpr int kStepSamples = 8;
 
 // check_kinematic_new_path (kinematics.cu:123-231)
 struct KinTask {
     float x, y, heading, beta, ds, hif, nodeCost, velocity;
-    int maxSize, loop_max, loop_count, size, last_x, last_z, pend_x, pend_z;
+    float pend_cost;            // the last cell's intrinsic cost, not yet added
+    int maxSize, loop_max, loop_count, size, last_x, last_z, pend_x, pend_z, has_pend;
     int ok;                     // 1 = feasible end cell, 0 = rejected
     float og_x, og_z;
     int W, H;
@@ -338,6 +337,7 @@ struct KinTask {
         last_z = sz;
         heading = start_heading;
         nodeCost = start_cost;
+        has_pend = 0;
         loop_count = 0;
         loop_max = (100 * maxSize) / dt;
         ok = 0;
@@ -364,7 +364,11 @@ struct KinTask {
             if (lpz < 0 || lpz >= H)
                 break;
             size += 1;
-            nodeCost += (intrinsic ? intrinsic[(long)lpz * W + lpx] : 0.0f) + 1;
+            // a cell's cost is added when the next cell is reached (or at the
+            // end), in the same order, so its load overlaps the steps between
+            settle();
+            pend_cost = intrinsic ? intrinsic[(long)lpz * W + lpx] : 0.0f;
+            has_pend = 1;
             if (quick_feasible(f, lpx, lpz, probes)) {
                 last_x = lpx;
                 last_z = lpz;
@@ -383,13 +387,22 @@ struct KinTask {
             pend_z = lpz;
             return kTaskProbe;
         }
+        settle();
         ok = size >= 1;
         return kTaskDone;
+    }
+    __device__ __forceinline__ void settle()
+    {
+        if (has_pend) {
+            nodeCost += pend_cost + 1;
+            has_pend = 0;
+        }
     }
     // returns false when the task ended (infeasible footprint)
     __device__ bool resolve(bool feasible)
     {
         if (!feasible) {
+            settle();
             ok = 0;
             return false;
         }
@@ -405,17 +418,11 @@ struct KinTask {
 struct HermTask {
     int x, z, goal_x, goal_z, numPoints, i, last_x, last_z, W, H, trav;
     float distance, t1x, t1y, t2x, t2y, nodeCost, max_curvature, pend_heading;
-    int safe, ok;
+    float pend_cost;           // the last cell's intrinsic cost, not yet added
+    int safe, ok, has_pend;
     const float *intrinsic;
     double inv_span;           // RN(1 / (numPoints - 1))
-#if FRRT_HERMITE_POLY
-    double c3x, c2x, c3z, c2z; // cubic coefficients of t^3 and t^2
-    double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-5))^2
-    double kap_s2min;          // |d|^2 below which the reference's values decide
-    static constexpr double kEdge = 1e-7;
-#else
     double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-6))^2
-#endif
 
     __device__ void init(const Inst &I, const Foot &f, float max_curv, int x_, int z_,
                          float local_heading, int gx, int gz, float goal_heading, int safe_zone,
@@ -443,27 +450,13 @@ struct HermTask {
         last_x = -1;
         last_z = -1;
         nodeCost = start_cost;
+        has_pend = 0;
         trav = f.trav ? f.trav[pos] : 0;
         inv_span = 1.0 / (double)(numPoints - 1);
-#if FRRT_HERMITE_POLY
-        c3x = 2.0 * x + (double)t1x - 2.0 * goal_x + (double)t2x;
-        c2x = -3.0 * x - 2.0 * (double)t1x + 3.0 * goal_x - (double)t2x;
-        c3z = 2.0 * z + (double)t1y - 2.0 * goal_z + (double)t2y;
-        c2z = -3.0 * z - 2.0 * (double)t1y + 3.0 * goal_z - (double)t2y;
-        const double khi = (double)max_curvature * (1.0 + 1e-5);
-        const double klo = (double)max_curvature * (1.0 - 1e-5);
-        kap_hi2 = khi * khi;
-        kap_lo2 = klo * klo;
-        // scale of the derivative's terms; |d| under 1e-4 of it is a cusp
-        const double sc = fabs(c3x) + fabs(c2x) + fabs(c3z) + fabs(c2z) + fabs((double)t1x) +
-                          fabs((double)t1y) + 1.0;
-        kap_s2min = 1e-8 * sc * sc;
-#else
         const double khi = (double)max_curvature * (1.0 + 1e-6);
         const double klo = (double)max_curvature * (1.0 - 1e-6);
         kap_hi2 = khi * khi;
         kap_lo2 = klo * klo;
-#endif
         safe = safe_zone;
         i = 0;
         ok = 0;
@@ -537,29 +530,6 @@ struct HermTask {
         const int stop = numPoints - i > budget ? i + budget : numPoints;
         for (; i < stop; ++i) {
             const double t = sample_t(i);
-#if FRRT_HERMITE_POLY
-            // The curve as a cubic in t (exact coefficients, Horner) lands
-            // within ~1e-12 px of the reference's basis-function sum; a cell
-            // whose fractional offsets are further than kEdge from an edge is
-            // the reference's cell, and the bounds tests follow from it.
-            // Closer to an edge the reference's sum decides.
-            double px = fma(fma(fma(c3x, t, c2x), t, (double)t1x), t, (double)x);
-            double pz = fma(fma(fma(c3z, t, c2z), t, (double)t1y), t, (double)z);
-            int cx = __double2int_rd(px);
-            int cz = __double2int_rd(pz);
-            {
-                const double rx = px - (double)cx, rz = pz - (double)cz;
-                if (rx < kEdge || rx > 1.0 - kEdge || rz < kEdge || rz > 1.0 - kEdge) {
-                    ref_pos(t, px, pz);
-                    if (px < 0 || px >= W)
-                        continue;
-                    if (pz < 0 || pz >= H)
-                        continue;
-                    cx = (int)(px);
-                    cz = (int)(pz);
-                }
-            }
-#else
             double px, pz;
             ref_pos(t, px, pz);
             if (px < 0 || px >= W)
@@ -568,56 +538,25 @@ struct HermTask {
                 continue;
             const int cx = (int)(px);
             const int cz = (int)(pz);
-#endif
             if (cx == last_x && cz == last_z)
                 continue;
             if (cx < 0 || cx >= W)
                 continue;
             if (cz < 0 || cz >= H)
                 continue;
-            nodeCost += (intrinsic ? intrinsic[(long)cz * W + cx] : 0.0f) + 1;
-#if FRRT_HERMITE_POLY
-            // derivatives of the cubic; the curvature test decides from them
-            // outside a 1e-5 band around the limit (their relative error is
-            // ~1e-14 of the curve's scale), the reference's values inside it
-            const double e3x = 3.0 * c3x, e3z = 3.0 * c3z;
-            const double ddx = fma(fma(e3x, t, 2.0 * c2x), t, (double)t1x);
-            const double ddz = fma(fma(e3z, t, 2.0 * c2z), t, (double)t1y);
-            const double s2 = ddx * ddx + ddz * ddz;
-            if (max_curvature > 0) {
-                const double dd2x = fma(2.0 * e3x, t, 2.0 * c2x);
-                const double dd2z = fma(2.0 * e3z, t, 2.0 * c2z);
-                const double num = fabs(ddx * dd2z - ddz * dd2x);
-                const double n2 = num * num;
-                const double s6 = s2 * s2 * s2;
-                bool over;
-                if (s2 > kap_s2min && n2 > kap_hi2 * s6)
-                    over = true;
-                else if (s2 > kap_s2min && n2 < kap_lo2 * s6)
-                    over = false;
-                else {
-                    double rdx, rdz, rd2x, rd2z;
-                    ref_deriv(t, rdx, rdz, rd2x, rd2z);
-                    const double khi = (double)max_curvature * (1.0 + 1e-6);
-                    const double klo = (double)max_curvature * (1.0 - 1e-6);
-                    over = ref_over(rdx, rdz, rd2x, rd2z, khi * khi, klo * klo);
-                }
-                if (over) {
-                    ok = 0;
-                    i = numPoints;
-                    return kTaskDone;
-                }
-            }
-#else
+            // added when the next cell is reached (or at the end), in order
+            settle();
+            pend_cost = intrinsic ? intrinsic[(long)cz * W + cx] : 0.0f;
+            has_pend = 1;
             double ddx, ddz, dd2x, dd2z;
             ref_deriv(t, ddx, ddz, dd2x, dd2z);
             const double s2 = ddx * ddx + ddz * ddz;
             if (max_curvature > 0 && ref_over(ddx, ddz, dd2x, dd2z, kap_hi2, kap_lo2)) {
+                settle();
                 ok = 0;
                 i = numPoints;
                 return kTaskDone;
             }
-#endif
             last_x = cx;
             last_z = cz;
             if (safe && (trav & 0x100))
@@ -632,31 +571,31 @@ struct HermTask {
                                  probes))
                     continue;
             }
-            // the heading is only needed to probe the footprint: the
-            // reference's derivative, rounded to float as it does
-#if FRRT_HERMITE_POLY
-            {
-                double rdx, rdz, rd2x, rd2z;
-                ref_deriv(t, rdx, rdz, rd2x, rd2z);
-                pend_heading = atan2f(rdz, rdx) + kHalfPi;
-            }
-#else
+            // the heading is only needed to probe the footprint
             pend_heading = atan2f(ddz, ddx) + kHalfPi;
-#endif
             ++i;
             return kTaskProbe;
         }
         if (i < numPoints)
             return kTaskPaused;
+        settle();
         if (numPoints <= 0 || (last_x != goal_x && last_z != goal_z))
             ok = 0;
         else
             ok = 1;
         return kTaskDone;
     }
+    __device__ __forceinline__ void settle()
+    {
+        if (has_pend) {
+            nodeCost += pend_cost + 1;
+            has_pend = 0;
+        }
+    }
     __device__ bool resolve(bool feasible)
     {
         if (!feasible) {
+            settle();
             ok = 0;
             i = numPoints;
             numPoints = -1;  // keep ok == 0 if advance() is called again

@@ -743,25 +743,53 @@ __global__ void __launch_bounds__(256) k_post(const Inst *insts, State *states, 
 // numNodes + 4 hops (graph_collision.cu:32-83; an exhausted walk keeps the node)
 __global__ void __launch_bounds__(256) k_erase(const Inst *insts, State *states, const Sched *sc)
 {
+    // the chunk's non-NULL cells (offsets in the chunk), walked one per thread
+    __shared__ uint16_t list[kSweepCells];
+    __shared__ int count;
     const int n = sc->n_slots;
     const int total = sc->sweep_total;
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
         const int slot = find_slot(sc->sweep_start, n, c);
         const State &S = states[slot];
         if (!live(S) || !S.collision || S.node_count <= 2)
-            continue;
+            continue;  // uniform across the block
         const Inst &I = insts[slot];
         volatile int8_t *type = I.type;
         const int cells = I.W * I.H;
-        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
-        if (base >= cells)
-            continue;
+        const int base0 = (c - sc->sweep_start[slot]) * kSweepCells;
+        if (threadIdx.x == 0)
+            count = 0;
+        __syncthreads();
+        const int base = base0 + threadIdx.x * 16;
         int8_t t[16];
-        load16(I.type + base, t);
-        for (int k = 0; k < 16; k++) {
-            const int pos = base + k;
-            if (pos >= cells || t[k] == T_NULL)
-                continue;
+        int mine = 0;
+        if (base < cells) {
+            load16(I.type + base, t);
+            for (int k = 0; k < 16; k++)
+                mine += (base + k < cells && t[k] != T_NULL) ? 1 : 0;
+        }
+        // warp-aggregated append into the block's list
+        const int lane = threadIdx.x & 31;
+        int incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o)
+                incl += v;
+        }
+        const int wsum = __shfl_sync(kFull, incl, 31);
+        int at = 0;
+        if (lane == 31 && wsum)
+            at = atomicAdd(&count, wsum);
+        at = __shfl_sync(kFull, at, 31) + incl - mine;
+        if (mine) {
+            for (int k = 0; k < 16; k++)
+                if (base + k < cells && t[k] != T_NULL)
+                    list[at++] = (uint16_t)(threadIdx.x * 16 + k);
+        }
+        __syncthreads();
+        const int m = count;
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {
+            const int pos = base0 + list[e];
             int curr = pos;
             int i = S.node_count + 4;
             while (i-- > 0) {
@@ -780,6 +808,7 @@ __global__ void __launch_bounds__(256) k_erase(const Inst *insts, State *states,
                 curr = next;
             }
         }
+        __syncthreads();  // the list is rebuilt for the next chunk
     }
 }
 
@@ -901,18 +930,22 @@ __device__ __forceinline__ int window_count(int c, float r, int &lo)
 
 // Lists, once per cell, the cells inside the windows of the nodes that the
 // goal search will search this iteration whose direct connection is unknown.
+// One warp per unit of the goal search (listed node, 32-cell window chunk),
+// one window cell per lane: a node's window is spread over many warps, so
+// the pass costs a few dependent memory round trips at any load.
 __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *states, const Sched *sc)
 {
     const int n = sc->n_slots;
-    const int total = sc->node_start[n];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = blockIdx.x; c < total; c += gridDim.x) {
-        const int slot = find_slot(sc->node_start, n, c);
+    const int total = sc->goal_start[n];
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < total; u += warps) {
+        const int slot = find_slot(sc->goal_start, n, u);
         const Inst &I = insts[slot];
         State &S = states[slot];
-        const int idx = (c - sc->node_start[slot]) * kNodeChunk + warp;
-        if (idx >= S.n_nodes)
-            continue;  // uniform across the warp
+        const int local = u - sc->goal_start[slot];
+        const int idx = local / I.win_chunks;
+        const int wc = local - idx * I.win_chunks;
         const int pos = I.nodes[idx];
         if (I.memo_key[pos] == memo_key_of(I, pos))
             continue;  // the search result is known: no window is read
@@ -921,30 +954,28 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
         const int nz = window_count(z, I.dist_tol, zlo);
         const int nx = window_count(x, I.dist_tol, xlo);
         const int wtotal = nx > 0 ? nz * nx : 0;
-        for (int w0 = 0; w0 < wtotal; w0 += 32) {
-            const int w = w0 + lane;
-            int cell = -1;
-            if (w < wtotal) {
-                const int zp = zlo + w / nx, xp = xlo + w % nx;
-                if (zp >= 0 && zp < I.H && xp >= 0 && xp < I.W) {
-                    const int cc = zp * I.W + xp;
-                    if (I.gd_flag[cc] == kGdUnknown) {
-                        const uint32_t bit = 1u << (cc & 31);
-                        if (!(atomicOr(&I.gd_req[cc >> 5], bit) & bit))
-                            cell = cc;
-                    }
+        const int w = wc * 32 + lane;
+        int cell = -1;
+        if (w < wtotal) {
+            const int zp = zlo + w / nx, xp = xlo + w % nx;
+            if (zp >= 0 && zp < I.H && xp >= 0 && xp < I.W) {
+                const int cc = zp * I.W + xp;
+                if (I.gd_flag[cc] == kGdUnknown) {
+                    const uint32_t bit = 1u << (cc & 31);
+                    if (!(atomicOr(&I.gd_req[cc >> 5], bit) & bit))
+                        cell = cc;
                 }
             }
-            const unsigned m = __ballot_sync(kFull, cell >= 0);
-            if (!m)
-                continue;
-            int at = 0;
-            if (lane == 0)
-                at = atomicAdd(&S.n_gd, __popc(m));
-            at = __shfl_sync(kFull, at, 0);
-            if (cell >= 0)
-                I.gd_list[at + __popc(m & ((1u << lane) - 1u))] = cell;
         }
+        const unsigned m = __ballot_sync(kFull, cell >= 0);
+        if (!m)
+            continue;
+        int at = 0;
+        if (lane == 0)
+            at = atomicAdd(&S.n_gd, __popc(m));
+        at = __shfl_sync(kFull, at, 0);
+        if (cell >= 0)
+            I.gd_list[at + __popc(m & ((1u << lane) - 1u))] = cell;
     }
 }
 
@@ -1466,8 +1497,8 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
 
 const char *const kIterKernelNames[kIterKernels] = {
     "k_scan", "k_plan(cand)", "k_propose(mlp)", "k_expand", "k_apply", "k_post", "k_erase",
-    "k_setnodes", "k_accept", "k_plan(nodes)", "k_gd_demand", "k_plan(cells)", "k_gd_eval",
-    "k_plan(windows)", "k_goal", "k_select", "k_finish"};
+    "k_setnodes", "k_accept", "k_plan(nodes)", "k_plan(windows)", "k_gd_demand", "k_plan(cells)",
+    "k_gd_eval", "k_goal", "k_select", "k_finish"};
 
 // ---------------------------------------------------------------------------
 // learned expansion proposal inside an iteration
@@ -1618,13 +1649,13 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 1);
     mark();
+    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 3);
+    mark();
     k_gd_demand<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 2);
     mark();
     k_gd_eval<<<L.sms * kEvalBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
-    mark();
-    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 3);
     mark();
     k_goal<<<L.sms * kGoalBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
