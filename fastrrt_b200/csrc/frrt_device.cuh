@@ -297,6 +297,11 @@ constexpr int kNoBudget = 1 << 30;
 // lane-refilling kernels (8 measured best of 8, 16 and unbounded on served
 // 256 x 256 planning)
 constexpr int kStepSamples = 8;
+#ifndef FRRT_COARSE_STRIDE
+#define FRRT_COARSE_STRIDE 8
+#endif
+// sample stride of the first pass of the direct goal connections
+constexpr int kCoarseStride = FRRT_COARSE_STRIDE;
 
 // check_kinematic_new_path (kinematics.cu:123-231)
 struct KinTask {
@@ -420,6 +425,7 @@ struct HermTask {
     float distance, t1x, t1y, t2x, t2y, nodeCost, max_curvature, pend_heading;
     float pend_cost;           // the last cell's intrinsic cost, not yet added
     int safe, ok, has_pend;
+    int coarse;                // stride of the first pass (0: none or done)
     const float *intrinsic;
     double inv_span;           // RN(1 / (numPoints - 1))
     double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-6))^2
@@ -451,6 +457,7 @@ struct HermTask {
         last_z = -1;
         nodeCost = start_cost;
         has_pend = 0;
+        coarse = 0;
         trav = f.trav ? f.trav[pos] : 0;
         inv_span = 1.0 / (double)(numPoints - 1);
         const double khi = (double)max_curvature * (1.0 + 1e-6);
@@ -525,8 +532,75 @@ struct HermTask {
         return __fma_rn(__fma_rn(-q, span, ak), inv_span, q);
     }
 
+    // A first pass over every `stride`-th sample before the walk in order.
+    // A sample in the frame whose predecessor is in the frame and in another
+    // cell is a sample the reference's loop tests, with the same heading, so
+    // a curvature or footprint failure there is the reference's answer
+    // (no connection) whatever it meets before.  Obstacles are wide next to
+    // the 1 px sample spacing and most curves to the goal fail, so the pass
+    // ends most of them after a few samples; a curve it clears is walked in
+    // order from the first sample.
+    __device__ void start_coarse(int stride)
+    {
+        if (stride >= 2) {
+            coarse = stride;
+            i = stride - 1;
+        }
+    }
+    __device__ int advance_coarse(const Foot &f, unsigned long long &probes, int budget)
+    {
+        for (; i < numPoints; i += coarse) {
+            if (budget-- <= 0)
+                return kTaskPaused;
+            const double t = sample_t(i);
+            double px, pz, qx, qz;
+            ref_pos(t, px, pz);
+            if (px < 0 || px >= W || pz < 0 || pz >= H)
+                continue;
+            ref_pos(sample_t(i - 1), qx, qz);
+            if (qx < 0 || qx >= W || qz < 0 || qz >= H)
+                continue;
+            const int cx = (int)(px);
+            const int cz = (int)(pz);
+            if (cx == (int)(qx) && cz == (int)(qz))
+                continue;
+            double ddx, ddz, dd2x, dd2z;
+            ref_deriv(t, ddx, ddz, dd2x, dd2z);
+            if (max_curvature > 0 && ref_over(ddx, ddz, dd2x, dd2z, kap_hi2, kap_lo2)) {
+                ok = 0;
+                coarse = 0;
+                i = numPoints;
+                numPoints = -1;  // keep ok == 0 if advance() is called again
+                return kTaskDone;
+            }
+            if (safe && (trav & 0x100))
+                continue;
+            if (quick_feasible(f, cx, cz, probes))
+                continue;
+            const double s2 = ddx * ddx + ddz * ddz;
+            if (f.sat && s2 > 0.0) {
+                const float inv = rsqrtf((float)s2);
+                if (box_feasible(f, cx, cz, fabsf((float)ddz) * inv, fabsf((float)ddx) * inv, probes))
+                    continue;
+            }
+            pend_heading = atan2f(ddz, ddx) + kHalfPi;
+            last_x = cx;  // the probed cell (probe_x / probe_z)
+            last_z = cz;
+            i += coarse;
+            return kTaskProbe;
+        }
+        // nothing failed: the reference's walk from the first sample
+        coarse = 0;
+        i = 0;
+        last_x = -1;
+        last_z = -1;
+        return kTaskPaused;
+    }
+
     __device__ int advance(const Foot &f, unsigned long long &probes, int budget = kNoBudget)
     {
+        if (coarse)
+            return advance_coarse(f, probes, budget);
         const int stop = numPoints - i > budget ? i + budget : numPoints;
         for (; i < stop; ++i) {
             const double t = sample_t(i);
@@ -597,6 +671,7 @@ struct HermTask {
         if (!feasible) {
             settle();
             ok = 0;
+            coarse = 0;
             i = numPoints;
             numPoints = -1;  // keep ok == 0 if advance() is called again
             return false;

@@ -1069,6 +1069,7 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
                     lh = compute_heading(x, z, I->goal_x, I->goal_z);
                     t.h.init(*I, f, I->gd_max_curvature, x, z, lh, I->goal_x, I->goal_z,
                              I->goal_heading, 0, I->gd_cost[pos]);
+                    t.h.start_coarse(kCoarseStride);
                     active = true;
                 }
             }
