@@ -74,10 +74,12 @@ class ProposalNet:
 
 
 def collect_dataset(n_plans, seed0=500_000, max_rows=200_000, slots=256, max_iterations=100,
-                    sizes=(128, 256, 512)):
+                    sizes=(128, 256, 512), c0_share=0.0, net=None, mix=0.8):
     """Training rows from the planner's own solves of seeded batched requests
-    (mixed frame sizes, 5-30% obstacles): one row per expansion on every
-    validated path.  Returns device tensors (X: rows x 1040 bf16, labels:
+    (mixed frame sizes, 5-30% obstacles; a share `c0_share` of them the
+    single-instance 256 x 256 layout, start at the centre, goal top centre):
+    one row per expansion on every validated path, with `net` attached at
+    `mix` when given.  Returns device tensors (X: rows x 1040 bf16, labels:
     int32) and the number of plans solved."""
     import torch
 
@@ -85,13 +87,19 @@ def collect_dataset(n_plans, seed0=500_000, max_rows=200_000, slots=256, max_ite
     from .batch import BatchPlanner, make_request
     size_max = max(sizes)
     planner = BatchPlanner(slots, size_max, size_max)
+    if net is not None:
+        planner.set_proposal(net, mix=mix)
     X = torch.zeros((max_rows, N_IN_PAD), dtype=torch.bfloat16, device="cuda")
     labels = torch.zeros(max_rows, dtype=torch.int32, device="cuda")
     rows = solved = 0
     for b0 in range(0, n_plans, slots):
         reqs = []
         for k in range(b0, min(n_plans, b0 + slots)):
-            cls, start, goal, steer, _ = synth.batch_request(seed0 + k, sizes=sizes)
+            if (k % 100) < int(round(100 * c0_share)):
+                cls, start, goal = synth.c0_request(seed0 + k)
+                steer = 40.0
+            else:
+                cls, start, goal, steer, _ = synth.batch_request(seed0 + k, sizes=sizes)
             reqs.append(make_request(cls, synth.CLASS_COSTS, start, goal, max_steering_deg=steer,
                                      seed=seed0 + k, max_iterations=max_iterations))
         valid, _, _, _ = planner.plan(reqs, max_launches=max_iterations + 8, check_every=4)
