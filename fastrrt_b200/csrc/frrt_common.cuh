@@ -133,7 +133,9 @@ struct State {
     int node_count;            // NODE count after expansion (erase bound)
     int temp_count;
     int all_count;
-    int n_nodes;               // listed NODE cells for the goal search
+    int n_nodes;               // listed NODE cells for the goal search (nodes[0, n_nodes))
+    int n_memo;                // listed nodes with a kept search result, at the list's end
+                               // (nodes[W H - n_memo, W H)), resolved when listed
     int n_gd;                  // cells listed for goal direct-connection evaluation
     int skip;                  // graph was empty: start re-added, rest skipped
     int found;                 // goal connection found this iteration

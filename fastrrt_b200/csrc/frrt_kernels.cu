@@ -450,6 +450,7 @@ __global__ void k_init_state(const Inst *insts, State *states, const int *slots,
     S.temp_count = 0;
     S.all_count = 0;
     S.n_nodes = 0;
+    S.n_memo = 0;
     S.n_gd = 0;
     S.skip = 0;
     S.found = 0;
@@ -531,13 +532,13 @@ __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, 
 }
 
 // prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
-// work units of one slot: 0 candidate chunks, 1 listed-node chunks, 2
-// listed cells, 3 (listed node, window chunk) pairs
+// work units of one slot: 0 candidate chunks, 1 listed-node chunks (both
+// ends of the list), 2 listed cells, 3 (node to search, window chunk) pairs
 __device__ __forceinline__ long long chunks_of(const Inst &I, const State &S, int which)
 {
     switch (which) {
     case 0: return (S.n_cand + kCandChunk - 1) / kCandChunk;
-    case 1: return (S.n_nodes + kNodeChunk - 1) / kNodeChunk;
+    case 1: return (S.n_nodes + S.n_memo + kNodeChunk - 1) / kNodeChunk;
     case 2: return S.n_gd;
     default: return (long long)S.n_nodes * I.win_chunks;
     }
@@ -872,8 +873,9 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
         const Inst &I = insts[slot];
         const int cells = I.W * I.H;
         const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
-        int temps = 0, all = 0, cnt = 0;
+        int temps = 0, all = 0, cnt = 0, kept = 0;
         int32_t mine[16];
+        int32_t mine_kept[16];
         if (base < cells) {
             int4 v = *reinterpret_cast<const int4 *>(I.type + base);
             int8_t *t = reinterpret_cast<int8_t *>(&v);
@@ -891,10 +893,16 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
                 if (t[k] != T_NODE)
                     continue;
                 const int pos = base + k;
-                if (I.memo_key[pos] == memo_key_of(I, pos) && I.memo_result[pos] == kNoConnection) {
-                    // searched before with this heading and cost and no
-                    // connection found: only the goal check remains
+                if (I.memo_key[pos] == memo_key_of(I, pos)) {
+                    // searched before with this heading and cost: the goal
+                    // check runs here, and a kept connection is listed as
+                    // the node's result without a search
                     goal_check_node(I, S, pos);
+                    const unsigned long long r = I.memo_result[pos];
+                    if (r != kNoConnection) {
+                        mine_kept[kept++] = pos;
+                        atomicMin(&S.best, (long long)(r >> 32));
+                    }
                     continue;
                 }
                 mine[cnt++] = pos;
@@ -908,6 +916,14 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
             I.node_key[at + k] = kNoConnection;
             I.node_pending[at + k] = I.win_chunks;
             I.node_pruned[at + k] = 0;
+        }
+        // kept results from the end of the list: the two ends never meet, as
+        // both hold distinct NODE cells of the frame
+        const int kat = warp_append(&S.n_memo, kept);
+        for (int k = 0; k < kept; k++) {
+            const int idx = cells - 1 - (kat + k);
+            I.nodes[idx] = mine_kept[k];
+            I.node_key[idx] = I.memo_result[mine_kept[k]];
         }
         temps = warp_sum(temps);
         all = warp_sum(all);
@@ -946,9 +962,7 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
         const int local = u - sc->goal_start[slot];
         const int idx = local / I.win_chunks;
         const int wc = local - idx * I.win_chunks;
-        const int pos = I.nodes[idx];
-        if (I.memo_key[pos] == memo_key_of(I, pos))
-            continue;  // the search result is known: no window is read
+        const int pos = I.nodes[idx];  // a node to search: no kept result
         const int z = pos / I.W, x = pos - z * I.W;
         int zlo, xlo;
         const int nz = window_count(z, I.dist_tol, zlo);
@@ -1305,19 +1319,10 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
         const int local = g - sc->goal_start[slot];
         const int idx = local / I.win_chunks;
         const int wc = local - idx * I.win_chunks;
+        // a node to search (nodes with a kept result were resolved when
+        // listed); the key of this heading and cost marks a complete result
         const int pos = I.nodes[idx];
         const unsigned long long key = memo_key_of(I, pos);
-        if (I.memo_key[pos] == key) {
-            // a complete search with this heading and cost was kept
-            if (wc == 0 && lane == 0) {
-                goal_check_node(I, S, pos);
-                const unsigned long long r = I.memo_result[pos];
-                I.node_key[idx] = r;
-                if (r != kNoConnection)
-                    atomicMin(&S.best, (long long)(r >> 32));
-            }
-            continue;
-        }
         if (wc == 0 && lane == 0)
             goal_check_node(I, S, pos);
         const Foot f = foot_of(I, I.blocked, I.clear);
@@ -1383,9 +1388,11 @@ __global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states
         const int slot = find_slot(sc->node_start, n, chunk);
         const Inst &I = insts[slot];
         State &S = states[slot];
-        const int idx = (chunk - sc->node_start[slot]) * kNodeChunk + (int)(e % kNodeChunk);
-        if (idx >= S.n_nodes || S.best >= kBigCost)
+        int idx = (chunk - sc->node_start[slot]) * kNodeChunk + (int)(e % kNodeChunk);
+        if (idx >= S.n_nodes + S.n_memo || S.best >= kBigCost)
             continue;
+        if (idx >= S.n_nodes)
+            idx = I.W * I.H - 1 - (idx - S.n_nodes);  // a kept result
         const unsigned long long nk = I.node_key[idx];
         if (nk != kNoConnection && (long long)(nk >> 32) == S.best) {
             const unsigned long long key =
@@ -1483,6 +1490,7 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
     S.temp_count = 0;
     S.all_count = 0;
     S.n_nodes = 0;
+    S.n_memo = 0;
     S.n_gd = 0;
     S.collision = 0;
     S.best = kBigCost;
