@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--requests", type=int, default=1024, help="requests per step and GPU")
+    ap.add_argument("--requests", type=int, default=4096, help="requests per step and GPU")
     ap.add_argument("--slots", type=int, default=None,
                     help="planning slots per GPU (default: the autotuned value, else 512)")
     ap.add_argument("--check-every", type=int, default=None,
@@ -116,17 +116,40 @@ def request_seeds(rank, step, B):
     return [(rank * 1000003 + step * B + k) & 0xFFFFFFFF for k in range(B)]
 
 
+def _c0_frames(seeds):
+    """C0 requests of `seeds` (a pool worker): (frames, starts, goals)"""
+    from fastrrt_b200 import synth
+    out = [synth.c0_request(seed, SIZE) for seed in seeds]
+    return np.stack([o[0] for o in out]), [o[1] for o in out], [o[2] for o in out]
+
+
 def workload(rank, step, B):
     """seeded requests of one step: (frames, starts, goals, seeds)"""
-    from fastrrt_b200 import synth
-    frames, starts, goals, seeds = [], [], [], []
-    for seed in request_seeds(rank, step, B):
-        cls, st, gl = synth.c0_request(seed, SIZE)
-        frames.append(cls)
-        starts.append(st)
-        goals.append(gl)
-        seeds.append(seed)
-    return np.stack(frames), starts, goals, seeds
+    seeds = request_seeds(rank, step, B)
+    frames, starts, goals = _c0_frames(seeds)
+    return frames, starts, goals, seeds
+
+
+def workloads(rank, steps, B, world=1):
+    """the requests of `steps` steps, generated by a process pool (spawned,
+    so it is independent of this process's CUDA state)"""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    seeds = [request_seeds(rank, s, B) for s in range(steps)]
+    flat = [x for ss in seeds for x in ss]
+    chunk = 256
+    parts = [flat[i:i + chunk] for i in range(0, len(flat), chunk)]
+    workers = max(1, min(32, (os.cpu_count() or 1) // max(1, world), len(parts)))
+    if workers == 1:
+        res = [_c0_frames(p) for p in parts]
+    else:
+        with cf.ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            res = list(ex.map(_c0_frames, parts))
+    frames = np.concatenate([r[0] for r in res])
+    starts = [x for r in res for x in r[1]]
+    goals = [x for r in res for x in r[2]]
+    return [(frames[s * B:(s + 1) * B], starts[s * B:(s + 1) * B], goals[s * B:(s + 1) * B], seeds[s])
+            for s in range(steps)]
 
 
 class ClockSampler:
@@ -353,7 +376,7 @@ def run_mine(args, rank, world, local):
     R = args.requests
     total_steps = args.warmup + args.steps
     t_gen = time.time()
-    work = [workload(rank, s, R) for s in range(total_steps)]
+    work = workloads(rank, total_steps, R, world)
     gen_s = time.time() - t_gen
     planner = F.BatchPlanner(args.slots, SIZE, SIZE)
     if tuned:

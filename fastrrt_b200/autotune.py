@@ -31,7 +31,7 @@ def load(path=DEFAULT_OUT):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--requests", type=int, default=768)
+    ap.add_argument("--requests", type=int, default=2048)
     ap.add_argument("--out", default=DEFAULT_OUT)
     a = ap.parse_args()
     import torch
