@@ -531,16 +531,23 @@ __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, 
     }
 }
 
+// 32-cell window chunks per goal-search unit, and the units of one node
+constexpr int kGoalGroup = 4;
+__device__ __forceinline__ int goal_groups(const Inst &I)
+{
+    return (I.win_chunks + kGoalGroup - 1) / kGoalGroup;
+}
+
 // prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
 // work units of one slot: 0 candidate chunks, 1 listed-node chunks (both
-// ends of the list), 2 listed cells, 3 (node to search, window chunk) pairs
+// ends of the list), 2 listed cells, 3 (node to search, window chunk group)
 __device__ __forceinline__ long long chunks_of(const Inst &I, const State &S, int which)
 {
     switch (which) {
     case 0: return (S.n_cand + kCandChunk - 1) / kCandChunk;
     case 1: return (S.n_nodes + S.n_memo + kNodeChunk - 1) / kNodeChunk;
     case 2: return S.n_gd;
-    default: return (long long)S.n_nodes * I.win_chunks;
+    default: return (long long)S.n_nodes * goal_groups(I);
     }
 }
 
@@ -914,7 +921,7 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
         for (int k = 0; k < cnt; k++) {
             I.nodes[at + k] = mine[k];
             I.node_key[at + k] = kNoConnection;
-            I.node_pending[at + k] = I.win_chunks;
+            I.node_pending[at + k] = goal_groups(I);
             I.node_pruned[at + k] = 0;
         }
         // kept results from the end of the list: the two ends never meet, as
@@ -946,9 +953,9 @@ __device__ __forceinline__ int window_count(int c, float r, int &lo)
 
 // Lists, once per cell, the cells inside the windows of the nodes that the
 // goal search will search this iteration whose direct connection is unknown.
-// One warp per unit of the goal search (listed node, 32-cell window chunk),
-// one window cell per lane: a node's window is spread over many warps, so
-// the pass costs a few dependent memory round trips at any load.
+// One warp per unit of the goal search (node to search, group of window
+// chunks), one window cell per lane and chunk: a node's window is spread
+// over many warps, so the pass costs a few memory round trips at any load.
 __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *states, const Sched *sc)
 {
     const int n = sc->n_slots;
@@ -960,36 +967,39 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
         const Inst &I = insts[slot];
         State &S = states[slot];
         const int local = u - sc->goal_start[slot];
-        const int idx = local / I.win_chunks;
-        const int wc = local - idx * I.win_chunks;
+        const int groups = goal_groups(I);
+        const int idx = local / groups;
+        const int wg = local - idx * groups;
         const int pos = I.nodes[idx];  // a node to search: no kept result
         const int z = pos / I.W, x = pos - z * I.W;
         int zlo, xlo;
         const int nz = window_count(z, I.dist_tol, zlo);
         const int nx = window_count(x, I.dist_tol, xlo);
         const int wtotal = nx > 0 ? nz * nx : 0;
-        const int w = wc * 32 + lane;
-        int cell = -1;
-        if (w < wtotal) {
-            const int zp = zlo + w / nx, xp = xlo + w % nx;
-            if (zp >= 0 && zp < I.H && xp >= 0 && xp < I.W) {
-                const int cc = zp * I.W + xp;
-                if (I.gd_flag[cc] == kGdUnknown) {
-                    const uint32_t bit = 1u << (cc & 31);
-                    if (!(atomicOr(&I.gd_req[cc >> 5], bit) & bit))
-                        cell = cc;
+        for (int q = 0; q < kGoalGroup; q++) {
+            const int w = (wg * kGoalGroup + q) * 32 + lane;
+            int cell = -1;
+            if (w < wtotal) {
+                const int zp = zlo + w / nx, xp = xlo + w % nx;
+                if (zp >= 0 && zp < I.H && xp >= 0 && xp < I.W) {
+                    const int cc = zp * I.W + xp;
+                    if (I.gd_flag[cc] == kGdUnknown) {
+                        const uint32_t bit = 1u << (cc & 31);
+                        if (!(atomicOr(&I.gd_req[cc >> 5], bit) & bit))
+                            cell = cc;
+                    }
                 }
             }
+            const unsigned m = __ballot_sync(kFull, cell >= 0);
+            if (!m)
+                continue;
+            int at = 0;
+            if (lane == 0)
+                at = atomicAdd(&S.n_gd, __popc(m));
+            at = __shfl_sync(kFull, at, 0);
+            if (cell >= 0)
+                I.gd_list[at + __popc(m & ((1u << lane) - 1u))] = cell;
         }
-        const unsigned m = __ballot_sync(kFull, cell >= 0);
-        if (!m)
-            continue;
-        int at = 0;
-        if (lane == 0)
-            at = atomicAdd(&S.n_gd, __popc(m));
-        at = __shfl_sync(kFull, at, 0);
-        if (cell >= 0)
-            I.gd_list[at + __popc(m & ((1u << lane) - 1u))] = cell;
     }
 }
 
@@ -1226,7 +1236,8 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
 // the node (graph_best_node.cu:181-222)
 struct GoalLane {
     HermTask h;
-    int w, wend, nx, zlo, xlo;
+    const int *list;           // the unit's connected window cells, in window order
+    int e, cnt;                // this lane's next entry (stride 32), entries
     bool in_task;
     int x, z;
     float heading, cost, gd_cost_cur;
@@ -1242,17 +1253,11 @@ struct GoalLane {
     {
         while (true) {
             if (!in_task) {
-                if (w >= wend)
+                if (e >= cnt)
                     return kTaskDone;
-                const int zp = zlo + w / nx, xp = xlo + w % nx;
-                w += 32;
-                if (zp < 0 || zp >= I->H)
-                    continue;
-                if (xp < 0 || xp >= I->W)
-                    continue;
-                const int cell = zp * I->W + xp;
-                if (!(I->gd_flag[cell] == 1))
-                    continue;
+                const int cell = list[e];
+                e += 32;
+                const int zp = cell / I->W, xp = cell - zp * I->W;
                 const float gdc = I->gd_cost[cell];
                 if (prune) {
                     // the connection costs at least cost + 1 (the first sample)
@@ -1296,16 +1301,22 @@ __device__ __forceinline__ unsigned long long connection_key(long long lc, int c
     return ((unsigned long long)lc << 32) | (unsigned long long)(0xffffffffu - (unsigned)cell);
 }
 
-// Goal search, one warp per (listed node, 32-cell chunk of its window), each
-// warp grabbing units on its own: a node's window is spread over many warps,
-// so a few nodes with busy windows do not hold a launch back.  The last
-// chunk of a node to finish keeps the node's result when no chunk skipped a
-// cell by the bound.  Masks are read through L1.
+// Goal search, one warp per (listed node, group of kGoalGroup 32-cell chunks
+// of its window), each warp grabbing units on its own: a node's window is
+// spread over many warps, so a few nodes with busy windows do not hold a
+// launch back.  The warp first lists the group's cells that have a direct
+// goal connection (a few percent of a window) and hands those to its lanes,
+// in window order.  The last group of a node to finish keeps the node's
+// result when no group skipped a cell by the bound.  Masks are read through
+// L1.
 __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, State *states, Sched *sc)
 {
+    __shared__ int cell_list[8][kGoalGroup * 32];
     const int n = sc->n_slots;
     const int total = sc->goal_start[n];
     const int lane = threadIdx.x & 31;
+    const unsigned lower = (1u << lane) - 1u;
+    int *list = cell_list[threadIdx.x >> 5];
     while (true) {
         int g = 0;
         if (lane == 0)
@@ -1317,13 +1328,14 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
         const Inst &I = insts[slot];
         State &S = states[slot];
         const int local = g - sc->goal_start[slot];
-        const int idx = local / I.win_chunks;
-        const int wc = local - idx * I.win_chunks;
+        const int groups = goal_groups(I);
+        const int idx = local / groups;
+        const int wg = local - idx * groups;
         // a node to search (nodes with a kept result were resolved when
         // listed); the key of this heading and cost marks a complete result
         const int pos = I.nodes[idx];
         const unsigned long long key = memo_key_of(I, pos);
-        if (wc == 0 && lane == 0)
+        if (wg == 0 && lane == 0)
             goal_check_node(I, S, pos);
         const Foot f = foot_of(I, I.blocked, I.clear);
         GoalLane gl;
@@ -1332,11 +1344,32 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
         gl.x = pos - gl.z * I.W;
         gl.heading = I.heading[pos];
         gl.cost = I.cost[pos];
-        const int nz = window_count(gl.z, I.dist_tol, gl.zlo);
-        gl.nx = window_count(gl.x, I.dist_tol, gl.xlo);
-        const int wtotal = gl.nx > 0 ? nz * gl.nx : 0;
-        gl.w = wc * 32 + lane;
-        gl.wend = min(wtotal, (wc + 1) * 32);
+        int zlo, xlo;
+        const int nz = window_count(gl.z, I.dist_tol, zlo);
+        const int nx = window_count(gl.x, I.dist_tol, xlo);
+        const int wtotal = nx > 0 ? nz * nx : 0;
+        __syncwarp();  // the previous unit's lanes are done with the list
+        int cnt = 0;
+        for (int q = 0; q < kGoalGroup; q++) {
+            const int w = (wg * kGoalGroup + q) * 32 + lane;
+            int cell = -1;
+            if (w < wtotal) {
+                const int zp = zlo + w / nx, xp = xlo + w % nx;
+                if (zp >= 0 && zp < I.H && xp >= 0 && xp < I.W) {
+                    const int cc = zp * I.W + xp;
+                    if (I.gd_flag[cc] == 1)
+                        cell = cc;
+                }
+            }
+            const unsigned m = __ballot_sync(kFull, cell >= 0);
+            if (cell >= 0)
+                list[cnt + __popc(m & lower)] = cell;
+            cnt += __popc(m);
+        }
+        __syncwarp();
+        gl.list = list;
+        gl.e = lane;
+        gl.cnt = cnt;
         gl.in_task = false;
         gl.best = kBigCost;
         gl.best_cell = -1;
