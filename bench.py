@@ -441,22 +441,27 @@ def run_mine(args, rank, world, local):
     d2h = R * (4 * 5 + 3 * 4 * 1024)
 
     # served at the C3 Poisson rates (latency from arrival to finish)
-    serving = {}
-    rng = np.random.default_rng(1234 + rank)
     n_rate = args.rate_requests
     rate_work = workload(rank, 10_000, n_rate)
     rate_dev = torch.from_numpy(rate_work[0]).cuda()
     rate_reqs = requests(*rate_work, device_frames=rate_dev)
-    for rate in [float(x) for x in args.rates.split(",") if x]:
-        arrival = np.cumsum(rng.exponential(1e3 / rate, n_rate))
-        out = serve(rate_reqs, arrival)
-        v = out["valid"] > 0
-        lat = out["latency_ms"][v]
-        serving[f"{rate:g}_req_s"] = {
-            "offered": rate, "requests": n_rate,
-            "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
-            "success_rate": float(v.mean()),
-            "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
+
+    def poisson():
+        res = {}
+        rng = np.random.default_rng(1234 + rank)
+        for rate in [float(x) for x in args.rates.split(",") if x]:
+            arrival = np.cumsum(rng.exponential(1e3 / rate, n_rate))
+            out = serve(rate_reqs, arrival)
+            v = out["valid"] > 0
+            lat = out["latency_ms"][v]
+            res[f"{rate:g}_req_s"] = {
+                "offered": rate, "requests": n_rate,
+                "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
+                "success_rate": float(v.mean()),
+                "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
+        return res
+
+    serving = poisson()
 
     # the same served workload with the learned expansion proposal attached
     learned = None
@@ -473,13 +478,15 @@ def run_mine(args, rank, world, local):
             v = out["valid"] > 0
             l_valid += int(v.sum())
             l_service.extend(out["service_ms"][v].tolist())
+        l_serving = poisson()  # the same arrivals, the network attached
         planner.set_proposal(None)
         l_t = max_over_ranks(l_ms, world)
         learned = {"value": sum_over_ranks(l_valid, world) / (l_t / 1e3), "unit": "plans/s",
                    "mix": args.mix, "success_rate": l_valid / float(R * args.steps),
                    "service_p50_ms": pct(l_service, 50), "service_p99_ms": pct(l_service, 99),
-                   "note": "same requests, network weights trained on the planner's own solves of "
-                           "held-out mixed-size requests (fastrrt_b200/train_proposal.py)"}
+                   "serving": l_serving,
+                   "note": "same requests and Poisson arrivals, network weights trained on the "
+                           "planner's own solves of held-out requests (fastrrt_b200/train_proposal.py)"}
 
     # kernel timing replay of one step (same inputs, kernels launched one by one)
     planner.profile(True)
