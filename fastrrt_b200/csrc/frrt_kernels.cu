@@ -531,8 +531,11 @@ __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, 
     }
 }
 
-// 32-cell window chunks per goal-search unit, and the units of one node
-constexpr int kGoalGroup = 4;
+// 32-cell window chunks per goal-search unit, and the units of one node.
+// One: with four, the units of a first iteration (one start window per
+// request) were too few to balance, and the launch ended with 8 % of its
+// warps active (2.1 ms against 0.7 ms, 512 fresh 256 x 256 requests).
+constexpr int kGoalGroup = 1;
 __device__ __forceinline__ int goal_groups(const Inst &I)
 {
     return (I.win_chunks + kGoalGroup - 1) / kGoalGroup;
