@@ -57,7 +57,7 @@ EXPORTS = [
     "fastrrt_batch_collect", "fastrrt_batch_path", "fastrrt_batch_release",
     "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
     "fastrrt_batch_kernel_times", "fastrrt_kernel_count", "fastrrt_kernel_name",
-    "fastrrt_batch_probes", "fastrrt_batch_serve",
+    "fastrrt_batch_probes", "fastrrt_batch_direct_connections", "fastrrt_batch_serve",
     # learned expansion proposal
     "fastrrt_mlp_create", "fastrrt_mlp_destroy", "fastrrt_mlp_get_weights",
     "fastrrt_mlp_set_weights", "fastrrt_mlp_forward", "fastrrt_mlp_gradients", "fastrrt_mlp_train",
@@ -146,6 +146,7 @@ def lib():
         "fastrrt_kernel_count": (C.c_int, []),
         "fastrrt_kernel_name": (C.c_char_p, [C.c_int]),
         "fastrrt_batch_probes": (C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+        "fastrrt_batch_direct_connections": (C.c_int, [vp, C.c_int, vp, vp, vp]),
         "fastrrt_mlp_create": (vp, [C.c_uint64, C.c_int]),
         "fastrrt_mlp_destroy": (None, [vp]),
         "fastrrt_mlp_get_weights": (C.c_int, [vp] + [f32p] * 6),

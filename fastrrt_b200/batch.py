@@ -187,5 +187,16 @@ class BatchPlanner:
                                                    _lib.C.byref(p)), "batch_probes")
         return {"k_expand": a.value, "k_goal": g.value, "k_gd_eval": p.value}
 
+    def direct_connections(self, slot, W, H):
+        """the goal direct connections of `slot`'s W x H cells evaluated so
+        far: (flag uint8, 0 / 1 or 255 = not evaluated, cost, heading)"""
+        flag = np.zeros(W * H, np.uint8)
+        cost = np.zeros(W * H, np.float32)
+        heading = np.zeros(W * H, np.float32)
+        _lib.check(_lib.lib().fastrrt_batch_direct_connections(
+            self._h, int(slot), flag.ctypes.data, cost.ctypes.data, heading.ctypes.data),
+            "batch_direct_connections")
+        return flag, cost, heading
+
     def release(self, slot):
         _lib.check(_lib.lib().fastrrt_batch_release(self._h, slot), "batch_release")

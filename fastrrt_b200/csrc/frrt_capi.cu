@@ -1183,6 +1183,31 @@ int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t
     return 0;
 }
 
+int fastrrt_batch_direct_connections(void *batch, int slot, uint8_t *flag, float *cost,
+                                     float *heading)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || slot < 0 || slot >= b->eng->n_slots() || !flag || !cost || !heading) {
+        set_error("batch_direct_connections: bad arguments");
+        return -1;
+    }
+    Engine &e = *b->eng;
+    if (!e.sync())
+        return -1;
+    const Inst &I = e.inst(slot);
+    const size_t cells = (size_t)I.W * I.H;
+    cudaError_t err = cudaMemcpy(flag, I.gd_flag, cells, cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess)
+        err = cudaMemcpy(cost, I.gd_cost, cells * sizeof(float), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess)
+        err = cudaMemcpy(heading, I.gd_heading, cells * sizeof(float), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) {
+        set_error(std::string("batch_direct_connections: ") + cudaGetErrorString(err));
+        return -1;
+    }
+    return 0;
+}
+
 int fastrrt_batch_profile(void *batch, int on)
 {
     auto *b = static_cast<Batch *>(batch);

@@ -250,6 +250,13 @@ int fastrrt_kernel_count(void);
  * evaluation */
 int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute);
 const char *fastrrt_kernel_name(int k);
+/* inspection, no counterpart in the reference (whose eager pass fills these
+ * arrays at set_plan_data, graph_direct_goal_connection.cu:169-227): the
+ * goal direct connections of `slot`'s cells as evaluated so far, W x H each
+ * (host arrays): flag 0 / 1, or 255 for a cell not evaluated yet; the cost
+ * and heading of connected cells */
+int fastrrt_batch_direct_connections(void *batch, int slot, uint8_t *flag, float *cost,
+                                     float *heading);
 
 /* ---- part 5: the learned expansion proposal ------------------------------
  * No counterpart in the reference.  A BF16 MLP (1030 -> 256 -> 256 -> 128,

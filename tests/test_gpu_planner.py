@@ -98,6 +98,29 @@ def test_smart_expansion_matches_oracle(gpu, dev_orc, seed):
     assert np.array_equal(grid_types(p.export_graph_nodes()), op.type.reshape(H, W))
 
 
+@pytest.mark.parametrize("seed", [3, 11])
+def test_deferred_direct_connections_match_eager_oracle(gpu, dev_orc, seed):
+    """Every cell whose goal direct connection the iterations evaluated (on
+    demand, with the coarse first pass over every 16th sample before the walk
+    in order) has the flag of the oracle's eager pass over the whole frame
+    (processDirectGoalConnection at set_plan_data), and a connected cell its
+    cost and heading."""
+    cls, start, goal = synth.c0_request(seed)
+    B = gpu.BatchPlanner(1, W, H)
+    B.admit_many([gpu.make_request(cls, COSTS, start, goal, seed=seed, max_iterations=30)])
+    B.run(60, 1)
+    flag, cost, heading = B.direct_connections(0, W, H)
+    op, _ = run_oracle(dev_orc, cls, start, goal, seed, 0)
+    done = flag != 255
+    assert done.sum() > 1000
+    want = np.asarray(op.gd_flag).reshape(-1)[done].astype(np.int32)
+    assert np.array_equal(flag[done].astype(np.int32), want)
+    ok = done & (flag == 1)
+    assert ok.sum() > 0
+    assert np.max(np.abs(cost[ok] - np.asarray(op.gd_cost)[ok])) <= 1e-3
+    assert np.array_equal(heading[ok], np.asarray(op.gd_heading)[ok])
+
+
 @pytest.mark.parametrize("seed", [3, 5, 7])
 def test_probe_counts_by_phase(gpu, dev_orc, seed):
     """Footprint probes of the reference algorithm, per phase, for one request.
