@@ -348,14 +348,19 @@ struct KinTask {
 
     __device__ int advance(const Foot &f, unsigned long long &probes, int budget = kNoBudget)
     {
+        // the next step's cosine and sine are computed before this step's
+        // cell tests (they depend only on the heading), so they overlap
+        float nc = cosf(heading + beta), ns = sinf(heading + beta);
         while (size < maxSize) {
             if (budget-- <= 0)
                 return kTaskPaused;
             if (loop_count++ > loop_max)
                 break;
-            x += ds * cosf(heading + beta);
-            y += ds * sinf(heading + beta);
+            x += ds * nc;
+            y += ds * ns;
             heading += hif;
+            nc = cosf(heading + beta);
+            ns = sinf(heading + beta);
             // convert_map_pose_to_waypoint (kinematics.cu:25-46)
             const double2 coord = {x, y};
             const int lpx = (int)(og_x + coord.y);
@@ -600,10 +605,14 @@ struct HermTask {
         if (coarse)
             return advance_coarse(f, probes, budget);
         const int stop = numPoints - i > budget ? i + budget : numPoints;
+        // the next sample's position is computed before this sample's tests
+        // (it does not depend on them), so the two FP64 chains overlap
+        double tn = sample_t(i), pxn, pzn;
+        ref_pos(tn, pxn, pzn);
         for (; i < stop; ++i) {
-            const double t = sample_t(i);
-            double px, pz;
-            ref_pos(t, px, pz);
+            const double t = tn, px = pxn, pz = pzn;
+            tn = sample_t(i + 1);
+            ref_pos(tn, pxn, pzn);
             if (px < 0 || px >= W)
                 continue;
             if (pz < 0 || pz >= H)
