@@ -118,7 +118,9 @@ def test_deferred_direct_connections_match_eager_oracle(gpu, dev_orc, seed):
     ok = done & (flag == 1)
     assert ok.sum() > 0
     assert np.max(np.abs(cost[ok] - np.asarray(op.gd_cost)[ok])) <= 1e-3
-    assert np.array_equal(heading[ok], np.asarray(op.gd_heading)[ok])
+    # the cell's heading to the goal comes from atan2f: the device's and the
+    # host library's differ in the last bit
+    assert np.max(np.abs(heading[ok] - np.asarray(op.gd_heading)[ok])) <= 1e-5
 
 
 @pytest.mark.parametrize("seed", [3, 5, 7])
