@@ -552,15 +552,20 @@ struct HermTask {
     }
     __device__ int advance_coarse(const Foot &f, unsigned long long &probes, int budget)
     {
+        // a sample and its predecessor, and those of the next coarse sample
+        // before this one's tests (they depend on none of them)
+        double tn = sample_t(i), pxn, pzn, qxn, qzn;
+        ref_pos(tn, pxn, pzn);
+        ref_pos(sample_t(i - 1), qxn, qzn);
         for (; i < numPoints; i += coarse) {
             if (budget-- <= 0)
                 return kTaskPaused;
-            const double t = sample_t(i);
-            double px, pz, qx, qz;
-            ref_pos(t, px, pz);
+            const double t = tn, px = pxn, pz = pzn, qx = qxn, qz = qzn;
+            tn = sample_t(i + coarse);
+            ref_pos(tn, pxn, pzn);
+            ref_pos(sample_t(i + coarse - 1), qxn, qzn);
             if (px < 0 || px >= W || pz < 0 || pz >= H)
                 continue;
-            ref_pos(sample_t(i - 1), qx, qz);
             if (qx < 0 || qx >= W || qz < 0 || qz >= H)
                 continue;
             const int cx = (int)(px);
