@@ -1696,7 +1696,9 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 3);
     mark();
-    k_gd_demand<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    // one warp per (node, window chunk): its grid follows the machine, not
+    // the frame's sweep chunks (16 for one 256 x 256 slot)
+    k_gd_demand<<<L.sms * 8, 256, 0, st>>>(d_inst, d_state, d_sched);
     mark();
     k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 2);
     mark();
