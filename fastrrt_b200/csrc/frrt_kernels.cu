@@ -22,12 +22,12 @@
 //   k_finish      connection / start adds, loop bookkeeping (fastrrt.cpp:130-180)
 //
 // Sweep kernels read the int8 type grid 16 cells at a time (one 16-byte
-// load per thread).  The expansion and goal kernels are persistent: blocks
-// pull chunks of one slot's work from a global counter and stage that
-// slot's bit-packed frame masks into shared memory with the bulk-copy (TMA)
-// engine.  Concurrent claims on one target cell are resolved by
-// atomicMin on the expanding cell index, which makes every iteration
-// deterministic for a given seed.
+// load per thread).  The expansion and goal kernels are persistent: warps
+// pull work from global counters across all slots and read the slots'
+// bit-packed frame masks through L1 (a slot's masks are 16 KB at 256 x 256).
+// Concurrent claims on one target cell are resolved by atomicMin on the
+// expanding cell index, which makes every iteration deterministic for a
+// given seed.
 #include <climits>
 #include <cstdio>
 
@@ -621,50 +621,6 @@ struct KinLane {
     __device__ bool resolve(bool ok) { return k.resolve(ok); }
     __device__ float probe_angle() const { return k.heading; }
 };
-
-// shared-memory frame staging state of a persistent block
-struct Stage {
-    int cur;
-    bool broken;
-    unsigned phase;
-};
-
-__device__ inline void stage_for(const Inst &I, int slot, Stage &sg, uint32_t *smem, int smem_words,
-                                 uint64_t *bar, State *states, const uint32_t *&blk,
-                                 const uint32_t *&clr)
-{
-    const bool fits = smem_words > 0 && I.mask_words <= smem_words && !sg.broken;
-    if (fits) {
-        if (slot != sg.cur) {
-            if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, bar, sg.phase))
-                sg.cur = slot;
-            else {
-                sg.broken = true;
-                sg.cur = -1;
-                if (threadIdx.x == 0)
-                    atomicExch(&states[slot].error, 1);
-            }
-        }
-    }
-    if (fits && !sg.broken) {
-        blk = smem;
-        clr = smem + smem_words;
-    } else {
-        blk = I.blocked;
-        clr = I.clear;
-    }
-}
-
-__device__ inline void stage_drain(Stage &sg, uint64_t *bar)
-{
-    if (sg.broken)
-        for (long k = 0; k < kWaitLimit; k++)
-            if (mbar_try_wait(bar, sg.phase ^ 1u))
-                break;
-}
-
-// expand_node (graph_expansion.cu:103-145): every listed NODE cell draws a
-// steering angle and a length, integrates, and claims its end cell
 
 // the winner of each claimed cell applies expand_node's transitions
 __global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states, const Sched *sc)
@@ -2225,7 +2181,8 @@ __global__ void __launch_bounds__(256) k_candidates(const Inst *insts, int slot,
                                                     const int32_t *sx, const int32_t *sz,
                                                     const float *steer, const float *len,
                                                     float velocity, float4 *out,
-                                                    unsigned long long *probes_out, int smem_words)
+                                                    unsigned long long *probes_out, int smem_words,
+                                                    int *bad_cell)
 {
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ __align__(8) uint64_t bar;
@@ -2250,16 +2207,26 @@ __global__ void __launch_bounds__(256) k_candidates(const Inst *insts, int slot,
     for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
         const long i = base + threadIdx.x;
         const bool has = i < n;
+        // a start cell outside the frame is rejected (and reported) without
+        // reading the grids at it
+        bool inside = false;
         KinLane t;
         if (has) {
-            const long pos = (long)sz[i] * I.W + sx[i];
-            t.k.init(I, sx[i], sz[i], steer[i], len[i], velocity, I.heading[pos], I.cost[pos]);
+            const int cx = sx[i], cz = sz[i];
+            inside = cx >= 0 && cx < I.W && cz >= 0 && cz < I.H;
+            if (inside) {
+                const long pos = (long)cz * I.W + cx;
+                t.k.init(I, cx, cz, steer[i], len[i], velocity, I.heading[pos], I.cost[pos]);
+            } else if (bad_cell) {
+                atomicOr(bad_cell, 1);
+            }
         }
-        run_warp(t, has, f, probes, [](const KinLane &q) { return q.k.pend_x; },
+        run_warp(t, inside, f, probes, [](const KinLane &q) { return q.k.pend_x; },
                  [](const KinLane &q) { return q.k.pend_z; });
         if (has)
-            out[i] = t.k.ok ? make_float4((float)t.k.last_x, (float)t.k.last_z, t.k.nodeCost, t.k.heading)
-                            : make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
+            out[i] = (inside && t.k.ok)
+                         ? make_float4((float)t.k.last_x, (float)t.k.last_z, t.k.nodeCost, t.k.heading)
+                         : make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
     }
     probes = warp_sum64(probes);
     if ((threadIdx.x & 31) == 0 && probes && probes_out)
@@ -2268,7 +2235,7 @@ __global__ void __launch_bounds__(256) k_candidates(const Inst *insts, int slot,
 
 void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, const int32_t *sz,
                        const float *steer, const float *len, float velocity, float4 *out,
-                       unsigned long long *probes, const Launch &L, cudaStream_t st)
+                       unsigned long long *probes, const Launch &L, cudaStream_t st, int *bad_cell)
 {
     if (n <= 0)
         return;
@@ -2277,7 +2244,7 @@ void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, c
         grid = L.work_blocks;
     const size_t smem = (size_t)L.smem_words * 2 * 4;
     k_candidates<<<grid, 256, smem, st>>>(d_inst, slot, n, sx, sz, steer, len, velocity, out, probes,
-                                          L.smem_words);
+                                          L.smem_words, bad_cell);
 }
 
 __global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, int n, const int32_t *x,
@@ -2309,14 +2276,21 @@ __global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, in
     for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
         const long i = base + threadIdx.x;
         const bool has = i < n;
+        // a start cell outside the frame is not connected (its cost and
+        // traversability are not read)
+        bool inside = false;
         PairLane t;
-        if (has)
-            t.h.init(I, f, maxc, x[i], z[i], lh[i], gx[i], gz[i], gh[i], safe,
-                     I.cost[(long)z[i] * I.W + x[i]]);
-        run_warp(t, has, f, probes, [](const PairLane &q) { return q.h.last_x; },
+        if (has) {
+            const int cx = x[i], cz = z[i];
+            inside = cx >= 0 && cx < I.W && cz >= 0 && cz < I.H;
+            if (inside)
+                t.h.init(I, f, maxc, cx, cz, lh[i], gx[i], gz[i], gh[i], safe,
+                         I.cost[(long)cz * I.W + cx]);
+        }
+        run_warp(t, inside, f, probes, [](const PairLane &q) { return q.h.last_x; },
                  [](const PairLane &q) { return q.h.last_z; });
         if (has)
-            out[i] = t.h.result();
+            out[i] = inside ? t.h.result() : -1.0f;
     }
     probes = warp_sum64(probes);
     if ((threadIdx.x & 31) == 0 && probes && probes_out)
@@ -2345,8 +2319,11 @@ __global__ void k_feasible(const Inst *insts, int slot, int n, const int32_t *x,
     const Foot f = foot_of(I, I.blocked, I.clear);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long pr = 0;
+    // a cell outside the frame is reported infeasible without reading it
     if (i < n)
-        out[i] = feasible_scalar(f, x[i], z[i], a[i], pr) ? 1 : 0;
+        out[i] = (x[i] >= 0 && x[i] < I.W && z[i] >= 0 && z[i] < I.H && feasible_scalar(f, x[i], z[i], a[i], pr))
+                     ? 1
+                     : 0;
     pr = warp_sum64(pr);
     if ((threadIdx.x & 31) == 0 && pr && probes_out)
         atomicAdd(probes_out, pr);

@@ -100,7 +100,8 @@ void launch_count(const Inst *d_inst, const int *d_slots, int n, int max_cells, 
 // per-candidate microbenchmarks over one frame slot
 void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, const int32_t *sz,
                        const float *steer, const float *len, float velocity, float4 *out,
-                       unsigned long long *probes, const Launch &L, cudaStream_t st);
+                       unsigned long long *probes, const Launch &L, cudaStream_t st,
+                       int *bad_cell = nullptr);
 void launch_hermite_pairs(const Inst *d_inst, int slot, int n, const int32_t *x, const int32_t *z,
                           const float *lh, const int32_t *gx, const int32_t *gz, const float *gh,
                           float max_curvature, int safe, float *out, unsigned long long *probes,

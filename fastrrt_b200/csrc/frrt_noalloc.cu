@@ -9,7 +9,10 @@
 // while other work is in flight can still call it.  Its working memory (the
 // instance record and the three bit-packed frame masks) lives in one
 // file-scope __device__ array, sized for frames up to 1024 x 1024 cells and
-// kept by every GPU that loads the library until the process exits.
+// kept by every GPU that loads the library until the process exits.  The
+// array's device address is looked up once per device and kept: a process
+// that calls cudaDeviceReset must not call this entry point afterwards on
+// that device (the reloaded module may place the array elsewhere).
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -32,6 +35,7 @@ constexpr size_t kInstOffset = 0;
 constexpr size_t kStateOffset = 1024;
 constexpr size_t kSlotOffset = 1536;     // one int: the slot list {0}
 constexpr size_t kBadOffset = 1540;      // one int: class id outside the cost table
+constexpr size_t kBadCellOffset = 1544;  // one int: candidate start cell outside the frame
 constexpr size_t kMaskOffset = 2048;     // blocked, clear, dilation scratch
 constexpr size_t kScratchBytes = kMaskOffset + 3 * 4 * kMaskWordsMax;
 static_assert(sizeof(Inst) <= kStateOffset - kInstOffset, "instance record exceeds its space");
@@ -121,6 +125,7 @@ extern "C" int fastrrt_candidates_kinematic_noalloc(
     State *d_state = reinterpret_cast<State *>(base + kStateOffset);
     int *d_slots = reinterpret_cast<int *>(base + kSlotOffset);
     int *d_bad = reinterpret_cast<int *>(base + kBadOffset);
+    int *d_bad_cell = reinterpret_cast<int *>(base + kBadCellOffset);
     uint32_t *masks = reinterpret_cast<uint32_t *>(base + kMaskOffset);
 
     // the instance record a candidates context would hold for this frame
@@ -169,19 +174,23 @@ extern "C" int fastrrt_candidates_kinematic_noalloc(
     L.smem_words = 0;  // masks are read from the array (through L2), not staged
     launch_candidates(d_inst, 0, n, sx, sz, steer, length, velocity_m_s,
                       reinterpret_cast<float4 *>(out4), reinterpret_cast<unsigned long long *>(probes),
-                      L, st);
-    int bad = 0;
+                      L, st, d_bad_cell);
+    int bad[2] = {0, 0};  // class id flag, cell flag (adjacent ints)
     e = cudaGetLastError();
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(bad, d_bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         set_error(std::string("candidates_noalloc: ") + cudaGetErrorString(e));
         return -1;
     }
-    if (bad) {
+    if (bad[0]) {
         set_error("candidates_noalloc: frame class id outside the class-cost table");
+        return -1;
+    }
+    if (bad[1]) {
+        set_error("candidates_noalloc: candidate start cell outside the frame");
         return -1;
     }
     return 0;

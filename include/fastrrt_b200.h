@@ -135,13 +135,17 @@ int fastrrt_candidates_hermite_device(void *ctx, int n, const int32_t *x, const 
  * the frame's width*height class ids, its n_classes costs (cost < 0 =
  * obstacle), the width*height heading and cost grids the candidates start
  * from, the n candidates and out4 (n float4); *probes, when given, is added
- * to.  Frames larger than 1024 x 1024 cells are rejected with an error, and
- * candidate cells must lie in the frame.  The first call on a device looks
- * up the array's address on that device: make it before any stream capture.
- * The call runs on `stream` (NULL = default) and returns after the stream
- * has finished it.  Calls share the array: calls from this library's callers
- * are serialised by a lock, but work that overlaps on the GPU from another
- * route (e.g. the same library loaded twice in one process) would race. */
+ * to.  Frames larger than 1024 x 1024 cells are rejected with an error; a
+ * candidate whose start cell lies outside the frame gets the rejected row
+ * (-1, -1, 0, 0) and the call returns an error.  The first call on a device
+ * looks up the array's address on that device and keeps it, so the entry
+ * point must not be used on a device after cudaDeviceReset.  The call runs
+ * on `stream` (NULL = default), copies its small error flags back and
+ * synchronises that stream before it returns, so it must not be called while
+ * `stream` is being captured into a CUDA graph.  Calls share the array:
+ * calls from this library's callers are serialised by a lock, but work that
+ * overlaps on the GPU from another route (e.g. the same library loaded twice
+ * in one process) would race. */
 int fastrrt_candidates_kinematic_noalloc(int width, int height, const uint8_t *class_ids,
                                          const float *class_costs, int n_classes,
                                          const float *heading_grid, const float *cost_grid,

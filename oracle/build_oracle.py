@@ -24,9 +24,20 @@ def build_oracle(force=False):
     return ORACLE_SO
 
 
-def build_ref(reference="/root/reference", jobs=8):
+# Where the reference source tree is read from: $FASTRRT_REFERENCE, else the
+# read-only mount this recipe was written against.
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_root():
+    """the reference tree to compile from ($FASTRRT_REFERENCE or the default mount)"""
+    return os.environ.get("FASTRRT_REFERENCE") or DEFAULT_REFERENCE
+
+
+def build_ref(reference=None, jobs=8):
     """Compile the reference's sources in place; skipped when the tree is absent
     (the prebuilt library travels with the repository snapshot)."""
+    reference = reference or reference_root()
     if not os.path.isdir(os.path.join(reference, "src", "cuda")):
         return REF_SO if os.path.exists(REF_SO) else None
     subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), f"-j{jobs}",

@@ -29,8 +29,8 @@ MAX_STEER = math.radians(40.0)
 LR = 5.4 / 2
 
 
-def main(reference="/root/reference"):
-    build_oracle.build_ref(reference)
+def main(reference=None):
+    build_oracle.build_ref(reference or build_oracle.reference_root())
     if O.ref_lib() is None:
         raise SystemExit("oracle/_ref not built")
     cls, _, _ = synth.c0_request(3)

@@ -39,22 +39,38 @@ def via_context(F, torch, cls, heading, cost, sx, sz, steer, seg):
     return out.cpu().numpy(), int(pr.item())
 
 
-def via_noalloc(F, torch, cls, heading, cost, sx, sz, steer, seg):
-    H, W = cls.shape
-    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    dcls, dcost_tab = dev(cls.astype(np.uint8)), dev(synth.CLASS_COSTS)
-    dh, dc = dev(heading), dev(cost)
-    dsx, dsz, dst, dln = dev(sx), dev(sz), dev(steer), dev(seg)
-    out = torch.full((len(sx), 4), 7.0, dtype=torch.float32, device="cuda")
-    pr = torch.zeros(1, dtype=torch.int64, device="cuda")
+class NoAllocCall:
+    """device copies of one case's inputs and outputs; call() runs the entry
+    point on them and returns (rc, error text)"""
+
+    def __init__(self, F, torch, cls, heading, cost, sx, sz, steer, seg, costs=synth.CLASS_COSTS):
+        self.F, self.torch = F, torch
+        self.H, self.W = cls.shape
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        self.dcls, self.dcost_tab = dev(cls.astype(np.uint8)), dev(costs)
+        self.n_classes = len(costs)
+        self.dh, self.dc = dev(heading), dev(cost)
+        self.dsx, self.dsz, self.dst, self.dln = dev(sx), dev(sz), dev(steer), dev(seg)
+        self.n = len(sx)
+        self.out = torch.full((self.n, 4), 7.0, dtype=torch.float32, device="cuda")
+        self.pr = torch.zeros(1, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+
+    def call(self):
+        rc = self.F.lib().fastrrt_candidates_kinematic_noalloc(
+            self.W, self.H, self.dcls.data_ptr(), self.dcost_tab.data_ptr(), self.n_classes,
+            self.dh.data_ptr(), self.dc.data_ptr(), 22, 40, -1, -1, -1, -1, MS, LR, self.n,
+            self.dsx.data_ptr(), self.dsz.data_ptr(), self.dst.data_ptr(), self.dln.data_ptr(), 2.0,
+            self.out.data_ptr(), self.pr.data_ptr(), None)
+        return rc, (self.F._lib.last_error() if rc else "")
+
+
+def via_noalloc(F, torch, *args):
+    c = NoAllocCall(F, torch, *args)
+    rc, err = c.call()
+    assert rc == 0, err
     torch.cuda.synchronize()
-    rc = F.lib().fastrrt_candidates_kinematic_noalloc(
-        W, H, dcls.data_ptr(), dcost_tab.data_ptr(), len(synth.CLASS_COSTS), dh.data_ptr(),
-        dc.data_ptr(), 22, 40, -1, -1, -1, -1, MS, LR, len(sx), dsx.data_ptr(), dsz.data_ptr(),
-        dst.data_ptr(), dln.data_ptr(), 2.0, out.data_ptr(), pr.data_ptr(), None)
-    assert rc == 0, F._lib.last_error()
-    torch.cuda.synchronize()
-    return out.cpu().numpy(), int(pr.item())
+    return c.out.cpu().numpy(), int(c.pr.item())
 
 
 @pytest.fixture(scope="module")
@@ -84,3 +100,43 @@ def test_noalloc_rejects_oversized_frames(gpu):
         2.0, one, None, None)
     assert rc < 0
     assert "1024" in gpu._lib.last_error()
+
+
+def test_noalloc_allocates_no_device_memory(gpu, torch_gpu):
+    # after a warm-up call (module load, first launches) a further call leaves
+    # the device's free memory unchanged: nothing was allocated or kept
+    torch = torch_gpu
+    c = NoAllocCall(gpu, torch, *case(13, 256, 0.15))
+    assert c.call()[0] == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    rc, err = c.call()
+    torch.cuda.synchronize()
+    assert rc == 0, err
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
+def test_noalloc_rejects_bad_class_ids_and_cells(gpu, torch_gpu):
+    torch = torch_gpu
+    cls, heading, cost, sx, sz, steer, seg = case(14, 128, 0.15)
+    # a class id beyond the cost table
+    bad = cls.copy()
+    bad[5, 7] = 9
+    rc, err = NoAllocCall(gpu, torch, bad, heading, cost, sx, sz, steer, seg, costs=synth.CLASS_COSTS[:4]).call()
+    assert rc < 0 and "class id" in err
+    # one candidate whose start cell lies outside the frame: its row is the
+    # rejected row, the others match the allocating entry point, and the call
+    # reports the cell
+    sx2 = sx.copy()
+    sx2[3] = 128
+    c = NoAllocCall(gpu, torch, cls, heading, cost, sx2, sz, steer, seg)
+    rc, err = c.call()
+    assert rc < 0 and "outside the frame" in err
+    torch.cuda.synchronize()
+    got = c.out.cpu().numpy()
+    assert np.array_equal(got[3], [-1.0, -1.0, 0.0, 0.0])
+    want, _ = via_context(gpu, torch, cls, heading, cost, sx, sz, steer, seg)
+    keep = np.arange(len(sx)) != 3
+    assert np.array_equal(got[keep].view(np.uint32), want[keep].view(np.uint32))
+    # the next good call succeeds: the flags start at zero on every call
+    assert via_noalloc(gpu, torch, cls, heading, cost, sx, sz, steer, seg)[1] > 0
