@@ -297,9 +297,12 @@ constexpr int kNoBudget = 1 << 30;
 // lane-refilling kernels (8 measured best of 8, 16 and unbounded on served
 // 256 x 256 planning)
 constexpr int kStepSamples = 8;
-// sample stride of the first pass of the direct goal connections (16
-// measured best of 4, 8, 16, 24 and 32 on served 256 x 256 planning)
-constexpr int kCoarseStride = 16;
+// sample stride of the first pass of the direct goal connections (0: none);
+// a build-time knob for measurement
+#ifndef FRRT_COARSE_STRIDE
+#define FRRT_COARSE_STRIDE 16
+#endif
+constexpr int kCoarseStride = FRRT_COARSE_STRIDE;
 
 // check_kinematic_new_path (kinematics.cu:123-231)
 struct KinTask {
@@ -421,14 +424,13 @@ struct KinTask {
     __device__ float probe_angle() const { return heading; }
 };
 
-// checkDirectConnectionToGoal (graph_direct_goal_connection.cu:16-167) with
-// isDistanceToGoalProcessed = false
+// The constants of one checkDirectConnectionToGoal curve
+// (graph_direct_goal_connection.cu:16-167, isDistanceToGoalProcessed =
+// false) and the reference's per-sample arithmetic; curve_warp walks it.
 struct HermTask {
-    int x, z, goal_x, goal_z, numPoints, i, last_x, last_z, W, H, trav;
-    float distance, t1x, t1y, t2x, t2y, nodeCost, max_curvature, pend_heading;
-    float pend_cost;           // the last cell's intrinsic cost, not yet added
-    int safe, ok, has_pend;
-    int coarse;                // stride of the first pass (0: none or done)
+    int x, z, goal_x, goal_z, numPoints, W, H, trav;
+    float distance, t1x, t1y, t2x, t2y, nodeCost, max_curvature;
+    int safe;
     const float *intrinsic;
     double inv_span;           // RN(1 / (numPoints - 1))
     double kap_hi2, kap_lo2;   // (max_curvature (1 +- 1e-6))^2
@@ -456,11 +458,7 @@ struct HermTask {
         t1y = distance * sinf(a1);
         t2x = distance * cosf(a2);
         t2y = distance * sinf(a2);
-        last_x = -1;
-        last_z = -1;
         nodeCost = start_cost;
-        has_pend = 0;
-        coarse = 0;
         trav = f.trav ? f.trav[pos] : 0;
         inv_span = 1.0 / (double)(numPoints - 1);
         const double khi = (double)max_curvature * (1.0 + 1e-6);
@@ -468,8 +466,6 @@ struct HermTask {
         kap_hi2 = khi * khi;
         kap_lo2 = klo * klo;
         safe = safe_zone;
-        i = 0;
-        ok = 0;
     }
 
     // the reference's evaluation of the curve at t: position, first and
@@ -535,166 +531,199 @@ struct HermTask {
         return __fma_rn(__fma_rn(-q, span, ak), inv_span, q);
     }
 
-    // A first pass over every `stride`-th sample before the walk in order.
-    // A sample in the frame whose predecessor is in the frame and in another
-    // cell is a sample the reference's loop tests, with the same heading, so
-    // a curvature or footprint failure there is the reference's answer
-    // (no connection) whatever it meets before.  Obstacles are wide next to
-    // the 1 px sample spacing and most curves to the goal fail, so the pass
-    // ends most of them after a few samples; a curve it clears is walked in
-    // order from the first sample.
-    __device__ void start_coarse(int stride)
-    {
-        if (stride >= 2) {
-            coarse = stride;
-            i = stride - 1;
-        }
-    }
-    __device__ int advance_coarse(const Foot &f, unsigned long long &probes, int budget)
-    {
-        // a sample and its predecessor, and those of the next coarse sample
-        // before this one's tests (they depend on none of them)
-        double tn = sample_t(i), pxn, pzn, qxn, qzn;
-        ref_pos(tn, pxn, pzn);
-        ref_pos(sample_t(i - 1), qxn, qzn);
-        for (; i < numPoints; i += coarse) {
-            if (budget-- <= 0)
-                return kTaskPaused;
-            const double t = tn, px = pxn, pz = pzn, qx = qxn, qz = qzn;
-            tn = sample_t(i + coarse);
-            ref_pos(tn, pxn, pzn);
-            ref_pos(sample_t(i + coarse - 1), qxn, qzn);
-            if (px < 0 || px >= W || pz < 0 || pz >= H)
-                continue;
-            if (qx < 0 || qx >= W || qz < 0 || qz >= H)
-                continue;
-            const int cx = (int)(px);
-            const int cz = (int)(pz);
-            if (cx == (int)(qx) && cz == (int)(qz))
-                continue;
-            double ddx, ddz, dd2x, dd2z;
-            ref_deriv(t, ddx, ddz, dd2x, dd2z);
-            if (max_curvature > 0 && ref_over(ddx, ddz, dd2x, dd2z, kap_hi2, kap_lo2)) {
-                ok = 0;
-                coarse = 0;
-                i = numPoints;
-                numPoints = -1;  // keep ok == 0 if advance() is called again
-                return kTaskDone;
-            }
-            if (safe && (trav & 0x100))
-                continue;
-            if (quick_feasible(f, cx, cz, probes))
-                continue;
-            const double s2 = ddx * ddx + ddz * ddz;
-            if (f.sat && s2 > 0.0) {
-                const float inv = rsqrtf((float)s2);
-                if (box_feasible(f, cx, cz, fabsf((float)ddz) * inv, fabsf((float)ddx) * inv, probes))
-                    continue;
-            }
-            pend_heading = atan2f(ddz, ddx) + kHalfPi;
-            last_x = cx;  // the probed cell (probe_x / probe_z)
-            last_z = cz;
-            i += coarse;
-            return kTaskProbe;
-        }
-        // nothing failed: the reference's walk from the first sample
-        coarse = 0;
-        i = 0;
-        last_x = -1;
-        last_z = -1;
-        return kTaskPaused;
-    }
+};
 
-    __device__ int advance(const Foot &f, unsigned long long &probes, int budget = kNoBudget)
-    {
-        if (coarse)
-            return advance_coarse(f, probes, budget);
-        const int stop = numPoints - i > budget ? i + budget : numPoints;
-        // the next sample's position is computed before this sample's tests
-        // (it does not depend on them), so the two FP64 chains overlap
-        double tn = sample_t(i), pxn, pzn;
-        ref_pos(tn, pxn, pzn);
-        for (; i < stop; ++i) {
-            const double t = tn, px = pxn, pz = pzn;
-            tn = sample_t(i + 1);
-            ref_pos(tn, pxn, pzn);
-            if (px < 0 || px >= W)
-                continue;
-            if (pz < 0 || pz >= H)
-                continue;
-            const int cx = (int)(px);
-            const int cz = (int)(pz);
-            if (cx == last_x && cz == last_z)
-                continue;
-            if (cx < 0 || cx >= W)
-                continue;
-            if (cz < 0 || cz >= H)
-                continue;
-            // added when the next cell is reached (or at the end), in order
-            settle();
-            pend_cost = intrinsic ? intrinsic[(long)cz * W + cx] : 0.0f;
-            has_pend = 1;
-            double ddx, ddz, dd2x, dd2z;
-            ref_deriv(t, ddx, ddz, dd2x, dd2z);
-            const double s2 = ddx * ddx + ddz * ddz;
-            if (max_curvature > 0 && ref_over(ddx, ddz, dd2x, dd2z, kap_hi2, kap_lo2)) {
-                settle();
-                ok = 0;
-                i = numPoints;
-                return kTaskDone;
-            }
-            last_x = cx;
-            last_z = cz;
-            if (safe && (trav & 0x100))
-                continue;
-            if (quick_feasible(f, last_x, last_z, probes))
-                continue;
-            // heading = atan2(ddz, ddx) + pi/2, so |cos| = |ddz| / |d| and
-            // |sin| = |ddx| / |d|
-            if (f.sat && s2 > 0.0) {
-                const float inv = rsqrtf((float)s2);
-                if (box_feasible(f, last_x, last_z, fabsf((float)ddz) * inv, fabsf((float)ddx) * inv,
-                                 probes))
-                    continue;
-            }
-            // the heading is only needed to probe the footprint
-            pend_heading = atan2f(ddz, ddx) + kHalfPi;
-            ++i;
-            return kTaskProbe;
-        }
-        if (i < numPoints)
-            return kTaskPaused;
-        settle();
-        if (numPoints <= 0 || (last_x != goal_x && last_z != goal_z))
-            ok = 0;
-        else
-            ok = 1;
-        return kTaskDone;
-    }
-    __device__ __forceinline__ void settle()
-    {
-        if (has_pend) {
-            nodeCost += pend_cost + 1;
-            has_pend = 0;
-        }
-    }
-    __device__ bool resolve(bool feasible)
-    {
-        if (!feasible) {
-            settle();
-            ok = 0;
-            coarse = 0;
-            i = numPoints;
-            numPoints = -1;  // keep ok == 0 if advance() is called again
-            return false;
-        }
+// The full footprint test of one cell by the whole warp (all lanes pass the
+// same arguments): the row-interval test clears most feasible footprints,
+// the probe loop in the reference's order decides the rest.  `cnt` gets the
+// reference's probe count.
+__device__ inline bool footprint_warp(const Foot &f, int x, int z, float angle, int lane, unsigned &cnt)
+{
+    if (rows_clear_warp(f, x, z, cosf(angle), sinf(angle), lane)) {
+        cnt = full_probes(f);  // feasible: the reference runs all its probes
         return true;
     }
-    __device__ float probe_angle() const { return pend_heading; }
-    __device__ int probe_x() const { return last_x; }
-    __device__ int probe_z() const { return last_z; }
-    __device__ float result() const { return ok ? nodeCost : -1.0f; }
-};
+    return probe_warp(f, x, z, angle, lane, cnt);
+}
+
+// checkDirectConnectionToGoal (graph_direct_goal_connection.cu:16-167) of
+// one curve, evaluated by the whole warp: lane k takes sample base + k, with
+// the same arithmetic as HermTask.
+//
+// The reference walks the samples in order and tests a sample when it and
+// its cell lie in the frame and the cell differs from the last tested cell.
+// Every such sample either repeats that cell or becomes it, so the last
+// tested cell before sample i is the cell of the nearest earlier sample in
+// the frame: a ballot and a shuffle, with the last chunk's cell carried over.
+// A tested sample fails on curvature, else on its footprint; the reference's
+// answer is "no connection" at the first failure.  Lanes that need the full
+// probe loop are probed by the whole warp one after another in sample order,
+// up to the chunk's first curvature failure, so the first footprint failure
+// found is the reference's and `probes` gets the reference's exact count for
+// the walk.  The connection cost is the start cost plus (intrinsic + 1) of
+// every tested sample, added in sample order (one lane's term after
+// another), so the float sum rounds as the reference's.
+//
+// `coarse` >= 2 first tests every coarse-th sample whose predecessor lies in
+// the frame and in another cell: such a sample is one the reference tests,
+// so a failure there is the reference's answer whatever comes before it (a
+// curve rejected there adds nothing to `probes`); a curve the pass clears is
+// walked in order.  Every argument is the same in all lanes, and so is the
+// result: the reference's return value (the cost, or -1 for no connection;
+// callers treat any negative value as none, as the reference's do).
+__device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv, int x, int z,
+                                   float local_heading, int gx, int gz, float goal_heading, int safe,
+                                   float start_cost, int coarse, int lane, unsigned long long &probes)
+{
+    HermTask h;
+    h.init(I, f, max_curv, x, z, local_heading, gx, gz, goal_heading, safe, start_cost);
+    const int np = h.numPoints;
+    const bool skip_foot = safe && (h.trav & 0x100);
+    const unsigned lower = (1u << lane) - 1u;
+    if (coarse >= 2) {
+        for (int base = coarse - 1; base < np; base += 32 * coarse) {
+            const int i = base + lane * coarse;
+            bool test = false;
+            int cx = 0, cz = 0;
+            double t = 0.0;
+            if (i < np) {
+                t = h.sample_t(i);
+                double px, pz, qx, qz;
+                h.ref_pos(t, px, pz);
+                h.ref_pos(h.sample_t(i - 1), qx, qz);
+                if (!(px < 0 || px >= h.W || pz < 0 || pz >= h.H) &&
+                    !(qx < 0 || qx >= h.W || qz < 0 || qz >= h.H)) {
+                    cx = (int)(px);
+                    cz = (int)(pz);
+                    const int ax = (int)(qx), az = (int)(qz);
+                    // both cells inside the frame (see the walk below)
+                    test = cx >= 0 && cx < h.W && cz >= 0 && cz < h.H && ax >= 0 && ax < h.W && az >= 0 &&
+                           az < h.H && !(cx == ax && cz == az);
+                }
+            }
+            bool over = false, hard = false;
+            float ang = 0.0f;
+            if (test) {
+                double ddx, ddz, dd2x, dd2z;
+                h.ref_deriv(t, ddx, ddz, dd2x, dd2z);
+                over = max_curv > 0 && h.ref_over(ddx, ddz, dd2x, dd2z, h.kap_hi2, h.kap_lo2);
+                unsigned long long uncounted = 0;
+                if (!over && !skip_foot && !quick_feasible(f, cx, cz, uncounted)) {
+                    const double s2 = ddx * ddx + ddz * ddz;
+                    bool box = false;
+                    if (f.sat && s2 > 0.0) {
+                        const float inv = rsqrtf((float)s2);
+                        box = box_feasible(f, cx, cz, fabsf((float)ddz) * inv, fabsf((float)ddx) * inv,
+                                           uncounted);
+                    }
+                    if (!box) {
+                        hard = true;
+                        ang = atan2f(ddz, ddx) + kHalfPi;
+                    }
+                }
+            }
+            if (__any_sync(kFull, over))
+                return -1.0f;
+            unsigned hm = __ballot_sync(kFull, hard);
+            while (hm) {
+                const int leader = __ffs(hm) - 1;
+                hm &= hm - 1;
+                unsigned cnt = 0;
+                if (!footprint_warp(f, __shfl_sync(kFull, cx, leader), __shfl_sync(kFull, cz, leader),
+                                    __shfl_sync(kFull, ang, leader), lane, cnt))
+                    return -1.0f;
+            }
+        }
+    }
+    int last_x = -1, last_z = -1;  // the reference's last tested cell
+    float cost = start_cost;
+    for (int base = 0; base < np; base += 32) {
+        const int i = base + lane;
+        const double t = h.sample_t(i);
+        double px, pz;
+        h.ref_pos(t, px, pz);
+        // A sample counts when it lies in the frame and so does its cell.  The
+        // reference tests the cell's bounds after the position's (they differ
+        // for a NaN position: with numPoints == 1, t = 0 / 0); a sample that
+        // fails either is skipped and leaves the last tested cell as it was.
+        int cx = 0, cz = 0;
+        bool valid = false;
+        if (i < np && !(px < 0 || px >= h.W) && !(pz < 0 || pz >= h.H)) {
+            cx = (int)(px);
+            cz = (int)(pz);
+            valid = cx >= 0 && cx < h.W && cz >= 0 && cz < h.H;
+        }
+        const unsigned im = __ballot_sync(kFull, valid);
+        const unsigned below = im & lower;
+        const int src = below ? 31 - __clz(below) : lane;
+        const int qx = __shfl_sync(kFull, cx, src), qz = __shfl_sync(kFull, cz, src);
+        const int pcx = below ? qx : last_x, pcz = below ? qz : last_z;
+        const bool tested = valid && !(cx == pcx && cz == pcz);
+        float v = 0.0f;
+        bool over = false, hard = false;
+        float ang = 0.0f;
+        unsigned long long pl = 0;  // this lane's probes (feasible footprints)
+        double ddx = 0, ddz = 0, dd2x = 0, dd2z = 0;
+        if (tested) {
+            v = (h.intrinsic ? h.intrinsic[(long)cz * h.W + cx] : 0.0f) + 1;
+            h.ref_deriv(t, ddx, ddz, dd2x, dd2z);
+            over = max_curv > 0 && h.ref_over(ddx, ddz, dd2x, dd2z, h.kap_hi2, h.kap_lo2);
+        }
+        const unsigned om = __ballot_sync(kFull, over);
+        const int fc = om ? __ffs(om) - 1 : 32;  // first curvature failure
+        if (tested && lane < fc && !skip_foot && !quick_feasible(f, cx, cz, pl)) {
+            const double s2 = ddx * ddx + ddz * ddz;
+            bool box = false;
+            if (f.sat && s2 > 0.0) {
+                const float inv = rsqrtf((float)s2);
+                box = box_feasible(f, cx, cz, fabsf((float)ddz) * inv, fabsf((float)ddx) * inv, pl);
+            }
+            if (!box) {
+                hard = true;
+                ang = atan2f(ddz, ddx) + kHalfPi;
+            }
+        }
+        unsigned hm = __ballot_sync(kFull, hard);
+        int ff = 32;  // first footprint failure
+        unsigned fcnt = 0;
+        while (hm) {
+            const int leader = __ffs(hm) - 1;
+            hm &= hm - 1;
+            unsigned cnt = 0;
+            const bool ok = footprint_warp(f, __shfl_sync(kFull, cx, leader), __shfl_sync(kFull, cz, leader),
+                                           __shfl_sync(kFull, ang, leader), lane, cnt);
+            if (!ok) {
+                ff = leader;
+                fcnt = cnt;
+                break;
+            }
+            if (lane == leader)
+                pl += cnt;
+        }
+        const int fail = min(fc, ff);
+        if (lane < fail)
+            probes += pl;
+        if (fail < 32) {
+            if (ff < fc && lane == 0)
+                probes += fcnt;
+            return -1.0f;
+        }
+        unsigned tm = __ballot_sync(kFull, tested);
+        while (tm) {
+            const int k = __ffs(tm) - 1;
+            tm &= tm - 1;
+            cost += __shfl_sync(kFull, v, k);
+        }
+        if (im) {
+            const int hi = 31 - __clz(im);
+            last_x = __shfl_sync(kFull, cx, hi);
+            last_z = __shfl_sync(kFull, cz, hi);
+        }
+    }
+    if (np <= 0 || (last_x != gx && last_z != gz))
+        return -1.0f;
+    return cost;
+}
 
 // Drives one task per lane.  `has` says whether the lane holds a task.
 // Probes needing a full footprint scan are answered cooperatively.

@@ -284,16 +284,6 @@ void launch_frame_masks(const Inst *d_inst, State *d_state, const int *d_slots, 
 // goal direct-connection precompute (graph_direct_goal_connection.cu:169-227)
 // ---------------------------------------------------------------------------
 
-struct PrecompTask {
-    HermTask h;
-    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
-    {
-        return h.advance(f, p, budget);
-    }
-    __device__ bool resolve(bool ok) { return h.resolve(ok); }
-    __device__ float probe_angle() const { return h.pend_heading; }
-};
-
 // Deferred precompute.  Only the goal search reads a cell's direct connection
 // (graph_check_goal_reached.cu:53-63), and only for cells inside the window
 // of a node it searches, so each cell is evaluated the first time such a
@@ -333,33 +323,28 @@ void launch_direct_goal_reset(const Inst *d_inst, const int *d_slots, int n, int
     k_gd_reset<<<dim3(bx, n), 256, 0, st>>>(d_inst, d_slots, fresh);
 }
 
-// Evaluates the goal direct connection of one cell per lane (has = the lane
-// holds a cell); the warp answers full footprint probes together.
-__device__ void gd_eval_cell(const Inst &I, const Foot &f, bool has, int pos,
-                             unsigned long long &probes)
+// Evaluates the goal direct connection of one cell with the whole warp and
+// stores it as __CUDA_direct_connection does (graph_direct_goal_connection.cu:
+// 169-193).  Every lane passes the same cell.
+__device__ void gd_eval_cell(const Inst &I, const Foot &f, int pos, int lane, unsigned long long &probes)
 {
-    PrecompTask t;
-    float lh = 0.0f;
-    if (has) {
-        const int z = pos / I.W;
-        const int x = pos - z * I.W;
-        lh = compute_heading(x, z, I.goal_x, I.goal_z);
-        t.h.init(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading, 0,
-                 I.gd_cost[pos]);
-    }
-    run_warp(t, has, f, probes, [](const PrecompTask &q) { return q.h.last_x; },
-             [](const PrecompTask &q) { return q.h.last_z; });
-    if (has) {
-        if (t.h.ok) {
+    const int z = pos / I.W;
+    const int x = pos - z * I.W;
+    const float lh = compute_heading(x, z, I.goal_x, I.goal_z);
+    const float c = curve_warp(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading, 0,
+                               I.gd_cost[pos], kCoarseStride, lane, probes);
+    if (lane == 0) {
+        if (c >= 0) {
             I.gd_heading[pos] = lh;
-            I.gd_cost[pos] = t.h.nodeCost;
+            I.gd_cost[pos] = c;
         }
-        I.gd_flag[pos] = t.h.ok ? 1 : 0;
+        I.gd_flag[pos] = c >= 0 ? 1 : 0;
     }
 }
 
 // every still unknown cell of the listed slots (before the intrinsic costs
-// that the deferred evaluation reads are replaced)
+// that the deferred evaluation reads are replaced); a warp takes 32 cells at
+// a time and evaluates their unknown ones one after another
 __global__ void __launch_bounds__(256) k_gd_complete(const Inst *insts, State *states,
                                                      const int *slots)
 {
@@ -369,14 +354,20 @@ __global__ void __launch_bounds__(256) k_gd_complete(const Inst *insts, State *s
     if ((long)blockIdx.x * blockDim.x >= cells)
         return;
     const Foot f = foot_of(I, I.blocked, I.clear);
+    const int lane = threadIdx.x & 31;
     unsigned long long probes = 0;
-    for (long base = (long)blockIdx.x * blockDim.x; base < cells; base += (long)gridDim.x * blockDim.x) {
-        const long pos = base + threadIdx.x;
-        const bool has = pos < cells && I.gd_flag[pos] == kGdUnknown;
-        gd_eval_cell(I, f, has, has ? (int)pos : 0, probes);
+    for (long base = (long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < cells;
+         base += (long)gridDim.x * blockDim.x) {
+        const long pos = base + lane;
+        unsigned m = __ballot_sync(kFull, pos < cells && I.gd_flag[pos] == kGdUnknown);
+        while (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1;
+            gd_eval_cell(I, f, (int)(base + k), lane, probes);
+        }
     }
     probes = warp_sum64(probes);
-    if ((threadIdx.x & 31) == 0 && probes)
+    if (lane == 0 && probes)
         atomicAdd(&states[slot].probes_pre, probes);
 }
 
@@ -1002,85 +993,44 @@ __device__ inline bool coop_probe(const Foot &mine, int leader, int lane, int x,
     return probe_warp(f, bx, bz, ba, lane, cnt);
 }
 
-// Listed cells are handed to lanes one by one: a lane whose curve ended
-// takes the next cell (of any slot) at the start of the warp's next step, so
-// lanes stay busy although curve lengths differ a lot.  Full footprint
-// probes are answered by the whole warp.  Masks are read through L1.
+// One listed cell per warp at a time, grabbed from a counter over all slots:
+// the warp evaluates the cell's curve to the goal sample-parallel
+// (curve_warp), so a launch with few cells still spreads each curve over 32
+// lanes, and lanes never wait for a longer curve of another lane.  Masks are
+// read through L1.
 __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts, State *states, Sched *sc)
 {
     const int n = sc->n_slots;
     const int total = sc->gd_start[n];
     const int lane = threadIdx.x & 31;
-    const unsigned lower = (1u << lane) - 1u;
-    const unsigned lanes = lanes_in_use(total, gridDim.x * (blockDim.x >> 5));
-    PrecompTask t;
-    Foot f{};
-    const Inst *I = nullptr;
-    int slot = 0, pos = 0;
-    float lh = 0.0f;
-    bool active = false, exhausted = false;
-    unsigned long long probes = 0;
-    auto finish = [&]() {
-        if (t.h.ok) {
-            I->gd_heading[pos] = lh;
-            I->gd_cost[pos] = t.h.nodeCost;
-        }
-        I->gd_flag[pos] = t.h.ok ? 1 : 0;
-        if (probes)
-            atomicAdd(&states[slot].probes_pre, probes);
-        probes = 0;
-        active = false;
-    };
     while (true) {
-        if (!exhausted) {
-            const unsigned idle = __ballot_sync(kFull, !active) & lanes;
-            if (idle) {
-                int base = 0;
-                if (lane == 0)
-                    base = (int)atomicAdd(&sc->grab[2], (unsigned)__popc(idle));
-                base = __shfl_sync(kFull, base, 0);
-                if (base + __popc(idle) >= total)
-                    exhausted = true;
-                const int e = base + __popc(idle & lower);
-                if (((idle >> lane) & 1u) && e < total) {
-                    slot = find_slot(sc->gd_start, n, e);
-                    I = &insts[slot];
-                    pos = I->gd_list[e - sc->gd_start[slot]];
-                    f = foot_of(*I, I->blocked, I->clear);
-                    const int z = pos / I->W;
-                    const int x = pos - z * I->W;
-                    lh = compute_heading(x, z, I->goal_x, I->goal_z);
-                    t.h.init(*I, f, I->gd_max_curvature, x, z, lh, I->goal_x, I->goal_z,
-                             I->goal_heading, 0, I->gd_cost[pos]);
-                    t.h.start_coarse(kCoarseStride);
-                    active = true;
-                }
-            }
-        }
-        if (!__any_sync(kFull, active))
+        int e = 0;
+        if (lane == 0)
+            e = (int)atomicAdd(&sc->grab[2], 1u);
+        e = __shfl_sync(kFull, e, 0);
+        if (e >= total)
             break;
-        bool need = false;
-        if (active) {
-            const int r = t.advance(f, probes, kStepSamples);
-            if (r == kTaskProbe)
-                need = true;
-            else if (r == kTaskDone)
-                finish();
-        }
-        unsigned m = __ballot_sync(kFull, need);
-        bool ok_mine = true;
-        while (m) {
-            const int leader = __ffs(m) - 1;
-            m &= m - 1;
-            unsigned cnt = 0;
-            const bool ok = coop_probe(f, leader, lane, t.h.last_x, t.h.last_z, t.probe_angle(), cnt);
-            if (lane == leader) {
-                ok_mine = ok;
-                probes += cnt;
+        const int slot = find_slot(sc->gd_start, n, e);
+        const Inst &I = insts[slot];
+        const int pos = I.gd_list[e - sc->gd_start[slot]];
+        const Foot f = foot_of(I, I.blocked, I.clear);
+        const int z = pos / I.W;
+        const int x = pos - z * I.W;
+        const float lh = compute_heading(x, z, I.goal_x, I.goal_z);
+        unsigned long long probes = 0;
+        const float c = curve_warp(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading,
+                                   0, I.gd_cost[pos], kCoarseStride, lane, probes);
+        probes = warp_sum64(probes);
+        if (lane == 0) {
+            // __CUDA_direct_connection (graph_direct_goal_connection.cu:169-193)
+            if (c >= 0) {
+                I.gd_heading[pos] = lh;
+                I.gd_cost[pos] = c;
             }
+            I.gd_flag[pos] = c >= 0 ? 1 : 0;
+            if (probes)
+                atomicAdd(&states[slot].probes_pre, probes);
         }
-        if (need && !t.resolve(ok_mine))
-            finish();
     }
 }
 
@@ -1190,92 +1140,27 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
     }
 }
 
-// best connection of one graph node to a precomputed goal-connected cell in
-// its window (graph_check_goal_reached.cu:17-70), plus checkGoalReached for
-// the node (graph_best_node.cu:181-222)
-struct GoalLane {
-    HermTask h;
-    const int *list;           // the unit's connected window cells, in window order
-    int e, cnt;                // this lane's next entry (stride 32), entries
-    bool in_task;
-    int x, z;
-    float heading, cost, gd_cost_cur;
-    int cell_cur;
-    long long best;
-    int best_cell;
-    const Inst *I;
-    const volatile long long *global_best;
-    bool prune;
-    bool pruned;               // a window cell was skipped by the bound
-
-    __device__ int advance(const Foot &f, unsigned long long &probes, int budget)
-    {
-        while (true) {
-            if (!in_task) {
-                if (e >= cnt)
-                    return kTaskDone;
-                const int cell = list[e];
-                e += 32;
-                const int zp = cell / I->W, xp = cell - zp * I->W;
-                const float gdc = I->gd_cost[cell];
-                if (prune) {
-                    // the connection costs at least cost + 1 (the first sample)
-                    const float lb_total = (cost + 1.0f) + gdc;
-                    const long long lb = __float2ll_rd(100 * lb_total);
-                    if (lb > *global_best) {
-                        pruned = true;
-                        continue;
-                    }
-                }
-                h.init(*I, f, I->max_curvature, x, z, heading, xp, zp, I->gd_heading[cell], 1, cost);
-                cell_cur = cell;
-                gd_cost_cur = gdc;
-                in_task = true;
-            }
-            const int r = h.advance(f, probes, budget);
-            if (r != kTaskDone)
-                return r;
-            in_task = false;
-            if (h.ok) {
-                const float total = h.nodeCost + gd_cost_cur;
-                const long long lc = __float2ll_rd(100 * total);
-                if (lc <= best) {
-                    best = lc;
-                    best_cell = cell_cur;
-                }
-            }
-        }
-    }
-    __device__ bool resolve(bool ok)
-    {
-        if (!h.resolve(ok))
-            in_task = false;
-        return true;
-    }
-    __device__ float probe_angle() const { return h.pend_heading; }
-};
-
 __device__ __forceinline__ unsigned long long connection_key(long long lc, int cell)
 {
     return ((unsigned long long)lc << 32) | (unsigned long long)(0xffffffffu - (unsigned)cell);
 }
 
-// Goal search, one warp per (listed node, group of kGoalGroup 32-cell chunks
-// of its window), each warp grabbing units on its own: a node's window is
-// spread over many warps, so a few nodes with busy windows do not hold a
-// launch back.  The warp first lists the group's cells that have a direct
-// goal connection (a few percent of a window) and hands those to its lanes,
-// in window order.  The last group of a node to finish keeps the node's
-// result when no group skipped a cell by the bound.  Masks are read through
-// L1.
+// Goal search (findBestGoalDirectConnection, graph_check_goal_reached.cu:
+// 17-70, plus checkGoalReached for the node, graph_best_node.cu:181-222),
+// one warp per (listed node, group of kGoalGroup 32-cell chunks of its
+// window), each warp grabbing units on its own: a node's window is spread
+// over many warps, so a few nodes with busy windows do not hold a launch
+// back.  The warp lists the group's cells that have a direct goal connection
+// (a few percent of a window) and evaluates the node's curve to each of them
+// in window order, sample-parallel (curve_warp).  The best connection keeps
+// the lowest fixed-point cost, ties to the later (higher) cell.  The last
+// group of a node to finish keeps the node's result when no group skipped a
+// cell by the bound.  Masks are read through L1.
 __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, State *states, Sched *sc)
 {
-    __shared__ int cell_list[8][kGoalGroup * 32];
     const int n = sc->n_slots;
     const int total = sc->goal_start[n];
     const int lane = threadIdx.x & 31;
-    const unsigned lower = (1u << lane) - 1u;
-    int *list = cell_list[threadIdx.x >> 5];
     while (true) {
         int g = 0;
         if (lane == 0)
@@ -1297,18 +1182,19 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
         if (wg == 0 && lane == 0)
             goal_check_node(I, S, pos);
         const Foot f = foot_of(I, I.blocked, I.clear);
-        GoalLane gl;
-        gl.I = &I;
-        gl.z = pos / I.W;
-        gl.x = pos - gl.z * I.W;
-        gl.heading = I.heading[pos];
-        gl.cost = I.cost[pos];
+        const int z = pos / I.W, x = pos - z * I.W;
+        const float heading = I.heading[pos];
+        const float cost = I.cost[pos];
         int zlo, xlo;
-        const int nz = window_count(gl.z, I.dist_tol, zlo);
-        const int nx = window_count(gl.x, I.dist_tol, xlo);
+        const int nz = window_count(z, I.dist_tol, zlo);
+        const int nx = window_count(x, I.dist_tol, xlo);
         const int wtotal = nx > 0 ? nz * nx : 0;
-        __syncwarp();  // the previous unit's lanes are done with the list
-        int cnt = 0;
+        const bool prune = I.intrinsic == nullptr;
+        const volatile long long *global_best = &S.best;
+        long long best = kBigCost;
+        int best_cell = -1;
+        bool pruned = false;
+        unsigned long long probes = 0;
         for (int q = 0; q < kGoalGroup; q++) {
             const int w = (wg * kGoalGroup + q) * 32 + lane;
             int cell = -1;
@@ -1320,36 +1206,45 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
                         cell = cc;
                 }
             }
-            const unsigned m = __ballot_sync(kFull, cell >= 0);
-            if (cell >= 0)
-                list[cnt + __popc(m & lower)] = cell;
-            cnt += __popc(m);
+            unsigned m = __ballot_sync(kFull, cell >= 0);
+            while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1;
+                const int cc = __shfl_sync(kFull, cell, k);
+                const float gdc = I.gd_cost[cc];
+                if (prune) {
+                    // the connection costs at least cost + 1 (the first sample)
+                    const float lb_total = (cost + 1.0f) + gdc;
+                    const long long lb = __float2ll_rd(100 * lb_total);
+                    // one read for the whole warp, so its lanes agree
+                    long long gb = 0;
+                    if (lane == 0)
+                        gb = *global_best;
+                    gb = __shfl_sync(kFull, gb, 0);
+                    if (lb > gb) {
+                        pruned = true;
+                        continue;
+                    }
+                }
+                const int zp = cc / I.W, xp = cc - zp * I.W;
+                const float seg = curve_warp(I, f, I.max_curvature, x, z, heading, xp, zp, I.gd_heading[cc],
+                                             1, cost, 0, lane, probes);
+                if (seg < 0)
+                    continue;
+                const float total_cost = seg + gdc;
+                const long long lc = __float2ll_rd(100 * total_cost);
+                if (lc <= best) {
+                    best = lc;
+                    best_cell = cc;
+                }
+            }
         }
-        __syncwarp();
-        gl.list = list;
-        gl.e = lane;
-        gl.cnt = cnt;
-        gl.in_task = false;
-        gl.best = kBigCost;
-        gl.best_cell = -1;
-        gl.global_best = &S.best;
-        gl.prune = I.intrinsic == nullptr;
-        gl.pruned = false;
-        unsigned long long probes = 0;
-        run_warp(gl, true, f, probes, [](const GoalLane &q) { return q.h.last_x; },
-                 [](const GoalLane &q) { return q.h.last_z; }, kStepSamples);
-        // warp minimum, ties to the highest cell index
-        unsigned long long k = gl.best < kBigCost ? connection_key(gl.best, gl.best_cell) : kNoConnection;
-        for (int o = 16; o; o >>= 1) {
-            const unsigned long long ok = __shfl_xor_sync(kFull, k, o);
-            k = ok < k ? ok : k;
-        }
-        const bool pruned = __any_sync(kFull, gl.pruned);
         probes = warp_sum64(probes);
         if (lane == 0) {
             if (probes)
                 atomicAdd(&S.probes_goal, probes);
-            if (k != kNoConnection) {
+            if (best < kBigCost) {
+                const unsigned long long k = connection_key(best, best_cell);
                 atomicMin(&I.node_key[idx], k);
                 atomicMin(&S.best, (long long)(k >> 32));
             }
@@ -1394,33 +1289,17 @@ __global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states
     }
 }
 
-struct SegLane {
-    HermTask h;
-    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
-    {
-        return h.advance(f, p, budget);
-    }
-    __device__ bool resolve(bool ok) { return h.resolve(ok); }
-    __device__ float probe_angle() const { return h.pend_heading; }
-};
-
 // The cost of the curve from node ppos to the goal-connected cell, as the goal
-// search computed it: the same task, on lane 0 of the calling warp, with the
-// warp's help for full footprint probes (graph_direct_goal_connection.cu:
-// 16-167 from the node).  Every lane of the warp calls it.
+// search computed it (graph_direct_goal_connection.cu:16-167 from the node),
+// by the calling warp.  Every lane of the warp calls it.
 __device__ float connection_segment_cost(const Inst &I, int ppos, int cell, int lane)
 {
     const Foot f = foot_of(I, I.blocked, I.clear);
     const int pz = ppos / I.W, px = ppos - pz * I.W;
     const int cz = cell / I.W, cx = cell - cz * I.W;
-    SegLane t;
-    if (lane == 0)
-        t.h.init(I, f, I.max_curvature, px, pz, I.heading[ppos], cx, cz, I.gd_heading[cell], 1,
-                 I.cost[ppos]);
     unsigned long long unused = 0;
-    run_warp(t, lane == 0, f, unused, [](const SegLane &q) { return q.h.last_x; },
-             [](const SegLane &q) { return q.h.last_z; });
-    return __shfl_sync(kFull, t.h.nodeCost, 0);
+    return curve_warp(I, f, I.max_curvature, px, pz, I.heading[ppos], cx, cz, I.gd_heading[cell], 1,
+                      I.cost[ppos], 0, lane, unused);
 }
 
 // the host-side tail of FastRRT::loop, one warp per slot (the warp helps
@@ -1803,17 +1682,8 @@ void launch_extract_paths(const Inst *d_inst, State *d_state, const int *d_slots
 }
 
 // optimizePathLoop (graph_optimization.cu:25-56, 92-195): every pair (i, j),
-// j >= i + 2, of path waypoints is tested with checkDirectConnectionToGoal
-struct PairLane {
-    HermTask h;
-    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
-    {
-        return h.advance(f, p, budget);
-    }
-    __device__ bool resolve(bool ok) { return h.resolve(ok); }
-    __device__ float probe_angle() const { return h.pend_heading; }
-};
-
+// j >= i + 2, of path waypoints is tested with checkDirectConnectionToGoal,
+// one pair per warp at a time (curve_warp)
 __global__ void k_opt_pairs(const Inst *insts, int slot, const float *path, const int *path_n,
                             float *newcost)
 {
@@ -1821,21 +1691,21 @@ __global__ void k_opt_pairs(const Inst *insts, int slot, const float *path, cons
     const int n = *path_n;
     const long pairs = (long)n * n;
     const Foot f = foot_of(I, I.blocked, I.clear);
+    const int lane = threadIdx.x & 31;
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
     unsigned long long probes = 0;
-    for (long base = (long)blockIdx.x * blockDim.x; base < pairs; base += (long)gridDim.x * blockDim.x) {
-        const long p = base + threadIdx.x;
-        const int i = (int)(p / (n > 0 ? n : 1)), j = (int)(p - (long)i * (n > 0 ? n : 1));
-        const bool has = p < pairs && j >= i + 2 && i < n - 2;
-        PairLane t;
-        if (has) {
+    for (long p = warp; p < pairs; p += warps) {
+        const int i = (int)(p / n), j = (int)(p - (long)i * n);
+        float r = -1.0f;
+        if (j >= i + 2 && i < n - 2) {
             const int x = (int)path[3 * i], z = (int)path[3 * i + 1];
-            t.h.init(I, f, I.max_curvature, x, z, path[3 * i + 2], (int)path[3 * j],
-                     (int)path[3 * j + 1], path[3 * j + 2], 1, I.cost[(long)z * I.W + x]);
+            r = curve_warp(I, f, I.max_curvature, x, z, path[3 * i + 2], (int)path[3 * j],
+                           (int)path[3 * j + 1], path[3 * j + 2], 1, I.cost[(long)z * I.W + x], 0, lane,
+                           probes);
         }
-        run_warp(t, has, f, probes, [](const PairLane &q) { return q.h.last_x; },
-                 [](const PairLane &q) { return q.h.last_z; });
-        if (p < pairs)
-            newcost[p] = has ? t.h.result() : -1.0f;
+        if (lane == 0)
+            newcost[p] = r;
     }
 }
 
@@ -1928,7 +1798,7 @@ void launch_optimize(const Inst *d_inst, int slot, int cells, float *d_path, int
                      float *d_newcost, int *d_changed, int cap, const Launch &L, cudaStream_t st)
 {
     const long pairs = (long)cap * cap;
-    int grid = (int)((pairs + 255) / 256);
+    int grid = (int)((pairs + 7) / 8);  // one pair per warp
     if (grid > L.sms * 8)
         grid = L.sms * 8;
     k_opt_pairs<<<grid, 256, 0, st>>>(d_inst, slot, d_path, d_path_n, d_newcost);
@@ -2247,6 +2117,8 @@ void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, c
                                           L.smem_words, bad_cell);
 }
 
+// One pose pair per warp at a time (curve_warp, samples across the lanes, no
+// coarse pass: the probe count is the reference's exact count).
 __global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, int n, const int32_t *x,
                                                  const int32_t *z, const float *lh, const int32_t *gx,
                                                  const int32_t *gz, const float *gh, float maxc,
@@ -2272,28 +2144,23 @@ __global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, in
         }
     }
     const Foot f = foot_of(I, blk, clr);
+    const int lane = threadIdx.x & 31;
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
     unsigned long long probes = 0;
-    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
-        const long i = base + threadIdx.x;
-        const bool has = i < n;
+    for (long i = warp; i < n; i += warps) {
         // a start cell outside the frame is not connected (its cost and
         // traversability are not read)
-        bool inside = false;
-        PairLane t;
-        if (has) {
-            const int cx = x[i], cz = z[i];
-            inside = cx >= 0 && cx < I.W && cz >= 0 && cz < I.H;
-            if (inside)
-                t.h.init(I, f, maxc, cx, cz, lh[i], gx[i], gz[i], gh[i], safe,
-                         I.cost[(long)cz * I.W + cx]);
-        }
-        run_warp(t, inside, f, probes, [](const PairLane &q) { return q.h.last_x; },
-                 [](const PairLane &q) { return q.h.last_z; });
-        if (has)
-            out[i] = inside ? t.h.result() : -1.0f;
+        const int cx = x[i], cz = z[i];
+        float r = -1.0f;
+        if (cx >= 0 && cx < I.W && cz >= 0 && cz < I.H)
+            r = curve_warp(I, f, maxc, cx, cz, lh[i], gx[i], gz[i], gh[i], safe, I.cost[(long)cz * I.W + cx],
+                           0, lane, probes);
+        if (lane == 0)
+            out[i] = r;
     }
     probes = warp_sum64(probes);
-    if ((threadIdx.x & 31) == 0 && probes && probes_out)
+    if (lane == 0 && probes && probes_out)
         atomicAdd(probes_out, probes);
 }
 
@@ -2304,9 +2171,10 @@ void launch_hermite_pairs(const Inst *d_inst, int slot, int n, const int32_t *x,
 {
     if (n <= 0)
         return;
-    int grid = (n + 255) / 256;
-    if (grid > L.work_blocks)
-        grid = L.work_blocks;
+    // one pair per warp: 8 per block
+    int grid = (n + 7) / 8;
+    if (grid > L.sms * 8)
+        grid = L.sms * 8;
     const size_t smem = (size_t)L.smem_words * 2 * 4;
     k_hermite<<<grid, 256, smem, st>>>(d_inst, slot, n, x, z, lh, gx, gz, gh, max_curvature, safe, out,
                                        probes, L.smem_words);

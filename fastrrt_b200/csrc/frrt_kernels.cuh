@@ -10,10 +10,16 @@ namespace frrt {
 constexpr int kSweepCells = 4096;   // cells per sweep chunk (256 threads x 16)
 constexpr int kCandChunk = 256;     // candidates per expansion chunk (one per thread)
 constexpr int kNodeChunk = 8;       // listed nodes per goal-search chunk (one per warp)
-// resident blocks per SM of the warp-grab kernels (register budgets: measured
-// best on B200, 2 for the cell evaluation, 3 for the goal search)
-constexpr int kEvalBlocks = 2;
-constexpr int kGoalBlocks = 3;   // 2 measured the same on served 256 x 256 planning
+// resident blocks per SM of the warp-grab kernels (their register budgets);
+// build-time knobs for measurement
+#ifndef FRRT_EVAL_BLOCKS
+#define FRRT_EVAL_BLOCKS 2
+#endif
+#ifndef FRRT_GOAL_BLOCKS
+#define FRRT_GOAL_BLOCKS 2
+#endif
+constexpr int kEvalBlocks = FRRT_EVAL_BLOCKS;
+constexpr int kGoalBlocks = FRRT_GOAL_BLOCKS;
 constexpr int32_t kClaimFree = 0x7F7F7F7F;
 
 // Scheduling tables shared by the iteration kernels (device memory).
