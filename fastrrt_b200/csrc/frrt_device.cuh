@@ -282,21 +282,9 @@ __device__ inline bool rows_clear_warp(const Foot &f, int x, int z, float c, flo
 }
 
 // ---------------------------------------------------------------------------
-// resumable per-lane tasks: advance() runs until a footprint needs a full
-// probe (returns kTaskProbe), the task ends (kTaskDone) or `budget` steps
-// have run (kTaskPaused); resolve() consumes the probe result.  run_warp()
-// drives 32 tasks and answers their probes with probe_warp, so lanes never
-// probe 943 cells serially.  A budget keeps the lanes of a warp in step: a
-// lane that needs a probe soon does not wait for a lane with a long clean
-// stretch, and the two resume together after the probe.
+// per-candidate checks, one candidate per warp
 // ---------------------------------------------------------------------------
 
-constexpr int kTaskDone = 0, kTaskProbe = 1, kTaskPaused = 2;
-constexpr int kNoBudget = 1 << 30;
-// curve samples / integration steps a lane runs per warp step in the
-// lane-refilling kernels (8 measured best of 8, 16 and unbounded on served
-// 256 x 256 planning)
-constexpr int kStepSamples = 8;
 // sample stride of the first pass of the direct goal connections (0: none);
 // a build-time knob for measurement
 #ifndef FRRT_COARSE_STRIDE
@@ -304,12 +292,11 @@ constexpr int kStepSamples = 8;
 #endif
 constexpr int kCoarseStride = FRRT_COARSE_STRIDE;
 
-// check_kinematic_new_path (kinematics.cu:123-231)
+// The start pose and constants of one check_kinematic_new_path candidate
+// (kinematics.cu:123-231); kin_warp integrates it.
 struct KinTask {
     float x, y, heading, beta, ds, hif, nodeCost, velocity;
-    float pend_cost;            // the last cell's intrinsic cost, not yet added
-    int maxSize, loop_max, loop_count, size, last_x, last_z, pend_x, pend_z, has_pend;
-    int ok;                     // 1 = feasible end cell, 0 = rejected
+    int maxSize, loop_max;
     float og_x, og_z;
     int W, H;
     const float *intrinsic;
@@ -338,90 +325,11 @@ struct KinTask {
         beta = atanf(steer / 2);
         hif = ds * cosf(beta) * steer / (2 * lr);
         maxSize = (int)(pathSize) + 1;
-        size = 0;
-        last_x = sx;
-        last_z = sz;
         heading = start_heading;
         nodeCost = start_cost;
-        has_pend = 0;
-        loop_count = 0;
         loop_max = (100 * maxSize) / dt;
-        ok = 0;
     }
 
-    __device__ int advance(const Foot &f, unsigned long long &probes, int budget = kNoBudget)
-    {
-        // the next step's cosine and sine are computed before this step's
-        // cell tests (they depend only on the heading), so they overlap
-        float nc = cosf(heading + beta), ns = sinf(heading + beta);
-        while (size < maxSize) {
-            if (budget-- <= 0)
-                return kTaskPaused;
-            if (loop_count++ > loop_max)
-                break;
-            x += ds * nc;
-            y += ds * ns;
-            heading += hif;
-            nc = cosf(heading + beta);
-            ns = sinf(heading + beta);
-            // convert_map_pose_to_waypoint (kinematics.cu:25-46)
-            const double2 coord = {x, y};
-            const int lpx = (int)(og_x + coord.y);
-            const int lpz = (int)(og_z - coord.x);
-            if (lpx == last_x && lpz == last_z)
-                continue;
-            if (lpx < 0 || lpx >= W)
-                break;
-            if (lpz < 0 || lpz >= H)
-                break;
-            size += 1;
-            // a cell's cost is added when the next cell is reached (or at the
-            // end), in the same order, so its load overlaps the steps between
-            settle();
-            pend_cost = intrinsic ? intrinsic[(long)lpz * W + lpx] : 0.0f;
-            has_pend = 1;
-            if (quick_feasible(f, lpx, lpz, probes)) {
-                last_x = lpx;
-                last_z = lpz;
-                continue;
-            }
-            if (f.sat) {
-                float sn, cs;
-                sincosf(heading, &sn, &cs);
-                if (box_feasible(f, lpx, lpz, fabsf(cs), fabsf(sn), probes)) {
-                    last_x = lpx;
-                    last_z = lpz;
-                    continue;
-                }
-            }
-            pend_x = lpx;
-            pend_z = lpz;
-            return kTaskProbe;
-        }
-        settle();
-        ok = size >= 1;
-        return kTaskDone;
-    }
-    __device__ __forceinline__ void settle()
-    {
-        if (has_pend) {
-            nodeCost += pend_cost + 1;
-            has_pend = 0;
-        }
-    }
-    // returns false when the task ended (infeasible footprint)
-    __device__ bool resolve(bool feasible)
-    {
-        if (!feasible) {
-            settle();
-            ok = 0;
-            return false;
-        }
-        last_x = pend_x;
-        last_z = pend_z;
-        return true;
-    }
-    __device__ float probe_angle() const { return heading; }
 };
 
 // The constants of one checkDirectConnectionToGoal curve
@@ -546,6 +454,164 @@ __device__ inline bool footprint_warp(const Foot &f, int x, int z, float angle, 
     return probe_warp(f, x, z, angle, lane, cnt);
 }
 
+// Result of one kinematic candidate (check_kinematic_new_path).
+struct KinResult {
+    int ok;            // 1: a feasible end cell
+    int last_x, last_z;
+    float cost, heading;
+};
+
+// check_kinematic_new_path (kinematics.cu:123-231) of one candidate,
+// evaluated by the whole warp: lane k takes integration step base + k.
+//
+// The pose chains are the reference's, in its order and roundings: the
+// heading before step s is the start heading plus s serial float adds of the
+// increment, and x, y advance by one fused multiply-add per step (the
+// contraction the compiler applies to the reference's `x += ds * cosf(..)`).
+// Those adds run as one serial chain per warp (32 steps, a shuffle each);
+// the cosines and sines, the cell of each step and its tests run across the
+// lanes.  Every step either stays in the last cell, leaves the frame (the
+// loop ends after the step) or enters a new cell, so the last cell before
+// step s is the cell of step s - 1.  The loop also ends before the step that
+// would exceed its iteration bound or follow the maxSize-th new cell.  New
+// cells before the first stop are checked (clear bit, summed-area box, then
+// the warp's probe loop in step order); the first infeasible one rejects the
+// candidate.  The cost adds (intrinsic + 1) of each new cell in step order.
+// `probes` gets the reference's exact probe count.  Every argument is the
+// same in all lanes, and so is the result.
+__device__ inline KinResult kin_warp(const Inst &I, const Foot &f, int sx, int sz, float steer, float len,
+                                     float velocity, float start_heading, float start_cost, int lane,
+                                     unsigned long long &probes)
+{
+    KinTask k;
+    k.init(I, sx, sz, steer, len, velocity, start_heading, start_cost);
+    const unsigned lower = (1u << lane) - 1u;
+    float x = k.x, y = k.y, hd = k.heading, cost = k.nodeCost;
+    int last_x = sx, last_z = sz, size = 0;
+    KinResult r;
+    for (int base = 0;; base += 32) {
+        // headings before (hb) and after (ha) this lane's step
+        float hb = hd, ha = hd;
+        {
+            float h = hd;
+#pragma unroll
+            for (int q = 0; q < 32; q++) {
+                if (q == lane)
+                    hb = h;
+                h = h + k.hif;
+                if (q == lane)
+                    ha = h;
+            }
+        }
+        const float c = cosf(hb + k.beta), s = sinf(hb + k.beta);
+        float px = x, py = y;  // pose after this lane's step
+        {
+            float xa = x, ya = y;
+#pragma unroll
+            for (int q = 0; q < 32; q++) {
+                xa = __fmaf_rn(k.ds, __shfl_sync(kFull, c, q), xa);
+                ya = __fmaf_rn(k.ds, __shfl_sync(kFull, s, q), ya);
+                if (q == lane) {
+                    px = xa;
+                    py = ya;
+                }
+            }
+        }
+        // convert_map_pose_to_waypoint (kinematics.cu:25-46)
+        const double2 coord = {px, py};
+        const int lpx = (int)(k.og_x + coord.y);
+        const int lpz = (int)(k.og_z - coord.x);
+        const int ux = __shfl_up_sync(kFull, lpx, 1), uz = __shfl_up_sync(kFull, lpz, 1);
+        const int prev_x = lane ? ux : last_x, prev_z = lane ? uz : last_z;
+        const bool moved = !(lpx == prev_x && lpz == prev_z);
+        const bool oob = moved && (lpx < 0 || lpx >= k.W || lpz < 0 || lpz >= k.H);
+        const bool fresh = moved && !oob;
+        const unsigned nm = __ballot_sync(kFull, fresh);
+        // the first step that does not run, and the first that leaves the frame
+        const int step = base + lane;
+        const unsigned over_m = __ballot_sync(kFull, step > k.loop_max || size + __popc(nm & lower) >= k.maxSize);
+        const int e_stop = over_m ? __ffs(over_m) - 1 : 32;
+        const unsigned oob_m = __ballot_sync(kFull, oob) & (e_stop < 32 ? ((1u << e_stop) - 1u) : kFull);
+        const int end = oob_m ? __ffs(oob_m) : e_stop;  // steps of this chunk that run
+        // the loop ends in this chunk (a step that leaves the frame may be the
+        // chunk's last, with all 32 steps run)
+        const bool stopped = oob_m != 0 || e_stop < 32;
+        const unsigned run_m = end >= 32 ? kFull : ((1u << end) - 1u);
+        const bool check = fresh && ((run_m >> lane) & 1u);
+        // footprint of each new cell: shortcuts per lane, then the warp's
+        // probe loop for the rest in step order up to the first failure
+        unsigned long long pl = 0;
+        float v = 0.0f;
+        bool hard = false;
+        if (check) {
+            v = (k.intrinsic ? k.intrinsic[(long)lpz * k.W + lpx] : 0.0f) + 1;
+            if (!quick_feasible(f, lpx, lpz, pl)) {
+                bool box = false;
+                if (f.sat) {
+                    float sn, cs;
+                    sincosf(ha, &sn, &cs);
+                    box = box_feasible(f, lpx, lpz, fabsf(cs), fabsf(sn), pl);
+                }
+                hard = !box;
+            }
+        }
+        unsigned hm = __ballot_sync(kFull, hard);
+        int ff = 32;
+        unsigned fcnt = 0;
+        while (hm) {
+            const int leader = __ffs(hm) - 1;
+            hm &= hm - 1;
+            unsigned cnt = 0;
+            const bool ok = footprint_warp(f, __shfl_sync(kFull, lpx, leader), __shfl_sync(kFull, lpz, leader),
+                                           __shfl_sync(kFull, ha, leader), lane, cnt);
+            if (!ok) {
+                ff = leader;
+                fcnt = cnt;
+                break;
+            }
+            if (lane == leader)
+                pl += cnt;
+        }
+        if (lane < ff)
+            probes += pl;
+        if (ff < 32 && lane == 0)
+            probes += fcnt;
+        // costs in step order, up to and including a failing cell
+        unsigned cm = __ballot_sync(kFull, check) & (ff < 32 ? ((2u << ff) - 1u) : kFull);
+        while (cm) {
+            const int q = __ffs(cm) - 1;
+            cm &= cm - 1;
+            cost += __shfl_sync(kFull, v, q);
+        }
+        if (ff < 32) {
+            r.ok = 0;
+            r.last_x = last_x;
+            r.last_z = last_z;
+            r.cost = cost;
+            r.heading = __shfl_sync(kFull, ha, ff);
+            return r;
+        }
+        const unsigned done_m = nm & run_m;
+        size += __popc(done_m);
+        if (done_m) {
+            const int q = 31 - __clz(done_m);
+            last_x = __shfl_sync(kFull, lpx, q);
+            last_z = __shfl_sync(kFull, lpz, q);
+        }
+        if (stopped) {
+            r.ok = size >= 1;
+            r.last_x = last_x;
+            r.last_z = last_z;
+            r.cost = cost;
+            r.heading = end > 0 ? __shfl_sync(kFull, ha, end - 1) : hd;
+            return r;
+        }
+        hd = __shfl_sync(kFull, ha, 31);
+        x = __shfl_sync(kFull, px, 31);
+        y = __shfl_sync(kFull, py, 31);
+    }
+}
+
 // checkDirectConnectionToGoal (graph_direct_goal_connection.cu:16-167) of
 // one curve, evaluated by the whole warp: lane k takes sample base + k, with
 // the same arithmetic as HermTask.
@@ -556,11 +622,13 @@ __device__ inline bool footprint_warp(const Foot &f, int x, int z, float angle, 
 // tested cell before sample i is the cell of the nearest earlier sample in
 // the frame: a ballot and a shuffle, with the last chunk's cell carried over.
 // A tested sample fails on curvature, else on its footprint; the reference's
-// answer is "no connection" at the first failure.  Lanes that need the full
-// probe loop are probed by the whole warp one after another in sample order,
-// up to the chunk's first curvature failure, so the first footprint failure
-// found is the reference's and `probes` gets the reference's exact count for
-// the walk.  The connection cost is the start cost plus (intrinsic + 1) of
+// answer is "no connection" at the first failure, so any failure decides it.
+// A chunk with a curvature failure ends the walk before its footprints are
+// tested.  Otherwise lanes that need the full probe loop are probed by the
+// whole warp one after another in sample order, so the first footprint
+// failure found is the reference's; `probes` gets the reference's count for
+// the chunks walked up to that failure (at most the reference's count for
+// the curve, equal to it for a connected curve).  The connection cost is the start cost plus (intrinsic + 1) of
 // every tested sample, added in sample order (one lane's term after
 // another), so the float sum rounds as the reference's.
 //
@@ -669,9 +737,12 @@ __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv,
             h.ref_deriv(t, ddx, ddz, dd2x, dd2z);
             over = max_curv > 0 && h.ref_over(ddx, ddz, dd2x, dd2z, h.kap_hi2, h.kap_lo2);
         }
-        const unsigned om = __ballot_sync(kFull, over);
-        const int fc = om ? __ffs(om) - 1 : 32;  // first curvature failure
-        if (tested && lane < fc && !skip_foot && !quick_feasible(f, cx, cz, pl)) {
+        // a curvature failure anywhere in the chunk decides the answer (no
+        // connection) whatever the footprints before it give; the chunk's
+        // feasible footprints are then left uncounted
+        if (__any_sync(kFull, over))
+            return -1.0f;
+        if (tested && !skip_foot && !quick_feasible(f, cx, cz, pl)) {
             const double s2 = ddx * ddx + ddz * ddz;
             bool box = false;
             if (f.sat && s2 > 0.0) {
@@ -700,11 +771,10 @@ __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv,
             if (lane == leader)
                 pl += cnt;
         }
-        const int fail = min(fc, ff);
-        if (lane < fail)
+        if (lane < ff)
             probes += pl;
-        if (fail < 32) {
-            if (ff < fc && lane == 0)
+        if (ff < 32) {
+            if (lane == 0)
                 probes += fcnt;
             return -1.0f;
         }
@@ -723,49 +793,6 @@ __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv,
     if (np <= 0 || (last_x != gx && last_z != gz))
         return -1.0f;
     return cost;
-}
-
-// Drives one task per lane.  `has` says whether the lane holds a task.
-// Probes needing a full footprint scan are answered cooperatively.
-template <class Task, class PX, class PZ>
-__device__ void run_warp(Task &t, bool has, const Foot &f, unsigned long long &probes, PX px, PZ pz,
-                         int budget = kNoBudget)
-{
-    const int lane = threadIdx.x & 31;
-    bool active = has;
-    while (__any_sync(kFull, active)) {
-        bool need = false;
-        if (active) {
-            const int r = t.advance(f, probes, budget);
-            if (r == kTaskProbe)
-                need = true;
-            else if (r == kTaskDone)
-                active = false;
-        }
-        unsigned m = __ballot_sync(kFull, need);
-        bool mine = true;
-        while (m) {
-            const int leader = __ffs(m) - 1;
-            m &= m - 1;
-            const int bx = __shfl_sync(kFull, px(t), leader);
-            const int bz = __shfl_sync(kFull, pz(t), leader);
-            const float ba = __shfl_sync(kFull, t.probe_angle(), leader);
-            unsigned cnt = 0;
-            bool ok;
-            if (rows_clear_warp(f, bx, bz, cosf(ba), sinf(ba), lane)) {
-                ok = true;  // feasible: the reference runs all its probes
-                cnt = full_probes(f);
-            } else {
-                ok = probe_warp(f, bx, bz, ba, lane, cnt);
-            }
-            if (lane == leader) {
-                mine = ok;
-                probes += cnt;
-            }
-        }
-        if (need && !t.resolve(mine))
-            active = false;
-    }
 }
 
 // computeHeading (graph.cu:219-234)

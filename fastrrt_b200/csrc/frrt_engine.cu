@@ -224,7 +224,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaMemsetAsync(d_state_, 0, sizeof(State) * n_slots, stream_), "state init") &&
               check(cudaMallocHost(&h_state_, sizeof(State) * n_slots), "pinned state") &&
               check(cudaMalloc(&d_sched_, sizeof(Sched)), "sched") &&
-              check(cudaMalloc(&d_sched_arrays_, sizeof(int) * 5 * (n_slots + 1)), "sched arrays") &&
+              check(cudaMalloc(&d_sched_arrays_, sizeof(int) * 6 * (n_slots + 1)), "sched arrays") &&
               check(cudaMalloc(&d_grab_, sizeof(unsigned) * 4), "grab counters") &&
               check(cudaMalloc(&d_slots_, sizeof(int) * n_slots), "slot list") &&
               check(cudaMalloc(&d_class_costs_, sizeof(float) * kMaxClasses * n_slots), "class costs") &&
@@ -235,7 +235,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
               check(cudaEventCreateWithFlags(&stage_ev_, cudaEventDisableTiming), "staging event") &&
               check(cudaMalloc(&d_newcost_, sizeof(float) * kOptCap * kOptCap), "optimize scratch") &&
               check(cudaMalloc(&d_changed_, sizeof(int)), "optimize flag") &&
-              check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 5 * (n_slots + 1), stream_), "sched init") &&
+              check(cudaMemsetAsync(d_sched_arrays_, 0, sizeof(int) * 6 * (n_slots + 1), stream_), "sched init") &&
               check(cudaMemsetAsync(d_grab_, 0, sizeof(unsigned) * 4, stream_), "grab init") &&
               check(cudaMemsetAsync(d_class_costs_, 0, sizeof(float) * kMaxClasses * n_slots, stream_), "costs init");
     if (!ok)
@@ -443,6 +443,7 @@ bool Engine::commit()
     h_sched_.node_start = d_sched_arrays_ + 2 * (n_slots_ + 1);
     h_sched_.gd_start = d_sched_arrays_ + 3 * (n_slots_ + 1);
     h_sched_.goal_start = d_sched_arrays_ + 4 * (n_slots_ + 1);
+    h_sched_.cand_exact = d_sched_arrays_ + 5 * (n_slots_ + 1);
     h_sched_.grab = d_grab_;
     const int sweep_blocks = std::max(1, std::min(L_.sms * sweep_per_sm_, run));
     if (sweep_blocks != L_.sweep_blocks) {

@@ -54,6 +54,16 @@ __device__ __forceinline__ int find_slot(const int *prefix, int n, int chunk)
 
 __device__ __forceinline__ bool live(const State &S) { return S.active && !S.done; }
 
+// Items a warp of the warp-per-item kernels takes from its work counter at
+// once: one while the items are few next to the grid's warps (every item on
+// a warp of its own, the shortest launch), more when there are many (fewer
+// atomics on the one counter).
+__device__ __forceinline__ int grab_batch(int total)
+{
+    const int warps = (int)(gridDim.x * (blockDim.x >> 5));
+    return total >= 16 * warps ? 4 : total >= 4 * warps ? 2 : 1;
+}
+
 // warp-aggregated append: returns this lane's first output index
 __device__ __forceinline__ int warp_append(int *counter, int n)
 {
@@ -532,28 +542,24 @@ __device__ __forceinline__ int goal_groups(const Inst &I)
     return (I.win_chunks + kGoalGroup - 1) / kGoalGroup;
 }
 
-// prefix of per-slot work chunks (one block); which = 0: candidates, 1: nodes
 // work units of one slot: 0 candidate chunks, 1 listed-node chunks (both
-// ends of the list), 2 listed cells, 3 (node to search, window chunk group)
+// ends of the list), 2 listed cells, 3 (node to search, window chunk group),
+// 4 candidates
 __device__ __forceinline__ long long chunks_of(const Inst &I, const State &S, int which)
 {
     switch (which) {
     case 0: return (S.n_cand + kCandChunk - 1) / kCandChunk;
     case 1: return (S.n_nodes + S.n_memo + kNodeChunk - 1) / kNodeChunk;
     case 2: return S.n_gd;
-    default: return (long long)S.n_nodes * goal_groups(I);
+    case 3: return (long long)S.n_nodes * goal_groups(I);
+    default: return S.n_cand;
     }
 }
 
-__global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states, Sched *sc,
-                                              int which)
+// exclusive prefix over the slots of their work units (one block)
+__device__ void plan_prefix(const Inst *insts, State *states, int n, int which, int *out)
 {
     __shared__ long long warp_tot[32];
-    const int n = sc->n_slots;
-    int *out = which == 0   ? sc->cand_start
-               : which == 1 ? sc->node_start
-               : which == 2 ? sc->gd_start
-                            : sc->goal_start;
     const int per = (n + blockDim.x - 1) / blockDim.x;
     const int s0 = threadIdx.x * per;
     long long local = 0;
@@ -571,6 +577,7 @@ __global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states,
         if (lane >= o)
             incl += v;
     }
+    __syncthreads();  // warp_tot is free (an earlier call is done with it)
     if (lane == 31)
         warp_tot[wid] = incl;
     __syncthreads();
@@ -599,19 +606,26 @@ __global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states,
     }
     if (threadIdx.x == blockDim.x - 1)
         out[n] = fits ? (int)run : 0;
+}
+
+// prefix of per-slot work (one block) for one kernel of the iteration, and
+// the reset of that kernel's work counter; which = 0 (candidates) writes the
+// chunk prefix and the exact candidate prefix
+__global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states, Sched *sc,
+                                              int which)
+{
+    const int n = sc->n_slots;
+    int *out = which == 0   ? sc->cand_start
+               : which == 1 ? sc->node_start
+               : which == 2 ? sc->gd_start
+                            : sc->goal_start;
+    plan_prefix(insts, states, n, which, out);
+    if (which == 0)
+        plan_prefix(insts, states, n, 4, sc->cand_exact);
     if (threadIdx.x == 0)
         sc->grab[which] = 0;
 }
 
-struct KinLane {
-    KinTask k;
-    __device__ int advance(const Foot &f, unsigned long long &p, int budget)
-    {
-        return k.advance(f, p, budget);
-    }
-    __device__ bool resolve(bool ok) { return k.resolve(ok); }
-    __device__ float probe_angle() const { return k.heading; }
-};
 
 // the winner of each claimed cell applies expand_node's transitions
 __global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states, const Sched *sc)
@@ -953,16 +967,6 @@ __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *sta
     }
 }
 
-// Lanes of a warp that take tasks: all 32 when there is work for every lane
-// of the grid, fewer when there is little (a warp answers its lanes' full
-// probes one after another, so a lightly loaded launch finishes sooner with
-// tasks spread over more warps); the other lanes only help with probes.
-__device__ __forceinline__ unsigned lanes_in_use(int total, int warps)
-{
-    const int per = min(32, max(1, (total + warps - 1) / max(warps, 1)));
-    return per >= 32 ? kFull : ((1u << per) - 1u);
-}
-
 // A full footprint probe for lane `leader`, answered by the whole warp; the
 // leader's footprint may belong to another slot than the other lanes' tasks.
 __device__ inline bool coop_probe(const Foot &mine, int leader, int lane, int x, int z, float angle,
@@ -1003,14 +1007,20 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
     const int n = sc->n_slots;
     const int total = sc->gd_start[n];
     const int lane = threadIdx.x & 31;
-    while (true) {
-        int e = 0;
-        if (lane == 0)
-            e = (int)atomicAdd(&sc->grab[2], 1u);
-        e = __shfl_sync(kFull, e, 0);
-        if (e >= total)
-            break;
-        const int slot = find_slot(sc->gd_start, n, e);
+    const int batch = grab_batch(total);
+    for (int e0 = 0, e1 = 0, e = 0, slot = 0;; e++) {
+        if (e >= e1) {
+            if (lane == 0)
+                e0 = (int)atomicAdd(&sc->grab[2], (unsigned)batch);
+            e0 = __shfl_sync(kFull, e0, 0);
+            if (e0 >= total)
+                break;
+            e = e0;
+            e1 = min(e0 + batch, total);
+            slot = find_slot(sc->gd_start, n, e);
+        }
+        while (e >= sc->gd_start[slot + 1])
+            slot++;
         const Inst &I = insts[slot];
         const int pos = I.gd_list[e - sc->gd_start[slot]];
         const Foot f = foot_of(I, I.blocked, I.clear);
@@ -1034,109 +1044,65 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
     }
 }
 
-// Expansion: candidates are handed to lanes one by one over all slots (the
-// padded space of 256-candidate chunks): a lane whose integration ended takes
-// the next candidate at the start of the warp's next step, so lanes stay busy
-// although path lengths differ.  Full footprint probes are answered by the
-// whole warp; masks are read through L1.
+// Expansion: one candidate per warp at a time, grabbed over all slots: the
+// warp integrates the candidate
+// step-parallel (kin_warp), so a launch with few candidates still spreads
+// each over 32 lanes.  Masks are read through L1.
 __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states, Sched *sc)
 {
     const int n = sc->n_slots;
-    const int total = sc->cand_start[n] * kCandChunk;
+    const int total = sc->cand_exact[n];
     const int lane = threadIdx.x & 31;
-    const unsigned lower = (1u << lane) - 1u;
-    const unsigned lanes = lanes_in_use(total, gridDim.x * (blockDim.x >> 5));
-    KinLane t;
-    Foot f{};
-    const Inst *I = nullptr;
-    int slot = 0, idx = 0, pos = 0;
-    bool active = false, exhausted = false;
-    unsigned long long probes = 0;
-    auto finish = [&]() {
-        int end = -1;
-        if (t.k.ok) {
-            const int ex = t.k.last_x, ez = t.k.last_z;
-            if (!(ex == I->og_x && ez == I->og_z)) {
-                const int ep = ez * I->W + ex;
+    const int batch = grab_batch(total);
+    for (int e0 = 0, e1 = 0, e = 0, slot = 0;; e++) {
+        if (e >= e1) {
+            if (lane == 0)
+                e0 = (int)atomicAdd(&sc->grab[0], (unsigned)batch);
+            e0 = __shfl_sync(kFull, e0, 0);
+            if (e0 >= total)
+                break;
+            e = e0;
+            e1 = min(e0 + batch, total);
+            slot = find_slot(sc->cand_exact, n, e);
+        }
+        while (e >= sc->cand_exact[slot + 1])
+            slot++;
+        const int idx = e - sc->cand_exact[slot];
+        const Inst &I = insts[slot];
+        const Foot f = foot_of(I, I.blocked, I.clear);
+        const int pos = I.cand[idx];
+        const int z = pos / I.W, x = pos - z * I.W;
+        float steer, len;
+        if (I.proposal && I.prop_row[idx] >= 0 && I.prop_len[idx] >= 0.0f) {
+            steer = I.prop_steer[idx];
+            len = I.prop_len[idx];
+        } else {
+            draw_expansion(I.seed, (uint32_t)pos, states[slot].iter, (float)I.max_steer, I.max_path, steer,
+                           len);
+        }
+        unsigned long long probes = 0;
+        const KinResult r = kin_warp(I, f, x, z, steer, len, I.velocity, I.heading[pos], I.cost[pos], lane,
+                                     probes);
+        probes = warp_sum64(probes);
+        if (lane == 0) {
+            // expand_node (graph_expansion.cu:103-145): no end cell at the
+            // coordinate origin or on the expanding cell itself
+            int end = -1;
+            if (r.ok && !(r.last_x == I.og_x && r.last_z == I.og_z)) {
+                const int ep = r.last_z * I.W + r.last_x;
                 if (ep != pos)
                     end = ep;
             }
+            I.cand_steer[idx] = steer;
+            I.cand_len[idx] = len;
+            I.cand_end[idx] = end;
+            I.cand_heading[idx] = r.heading;
+            I.cand_cost[idx] = r.cost;
+            if (end >= 0)
+                atomicMin(&I.claim[end], pos);
+            if (probes)
+                atomicAdd(&states[slot].probes, probes);
         }
-        I->cand_end[idx] = end;
-        I->cand_heading[idx] = t.k.heading;
-        I->cand_cost[idx] = t.k.nodeCost;
-        if (end >= 0)
-            atomicMin(&I->claim[end], pos);
-        if (probes)
-            atomicAdd(&states[slot].probes, probes);
-        probes = 0;
-        active = false;
-    };
-    while (true) {
-        if (!exhausted) {
-            const unsigned idle = __ballot_sync(kFull, !active) & lanes;
-            if (idle) {
-                int base = 0;
-                if (lane == 0)
-                    base = (int)atomicAdd(&sc->grab[0], (unsigned)__popc(idle));
-                base = __shfl_sync(kFull, base, 0);
-                if (base + __popc(idle) >= total)
-                    exhausted = true;
-                const int e = base + __popc(idle & lower);
-                if (((idle >> lane) & 1u) && e < total) {
-                    const int c = e / kCandChunk;
-                    const int s = find_slot(sc->cand_start, n, c);
-                    const int k = (c - sc->cand_start[s]) * kCandChunk + (e - c * kCandChunk);
-                    if (k < states[s].n_cand) {
-                        slot = s;
-                        idx = k;
-                        I = &insts[s];
-                        f = foot_of(*I, I->blocked, I->clear);
-                        pos = I->cand[idx];
-                        const int z = pos / I->W, x = pos - z * I->W;
-                        float steer, len;
-                        if (I->proposal && I->prop_row[idx] >= 0 && I->prop_len[idx] >= 0.0f) {
-                            steer = I->prop_steer[idx];
-                            len = I->prop_len[idx];
-                        } else {
-                            draw_expansion(I->seed, (uint32_t)pos, states[s].iter, (float)I->max_steer,
-                                           I->max_path, steer, len);
-                        }
-                        I->cand_steer[idx] = steer;
-                        I->cand_len[idx] = len;
-                        t.k.init(*I, x, z, steer, len, I->velocity, I->heading[pos], I->cost[pos]);
-                        active = true;
-                    }
-                }
-            }
-        }
-        if (!__any_sync(kFull, active)) {
-            if (exhausted)
-                break;
-            continue;
-        }
-        bool need = false;
-        if (active) {
-            const int r = t.advance(f, probes, kStepSamples);
-            if (r == kTaskProbe)
-                need = true;
-            else if (r == kTaskDone)
-                finish();
-        }
-        unsigned m = __ballot_sync(kFull, need);
-        bool ok_mine = true;
-        while (m) {
-            const int leader = __ffs(m) - 1;
-            m &= m - 1;
-            unsigned cnt = 0;
-            const bool ok = coop_probe(f, leader, lane, t.k.pend_x, t.k.pend_z, t.probe_angle(), cnt);
-            if (lane == leader) {
-                ok_mine = ok;
-                probes += cnt;
-            }
-        }
-        if (need && !t.resolve(ok_mine))
-            finish();
     }
 }
 
@@ -1148,37 +1114,92 @@ __device__ __forceinline__ unsigned long long connection_key(long long lc, int c
 // Goal search (findBestGoalDirectConnection, graph_check_goal_reached.cu:
 // 17-70, plus checkGoalReached for the node, graph_best_node.cu:181-222),
 // one warp per (listed node, group of kGoalGroup 32-cell chunks of its
-// window), each warp grabbing units on its own: a node's window is spread
-// over many warps, so a few nodes with busy windows do not hold a launch
-// back.  The warp lists the group's cells that have a direct goal connection
-// (a few percent of a window) and evaluates the node's curve to each of them
-// in window order, sample-parallel (curve_warp).  The best connection keeps
-// the lowest fixed-point cost, ties to the later (higher) cell.  The last
-// group of a node to finish keeps the node's result when no group skipped a
-// cell by the bound.  Masks are read through L1.
+// window) unit, each warp grabbing units on its own: a node's window is
+// spread over many warps, so a few nodes with busy windows do not hold a
+// launch back.  The warp lists the unit's cells that have a direct goal
+// connection (a few percent of a window) and evaluates the node's curve to
+// each of them in window order, sample-parallel (curve_warp).  The best
+// connection keeps the lowest fixed-point cost, ties to the later (higher)
+// cell.  Consecutive units a warp takes of one node are merged before they
+// are published; the node's last unit to finish keeps the node's result when
+// no unit skipped a cell by the bound.  Masks are read through L1.
 __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, State *states, Sched *sc)
 {
     const int n = sc->n_slots;
     const int total = sc->goal_start[n];
     const int lane = threadIdx.x & 31;
-    while (true) {
-        int g = 0;
-        if (lane == 0)
-            g = (int)atomicAdd(&sc->grab[3], 1u);
-        g = __shfl_sync(kFull, g, 0);
-        if (g >= total)
-            break;
-        const int slot = find_slot(sc->goal_start, n, g);
+    const int batch = grab_batch(total);
+    // the node whose units this warp is merging
+    int cur_slot = -1, cur_idx = -1, cur_units = 0;
+    long long best = kBigCost;
+    int best_cell = -1;
+    bool pruned = false;
+    unsigned long long probes = 0, key = 0;
+    int cur_pos = 0;
+    auto publish = [&]() {
+        if (cur_idx < 0)
+            return;
+        const Inst &I = insts[cur_slot];
+        State &S = states[cur_slot];
+        probes = warp_sum64(probes);
+        if (lane == 0) {
+            if (probes)
+                atomicAdd(&S.probes_goal, probes);
+            if (best < kBigCost) {
+                const unsigned long long k = connection_key(best, best_cell);
+                atomicMin(&I.node_key[cur_idx], k);
+                atomicMin(&S.best, (long long)(k >> 32));
+            }
+            if (pruned)
+                atomicOr(&I.node_pruned[cur_idx], 1);
+            __threadfence();
+            if (atomicSub(&I.node_pending[cur_idx], cur_units) == cur_units) {
+                // every unit of the node is done
+                __threadfence();
+                const unsigned long long r = atomicAdd(&I.node_key[cur_idx], 0ull);
+                if (!atomicAdd(&I.node_pruned[cur_idx], 0)) {
+                    I.memo_result[cur_pos] = r;
+                    I.memo_key[cur_pos] = key;
+                }
+            }
+        }
+        probes = 0;
+        best = kBigCost;
+        best_cell = -1;
+        pruned = false;
+        cur_idx = -1;
+        cur_units = 0;
+    };
+    for (int e0 = 0, e1 = 0, e = 0, slot = 0;; e++) {
+        if (e >= e1) {
+            if (lane == 0)
+                e0 = (int)atomicAdd(&sc->grab[3], (unsigned)batch);
+            e0 = __shfl_sync(kFull, e0, 0);
+            if (e0 >= total)
+                break;
+            e = e0;
+            e1 = min(e0 + batch, total);
+            slot = find_slot(sc->goal_start, n, e);
+        }
+        while (e >= sc->goal_start[slot + 1])
+            slot++;
         const Inst &I = insts[slot];
         State &S = states[slot];
-        const int local = g - sc->goal_start[slot];
+        const int local = e - sc->goal_start[slot];
         const int groups = goal_groups(I);
         const int idx = local / groups;
         const int wg = local - idx * groups;
         // a node to search (nodes with a kept result were resolved when
         // listed); the key of this heading and cost marks a complete result
         const int pos = I.nodes[idx];
-        const unsigned long long key = memo_key_of(I, pos);
+        if (slot != cur_slot || idx != cur_idx) {
+            publish();
+            cur_slot = slot;
+            cur_idx = idx;
+            cur_pos = pos;
+            key = memo_key_of(I, pos);
+        }
+        cur_units++;
         if (wg == 0 && lane == 0)
             goal_check_node(I, S, pos);
         const Foot f = foot_of(I, I.blocked, I.clear);
@@ -1191,10 +1212,6 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
         const int wtotal = nx > 0 ? nz * nx : 0;
         const bool prune = I.intrinsic == nullptr;
         const volatile long long *global_best = &S.best;
-        long long best = kBigCost;
-        int best_cell = -1;
-        bool pruned = false;
-        unsigned long long probes = 0;
         for (int q = 0; q < kGoalGroup; q++) {
             const int w = (wg * kGoalGroup + q) * 32 + lane;
             int cell = -1;
@@ -1239,29 +1256,8 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
                 }
             }
         }
-        probes = warp_sum64(probes);
-        if (lane == 0) {
-            if (probes)
-                atomicAdd(&S.probes_goal, probes);
-            if (best < kBigCost) {
-                const unsigned long long k = connection_key(best, best_cell);
-                atomicMin(&I.node_key[idx], k);
-                atomicMin(&S.best, (long long)(k >> 32));
-            }
-            if (pruned)
-                atomicOr(&I.node_pruned[idx], 1);
-            __threadfence();
-            if (atomicSub(&I.node_pending[idx], 1) == 1) {
-                // every chunk of the node is done
-                __threadfence();
-                const unsigned long long r = atomicAdd(&I.node_key[idx], 0ull);
-                if (!atomicAdd(&I.node_pruned[idx], 0)) {
-                    I.memo_result[pos] = r;
-                    I.memo_key[pos] = key;
-                }
-            }
-        }
     }
+    publish();
 }
 
 // among listed nodes with the minimum, the highest node cell index wins
@@ -2073,33 +2069,32 @@ __global__ void __launch_bounds__(256) k_candidates(const Inst *insts, int slot,
         }
     }
     const Foot f = foot_of(I, blk, clr);
+    const int lane = threadIdx.x & 31;
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long warps = ((long)gridDim.x * blockDim.x) >> 5;
     unsigned long long probes = 0;
-    for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
-        const long i = base + threadIdx.x;
-        const bool has = i < n;
+    // one candidate per warp at a time (kin_warp)
+    for (long i = warp; i < n; i += warps) {
         // a start cell outside the frame is rejected (and reported) without
         // reading the grids at it
-        bool inside = false;
-        KinLane t;
-        if (has) {
-            const int cx = sx[i], cz = sz[i];
-            inside = cx >= 0 && cx < I.W && cz >= 0 && cz < I.H;
-            if (inside) {
-                const long pos = (long)cz * I.W + cx;
-                t.k.init(I, cx, cz, steer[i], len[i], velocity, I.heading[pos], I.cost[pos]);
-            } else if (bad_cell) {
-                atomicOr(bad_cell, 1);
+        const int cx = sx[i], cz = sz[i];
+        if (!(cx >= 0 && cx < I.W && cz >= 0 && cz < I.H)) {
+            if (lane == 0) {
+                out[i] = make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
+                if (bad_cell)
+                    atomicOr(bad_cell, 1);
             }
+            continue;
         }
-        run_warp(t, inside, f, probes, [](const KinLane &q) { return q.k.pend_x; },
-                 [](const KinLane &q) { return q.k.pend_z; });
-        if (has)
-            out[i] = (inside && t.k.ok)
-                         ? make_float4((float)t.k.last_x, (float)t.k.last_z, t.k.nodeCost, t.k.heading)
-                         : make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
+        const long pos = (long)cz * I.W + cx;
+        const KinResult r = kin_warp(I, f, cx, cz, steer[i], len[i], velocity, I.heading[pos], I.cost[pos],
+                                     lane, probes);
+        if (lane == 0)
+            out[i] = r.ok ? make_float4((float)r.last_x, (float)r.last_z, r.cost, r.heading)
+                          : make_float4(-1.0f, -1.0f, 0.0f, 0.0f);
     }
     probes = warp_sum64(probes);
-    if ((threadIdx.x & 31) == 0 && probes && probes_out)
+    if (lane == 0 && probes && probes_out)
         atomicAdd(probes_out, probes);
 }
 
@@ -2109,9 +2104,10 @@ void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, c
 {
     if (n <= 0)
         return;
-    int grid = (n + 255) / 256;
-    if (grid > L.work_blocks)
-        grid = L.work_blocks;
+    // one candidate per warp: 8 per block
+    int grid = (n + 7) / 8;
+    if (grid > L.sms * 8)
+        grid = L.sms * 8;
     const size_t smem = (size_t)L.smem_words * 2 * 4;
     k_candidates<<<grid, 256, smem, st>>>(d_inst, slot, n, sx, sz, steer, len, velocity, out, probes,
                                           L.smem_words, bad_cell);

@@ -31,6 +31,7 @@ struct Sched {
     int *node_start;          // [n_slots + 1] prefix of node chunks per slot
     int *gd_start;            // [n_slots + 1] prefix of listed direct-connection cells per slot
     int *goal_start;          // [n_slots + 1] prefix of (node, window chunk) units per slot
+    int *cand_exact;          // [n_slots + 1] prefix of candidates per slot
     unsigned *grab;           // [4] dynamic work counters
 };
 
