@@ -13,7 +13,10 @@ requests through S slots with continuous batching: a request is admitted
 when a slot frees up (frame masks, deferred goal connections, start node),
 planned in the same graph launches as the others until it reaches its goal
 or its timeout, then extracted and validated on the device.  Only validated
-plans count.
+plans count.  The headline operating point is the autotuner's
+(fastrrt_b200/tuned.json): the fastest slot count, harvest interval and
+expansion proposal (the learned network or uniform draws) whose success
+rate meets the reference planner's minus one point.
 
   value   : validated plans/s with the frames already in HBM (device clock,
             CUDA events around each step, max over ranks)
@@ -26,9 +29,10 @@ plans count.
             (oracle/, all host cores) on a bounded sample of the workload
 
 Each step plans frames never planned before; the per-step working set (S
-slots x ~6.3 MB of node grid and scratch) exceeds L2.  Under torchrun every
-rank serves its own requests (weak scaling, no collective on the data path);
-the time is the maximum over ranks.
+slots x ~6.6 MB of node grid and scratch) exceeds L2.  With --gpus N > 1 and
+no torchrun environment the script starts N ranks itself (one process per
+GPU); every rank serves its own requests (weak scaling, no collective on the
+data path) and the time is the maximum over ranks.
 """
 import argparse
 import json
@@ -56,19 +60,36 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--requests", type=int, default=4096, help="requests per step and GPU")
+    ap.add_argument("--requests", type=int, default=8192, help="requests per step and GPU")
     ap.add_argument("--slots", type=int, default=None,
                     help="planning slots per GPU (default: the autotuned value, else 512)")
     ap.add_argument("--check-every", type=int, default=None,
                     help="graph launches between harvests (default: autotuned, else 2)")
     ap.add_argument("--rates", default="200,1000,5000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--rate-requests", type=int, default=600)
-    ap.add_argument("--mix", type=float, default=0.8, help="learned-proposal sampling probability")
+    ap.add_argument("--mix", type=float, default=None,
+                    help="learned-proposal sampling probability (default: the autotuned one; "
+                         "< 0: uniform draws only)")
     ap.add_argument("--candidates", type=int, default=1 << 20, help="per-candidate microbench size")
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--plain", type=int, default=16, help="plans of the plain single-instance loop")
+    ap.add_argument("--plain", type=int, default=256, help="plans of the plain single-instance loop")
+    ap.add_argument("--ref-plans", type=int, default=None,
+                    help="plans per step of the reference arm (default: one per host core)")
     return ap.parse_args()
+
+
+def spawn_ranks(n, argv):
+    """starts this script as n ranks on this node (torch.distributed.run,
+    rendezvous on 127.0.0.1) and returns their exit status"""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + argv
+    return subprocess.call(cmd)
 
 
 def dist_setup(gpus):
@@ -80,8 +101,11 @@ def dist_setup(gpus):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # NCCL over the GPUs; gloo where there is no GPU (the CPU tests)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -234,9 +258,9 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    per_step = cores
+    per_step = args.ref_plans or cores
     for _ in range(args.warmup):
-        cpu_baseline(cores, cores)
+        cpu_baseline(per_step, cores)
     vals, walls = [], []
     for _ in range(args.steps):
         t0 = time.time()
@@ -245,7 +269,7 @@ def run_reference(args, rank, world):
         vals.append(r["value"])
     value = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "plans/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * float(np.mean(walls)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"C0 plans of seeded {SIZE}x{SIZE} frames, {per_step} per step",
@@ -359,11 +383,169 @@ def pct(a, q):
     return float(np.percentile(a, q)) if len(a) else None
 
 
+def _mixed_frames(args):
+    """requests of the batched workload (a pool worker): seeds and sizes ->
+    (class ids, start, goal, steering limit) per request"""
+    from fastrrt_b200 import synth
+    out = []
+    for seed, sizes in args:
+        cls, st, gl, steer, _ = synth.batch_request(seed, sizes=sizes)
+        out.append((cls, st, gl, steer))
+    return out
+
+
+def mixed_requests(specs, world=1):
+    """batched-workload requests for (seed, sizes) specs, generated by a
+    spawned process pool"""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    parts = [specs[i:i + 64] for i in range(0, len(specs), 64)]
+    workers = max(1, min(32, (os.cpu_count() or 1) // max(1, world), len(parts)))
+    if workers == 1:
+        res = [_mixed_frames(p) for p in parts]
+    else:
+        with cf.ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            res = list(ex.map(_mixed_frames, parts))
+    return [r for part in res for r in part]
+
+
+# frame sizes of the served mixed workload and their shares
+C3_SIZES = ((256, 0.6), (128, 0.3), (512, 0.1))
+C3_BUDGET = 40 << 30  # node-grid budget of the served mixed workload (bytes)
+
+
+def c2_batched(args, rank, world, tuned):
+    """Batched planning of 512 instances in one go (frame sizes 128, 256 and
+    512 drawn uniformly, obstacle coverage U(5, 30) %, start near the bottom
+    centre, goal on the top band, steering limit U(30, 45) deg), 100 ms
+    timeout per instance: validated plans/s of whole batches (device clock),
+    success rate, per-kernel shares of one batch (kernel-timing replay)."""
+    import torch
+
+    import fastrrt_b200 as F
+    from fastrrt_b200 import synth
+    n = 512
+    steps = max(1, min(args.steps, 3))
+    specs = [(20_000_000 + rank * 1_000_003 + s * n + k, (128, 256, 512)) for s in range(steps + 1)
+             for k in range(n)]
+    data = mixed_requests(specs, world)
+    launch = (tuned or {}).get("c2_launch") or {"sweep_blocks_per_sm": 16, "work_blocks_per_sm": 2}
+    planner = F.BatchPlanner(n, 512, 512)
+    planner.set_launch(launch["sweep_blocks_per_sm"], launch["work_blocks_per_sm"])
+    keep = []
+
+    def batch(s):
+        reqs = []
+        for k in range(n):
+            cls, st, gl, steer = data[s * n + k]
+            d = torch.from_numpy(np.ascontiguousarray(cls)).cuda()
+            keep.append(d)
+            reqs.append(F.batch.device_request(
+                F.make_request(cls, synth.CLASS_COSTS, st, gl, max_steering_deg=steer,
+                               seed=specs[s * n + k][0], m_per_px=M_PER_PX, timeout_ms=TIMEOUT_MS),
+                d.data_ptr()))
+        return reqs
+
+    batches = [batch(s) for s in range(steps + 1)]
+    torch.cuda.synchronize()
+    planner.plan(batches[0], 100000, 2)  # warm-up, graph capture
+    valid, dev_ms = 0, 0.0
+    for s in range(1, steps + 1):
+        v, _, _, ms = planner.plan(batches[s], 100000, 2)
+        valid += int(v.sum())
+        dev_ms += ms
+    planner.profile(True)
+    planner.plan(batches[1], 100000, 2)
+    kt = planner.kernel_times()
+    planner.profile(False)
+    tot = sum(t[0] for t in kt.values()) or 1.0
+    t_max = max_over_ranks(dev_ms, world)
+    return {"workload": f"{n} instances per batch, frames 128/256/512 uniformly, obstacle coverage "
+                        f"U(5,30)%, steering U(30,45) deg, {TIMEOUT_MS} ms timeout per instance, "
+                        f"one CUDA graph launch per iteration over all instances",
+            "batches": steps, "value": sum_over_ranks(valid, world) / (t_max / 1e3), "unit": "plans/s",
+            "success_rate": valid / float(n * steps), "ms_per_batch": t_max / steps,
+            "launch_shape": launch,
+            "kernel_share": {k: round(t[0] / tot, 4) for k, t in
+                             sorted(kt.items(), key=lambda kv: -kv[1][0]) if t[0] > 0}}
+
+
+def c3_serving(args, rank, world, tuned, attach_net):
+    """Served planning of the mixed workload: Poisson arrivals at the C3
+    rates, frames 60 % 256x256, 30 % 128x128, 10 % 512x512 (the batched
+    workload's generator), admission by device memory against a 40 GB
+    node-grid budget (each request takes storage sized by its frame), 100
+    ms timeout per request, latency from arrival to finish."""
+    import torch
+
+    import fastrrt_b200 as F
+    from fastrrt_b200 import synth
+    n = args.rate_requests
+    rng = np.random.default_rng(4321 + rank)
+    sizes = rng.choice([c[0] for c in C3_SIZES], size=n, p=[c[1] for c in C3_SIZES])
+    specs = [(30_000_000 + rank * 1_000_003 + k, (int(sizes[k]),)) for k in range(n)]
+    data = mixed_requests(specs, world)
+    slots = args.slots
+    planner = F.BatchPlanner(slots, 512, 512, budget_bytes=C3_BUDGET)
+    launch = (tuned or {})
+    if launch:
+        planner.set_launch(launch["sweep_blocks_per_sm"], launch["work_blocks_per_sm"])
+    attach_net(planner)
+    keep, reqs = [], []
+    for k in range(n):
+        cls, st, gl, steer = data[k]
+        d = torch.from_numpy(np.ascontiguousarray(cls)).cuda()
+        keep.append(d)
+        reqs.append(F.batch.device_request(
+            F.make_request(cls, synth.CLASS_COSTS, st, gl, max_steering_deg=steer, seed=specs[k][0],
+                           m_per_px=M_PER_PX, timeout_ms=TIMEOUT_MS), d.data_ptr()))
+    torch.cuda.synchronize()
+    planner.serve(reqs[:min(n, 64)], timeout_ms=TIMEOUT_MS, check_every=args.check_every)
+    res = {"workload": "Poisson arrivals, frames 60% 256x256 / 30% 128x128 / 10% 512x512, "
+                       f"{TIMEOUT_MS} ms timeout, admission by device memory against a "
+                       f"{C3_BUDGET >> 30} GB node-grid budget, at most {slots} requests at once",
+           "requests_per_rate": n, "size_counts": {str(c[0]): int((sizes == c[0]).sum()) for c in C3_SIZES},
+           "slot_bytes": {str(c[0]): F.batch.slot_bytes(c[0], c[0]) for c in C3_SIZES}}
+    for rate in [float(x) for x in args.rates.split(",") if x]:
+        arrival = np.cumsum(rng.exponential(1e3 / rate, n))
+        out = planner.serve(reqs, arrival_ms=arrival, timeout_ms=TIMEOUT_MS, check_every=args.check_every)
+        v = out["valid"] > 0
+        lat = out["latency_ms"][v]
+        res[f"{rate:g}_req_s"] = {
+            "offered": rate, "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
+            "success_rate": float(v.mean()), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
+            "p99_ms": pct(lat, 99),
+            "success_by_size": {str(c[0]): float(v[sizes == c[0]].mean()) for c in C3_SIZES
+                                if (sizes == c[0]).any()}}
+    budget, used, peak = planner.memory()
+    res["memory"] = {"budget_bytes": budget, "peak_bytes_held": peak, "bytes_held_after": used}
+    planner.set_proposal(None)
+    return res
+
+
+def issue_peak(peaks):
+    """lane-issue peak of the footprint-probe roofline: SMs x 32 lanes x the
+    measured maximum SM clock (probe lanes per second)"""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    return sms * 32 * mhz * 1e6, sms, mhz
+
+
+# DRAM bytes per launch of the dominant search kernels, from one ncu capture
+# each (profiles/search_kernels_served_256x256.txt: dram__bytes_read.sum +
+# dram__bytes_write.sum of a steady-state launch, scaled to the bench's
+# launch by the listed units)
+NCU_DRAM_BYTES_PER_UNIT = {}
+
+
 def run_mine(args, rank, world, local):
     import torch
 
     import fastrrt_b200 as F
     from fastrrt_b200 import autotune, synth
+    from fastrrt_b200 import proposal as P
+    from fastrrt_b200 import train_proposal as TP
     F._lib.require_cuda()
     torch.cuda.set_device(local)
     tuned = autotune.load()
@@ -371,8 +553,12 @@ def run_mine(args, rank, world, local):
         args.slots = tuned["slots"]
     if tuned and args.check_every is None:
         args.check_every = tuned["check_every"]
+    if args.mix is None:
+        args.mix = tuned.get("mix") if tuned else 0.8
+        if args.mix is None:
+            args.mix = -1.0
     args.slots = args.slots or 512
-    args.check_every = args.check_every or 2
+    args.check_every = args.check_every or 1
     R = args.requests
     total_steps = args.warmup + args.steps
     t_gen = time.time()
@@ -382,6 +568,12 @@ def run_mine(args, rank, world, local):
     if tuned:
         planner.set_launch(tuned["sweep_blocks_per_sm"], tuned["work_blocks_per_sm"])
     costs = synth.CLASS_COSTS
+    net = P.ProposalNet(seed=0, max_batch=512)
+    have_net = TP.load(net)
+    learned = args.mix >= 0 and have_net
+
+    def attach(use_net):
+        planner.set_proposal(net if use_net else None, mix=args.mix if use_net else 0.0)
 
     def requests(frames, starts, goals, seeds, device_frames=None):
         reqs = []
@@ -397,44 +589,41 @@ def run_mine(args, rank, world, local):
         return planner.serve(reqs, arrival_ms=arrival, timeout_ms=TIMEOUT_MS,
                              check_every=args.check_every)
 
+    def timed_steps(reqs_of_step, clocks=None):
+        """the timed steps: (device ms summed, validated plans, service ms, loops, lengths)"""
+        barrier(world)
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        dev_ms, valid, service, loops, lengths = 0.0, 0, [], [], []
+        for s in range(args.warmup, total_steps):
+            out = serve(reqs_of_step(s))
+            dev_ms += out["device_ms"]
+            v = out["valid"] > 0
+            valid += int(v.sum())
+            service.extend(out["service_ms"][v].tolist())
+            lengths.extend(out["length"][v].tolist())
+            loops.extend(out["loops"].tolist())
+        torch.cuda.synchronize()
+        barrier(world)
+        return dev_ms, valid, service, loops, lengths
+
     # frames resident in HBM for `value`
     dev = [torch.from_numpy(work[s][0]).cuda() for s in range(total_steps)]
     reqs_dev = [requests(*work[s], device_frames=dev[s]) for s in range(total_steps)]
     torch.cuda.synchronize()
+    attach(learned)
     for s in range(args.warmup):
         serve(reqs_dev[s])
     sampler = ClockSampler(local)
-    sampler.start()
-    barrier(world)
-    torch.cuda.synchronize()
-    dev_ms = 0.0
-    valid_total = 0
-    service, lengths, loops = [], [], []
-    for s in range(args.warmup, total_steps):
-        out = serve(reqs_dev[s])
-        dev_ms += out["device_ms"]
-        v = out["valid"] > 0
-        valid_total += int(v.sum())
-        service.extend(out["service_ms"][v].tolist())
-        lengths.extend(out["length"][v].tolist())
-        loops.extend(out["loops"].tolist())
-    torch.cuda.synchronize()
-    barrier(world)
+    dev_ms, valid_total, service, loops, lengths = timed_steps(lambda s: reqs_dev[s], sampler)
     clocks = sampler.stop()
     t_max = max_over_ranks(dev_ms, world)
     plans = sum_over_ranks(valid_total, world)
     value = plans / (t_max / 1e3)
 
     # e2e: host frames through the C ABI (H2D of frames, D2H of results inside)
-    e2e_ms = 0.0
-    e2e_valid = 0
-    barrier(world)
-    torch.cuda.synchronize()
-    for s in range(args.warmup, total_steps):
-        out = serve(requests(*work[s]))
-        e2e_ms += out["device_ms"]
-        e2e_valid += int((out["valid"] > 0).sum())
-    barrier(world)
+    e2e_ms, e2e_valid, _, _, _ = timed_steps(lambda s: requests(*work[s]))
     e2e_t = max_over_ranks(e2e_ms, world)
     e2e_plans = sum_over_ranks(e2e_valid, world)
     h2d = R * (SIZE * SIZE + 4 * len(costs))
@@ -463,30 +652,28 @@ def run_mine(args, rank, world, local):
 
     serving = poisson()
 
-    # the same served workload with the learned expansion proposal attached
-    learned = None
-    from fastrrt_b200 import proposal as P
-    from fastrrt_b200 import train_proposal as TP
-    net = P.ProposalNet(seed=0, max_batch=512)
-    if TP.load(net):
-        planner.set_proposal(net, mix=args.mix)
+    # the same served workload with the other proposal (uniform draws when
+    # the headline uses the network, the network when it does not)
+    other = None
+    if have_net:
+        attach(not learned)
         serve(reqs_dev[0])
-        l_ms, l_valid, l_service = 0.0, 0, []
-        for s in range(args.warmup, total_steps):
-            out = serve(reqs_dev[s])
-            l_ms += out["device_ms"]
-            v = out["valid"] > 0
-            l_valid += int(v.sum())
-            l_service.extend(out["service_ms"][v].tolist())
-        l_serving = poisson()  # the same arrivals, the network attached
-        planner.set_proposal(None)
-        l_t = max_over_ranks(l_ms, world)
-        learned = {"value": sum_over_ranks(l_valid, world) / (l_t / 1e3), "unit": "plans/s",
-                   "mix": args.mix, "success_rate": l_valid / float(R * args.steps),
-                   "service_p50_ms": pct(l_service, 50), "service_p99_ms": pct(l_service, 99),
-                   "serving": l_serving,
-                   "note": "same requests and Poisson arrivals, network weights trained on the "
-                           "planner's own solves of held-out requests (fastrrt_b200/train_proposal.py)"}
+        o_ms, o_valid, o_service, o_loops, _ = timed_steps(lambda s: reqs_dev[s])
+        o_serving = poisson()
+        o_t = max_over_ranks(o_ms, world)
+        other = {"proposal": "uniform" if learned else f"learned (mix {max(args.mix, 0.8):g})",
+                 "value": sum_over_ranks(o_valid, world) / (o_t / 1e3), "unit": "plans/s",
+                 "success_rate": o_valid / float(R * args.steps),
+                 "service_p50_ms": pct(o_service, 50), "service_p99_ms": pct(o_service, 99),
+                 "mean_loops": float(np.mean(o_loops)) if o_loops else None,
+                 "serving": o_serving}
+        attach(learned)
+
+    def attach_to(pl):
+        pl.set_proposal(net if learned else None, mix=args.mix if learned else 0.0)
+
+    c3 = c3_serving(args, rank, world, tuned, attach_to)
+    c2 = c2_batched(args, rank, world, tuned)
 
     # kernel timing replay of one step (same inputs, kernels launched one by one)
     planner.profile(True)
@@ -494,24 +681,29 @@ def run_mine(args, rank, world, local):
     ktimes = planner.kernel_times()
     probes = planner.probes()
     planner.profile(False)
-    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
-    name, (kms, kn) = dom
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
-    alg_bytes = probes.get(name.split("(")[0], 0)  # 1 byte per reference footprint probe
-    per_launch_ms = kms / max(kn, 1)
-    achieved = (alg_bytes / max(kn, 1)) / (per_launch_ms * 1e-3) / 1e9 if alg_bytes else 0.0
     total_k = sum(v[0] for v in ktimes.values())
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
+    name, (kms, kn) = dom
+    per_launch_ms = kms / max(kn, 1)
+    # the probe-issue roofline of the dominant search kernel: reference
+    # footprint probes per second against one probe per lane per cycle
+    peak, sms, mhz = issue_peak(peaks)
+    alg = probes.get(name.split("(")[0], 0)
+    achieved = (alg / max(kn, 1)) / (per_launch_ms * 1e-3) if alg else 0.0
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
 
     line = None
     if rank == 0:
         plain = plain_loop(args.plain, rank)
         cpu = None if args.no_cpu_baseline else cpu_baseline()
         micro = candidate_microbench(args.candidates, cpu=not args.no_cpu_baseline)
+        proposal = (f"learned network (mix {args.mix:g}, fastrrt_b200/proposal_weights.npz)"
+                    if learned else "uniform draws")
         line = {
             "metric": METRIC, "value": value, "unit": "plans/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -519,9 +711,10 @@ def run_mine(args, rank, world, local):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"served C0 planning: {R} requests of seeded {SIZE}x{SIZE} "
                                    f"frames per step and GPU, continuous batching over "
-                                   f"{args.slots} slots, {TIMEOUT_MS} ms timeout per request",
+                                   f"{args.slots} slots, {TIMEOUT_MS} ms timeout per request, "
+                                   f"expansion proposal: {proposal}",
                        "requests_per_step_per_gpu": R, "slots_per_gpu": args.slots,
-                       "check_every": args.check_every,
+                       "check_every": args.check_every, "proposal": proposal,
                        "launch_shape": ({k: tuned[k] for k in ("sweep_blocks_per_sm", "work_blocks_per_sm")}
                                         if tuned else "default"),
                        "frame": f"{SIZE}x{SIZE} @ {M_PER_PX} m/px",
@@ -532,20 +725,26 @@ def run_mine(args, rank, world, local):
             "mean_loops": float(np.mean(loops)) if loops else None,
             "mean_path_len_px": float(np.mean(lengths)) if lengths else None,
             "serving": serving,
-            "learned_proposal": learned,
+            "serving_mixed_sizes": c3,
+            "batched_mixed_sizes": c2,
+            "other_proposal": other,
             "candidate_kernels": micro,
             "plain_gpu_loop": plain,
             "served_over_plain": value / plain["plans_per_s"] if plain["plans_per_s"] else None,
             "e2e": {"value": e2e_plans / (e2e_t / 1e3), "unit": "plans/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(v[1] for v in ktimes.values()) * args.steps),
-            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm if hbm else None,
-                         "traffic": None,
-                         "algorithmic": "1 byte (frame class) per footprint probe of the reference "
-                                        "algorithm executed by this kernel's work",
+            "roofline": {"bound": "issue", "kernel": name, "achieved": achieved / 1e9, "peak": peak / 1e9,
+                         "unit": "Gprobe/s", "frac": achieved / peak if peak else None,
+                         "traffic": NCU_DRAM_BYTES_PER_UNIT.get(name),
+                         "algorithmic": "reference footprint probes (class lookups of "
+                                        "__computeFeasibleForAngle) the kernel's work stands for, "
+                                        f"against one per lane per cycle ({sms} SMs x 32 lanes x "
+                                        f"{mhz:g} MHz, of measured clock)",
                          "avg_launch_ms": per_launch_ms, "launches": kn,
-                         "share_of_device_time": kms / total_k if total_k else None},
+                         "share_of_device_time": kms / total_k if total_k else None,
+                         "probe_bytes_gbs": alg / max(kn, 1) / (per_launch_ms * 1e-3) / 1e9,
+                         "hbm_gbs_of_measured": hbm},
             "kernel_ms": {k: round(v[0], 3) for k, v in ktimes.items()},
             "clocks": clocks,
             "cpu_baseline": cpu,
@@ -561,6 +760,8 @@ def run_mine(args, rank, world, local):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus, sys.argv[1:]))
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)

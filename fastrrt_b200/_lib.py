@@ -42,7 +42,8 @@ EXPORTS = [
     "loop", "path_optimize", "export_graph_nodes", "release_export_graph_nodes",
     "get_planned_path", "interpolate_planned_path", "release_planned_path_data",
     "interpolate_planned_path_p", "ideal_curve", "compute_region_debug_performance",
-    "save_current_graph_state", "load_graph_state",
+    "save_current_graph_state", "load_graph_state", "fastrrt_check_graph_consistent",
+    "fastrrt_validate_path",
     # frames, seeding, errors
     "fastrrt_last_error", "fastrrt_frame_create", "fastrrt_frame_create_f3",
     "fastrrt_frame_destroy", "fastrrt_set_seed", "fastrrt_probe_count", "fastrrt_loop_count",
@@ -52,7 +53,8 @@ EXPORTS = [
     "fastrrt_candidates_hermite_device", "fastrrt_candidates_feasible",
     "fastrrt_candidates_kinematic_noalloc",
     # batched planner
-    "fastrrt_batch_create", "fastrrt_batch_destroy", "fastrrt_batch_admit",
+    "fastrrt_batch_create", "fastrrt_batch_create_budget", "fastrrt_slot_bytes",
+    "fastrrt_batch_memory", "fastrrt_batch_destroy", "fastrrt_batch_admit",
     "fastrrt_batch_admit_many", "fastrrt_batch_run", "fastrrt_batch_step", "fastrrt_batch_status",
     "fastrrt_batch_collect", "fastrrt_batch_path", "fastrrt_batch_release",
     "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
@@ -102,6 +104,8 @@ def lib():
         "compute_region_debug_performance": (None, [vp]),
         "save_current_graph_state": (None, [vp, C.c_char_p]),
         "load_graph_state": (None, [vp, C.c_char_p]),
+        "fastrrt_check_graph_consistent": (C.c_int, [vp]),
+        "fastrrt_validate_path": (C.c_int, [vp, f32p, C.c_int]),
         "fastrrt_last_error": (C.c_char_p, []),
         "fastrrt_frame_create": (vp, [C.c_int, C.c_int, u8p, f32p, C.c_int, vp]),
         "fastrrt_frame_create_f3": (vp, [C.c_int, C.c_int, f32p, f32p, C.c_int]),
@@ -128,6 +132,9 @@ def lib():
                                                            C.c_double, C.c_int, vp, vp, vp, vp,
                                                            C.c_float, vp, vp, vp]),
         "fastrrt_batch_create": (vp, [C.c_int, C.c_int, C.c_int]),
+        "fastrrt_batch_create_budget": (vp, [C.c_int, C.c_int, C.c_int, C.c_uint64]),
+        "fastrrt_slot_bytes": (C.c_uint64, [C.c_int, C.c_int]),
+        "fastrrt_batch_memory": (C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
         "fastrrt_batch_destroy": (None, [vp]),
         "fastrrt_batch_admit": (C.c_int, [vp, C.c_int, P(Request), C.c_int]),
         "fastrrt_batch_admit_many": (C.c_int, [vp, C.c_int, P(Request), C.c_int]),

@@ -58,13 +58,37 @@ def device_request(r, device_ptr):
     return d
 
 
+def slot_bytes(width, height):
+    """device memory of one planning slot's storage for a width x height frame"""
+    return int(_lib.lib().fastrrt_slot_bytes(int(width), int(height)))
+
+
 class BatchPlanner:
-    def __init__(self, n_slots, max_width, max_height):
-        h = _lib.lib().fastrrt_batch_create(n_slots, max_width, max_height)
+    """Many planning requests in one CUDA graph launch per iteration.
+
+    Without `budget_bytes` every one of the n_slots slots holds storage for
+    a max_width x max_height frame.  With it, n_slots is the most requests
+    planned at once and each admitted request takes storage sized by its own
+    frame from an arena of budget_bytes; admission waits (serve) or fails
+    (admit) while the arena has no room."""
+
+    def __init__(self, n_slots, max_width, max_height, budget_bytes=0):
+        L = _lib.lib()
+        if budget_bytes:
+            h = L.fastrrt_batch_create_budget(n_slots, max_width, max_height, int(budget_bytes))
+        else:
+            h = L.fastrrt_batch_create(n_slots, max_width, max_height)
         if not h:
             raise _lib.FastRRTError("batch_create: " + _lib.last_error())
         self._h = h
         self.n_slots = n_slots
+
+    def memory(self):
+        """(budget, bytes held now, most bytes held) of the slots' storage"""
+        b, u, p = _lib.C.c_uint64(), _lib.C.c_uint64(), _lib.C.c_uint64()
+        _lib.check(_lib.lib().fastrrt_batch_memory(self._h, _lib.C.byref(b), _lib.C.byref(u),
+                                                   _lib.C.byref(p)), "batch_memory")
+        return b.value, u.value, p.value
 
     def __del__(self):
         try:

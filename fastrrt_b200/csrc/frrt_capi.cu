@@ -424,6 +424,34 @@ int *export_graph_nodes(void *ptr)
 
 void release_export_graph_nodes(int *ptr) { delete[] ptr; }
 
+int fastrrt_check_graph_consistent(void *ptr)
+{
+    Planner *p = as_planner(ptr);
+    if (!p)
+        return -1;
+    if (p->eng->inst(0).W == 0) {
+        set_error("check_graph_consistent: set_plan_data first");
+        return -1;
+    }
+    int ok = 0;
+    return p->eng->check_graph(0, ok) ? ok : -1;
+}
+
+int fastrrt_validate_path(void *ptr, const float *xyh, int n)
+{
+    Planner *p = as_planner(ptr);
+    if (!p || n < 0 || (n > 0 && !xyh)) {
+        set_error("validate_path: bad arguments");
+        return -1;
+    }
+    if (p->eng->inst(0).W == 0) {
+        set_error("validate_path: set_plan_data first");
+        return -1;
+    }
+    int ok = 0;
+    return p->eng->check_path(0, xyh, n, ok) ? ok : -1;
+}
+
 void compute_region_debug_performance(void *ptr)
 {
     // computeGraphRegionDensity (graph_expansion_search_zones.cu:111-159)
@@ -784,6 +812,45 @@ void *fastrrt_batch_create(int n_slots, int max_width, int max_height)
     return b;
 }
 
+void *fastrrt_batch_create_budget(int max_slots, int max_width, int max_height, uint64_t budget_bytes)
+{
+    if (budget_bytes == 0) {
+        set_error("batch create: a memory budget of 0 bytes");
+        return nullptr;
+    }
+    auto *b = new (std::nothrow) Batch();
+    if (!b)
+        return nullptr;
+    b->eng.reset(new (std::nothrow) Engine(max_slots, max_width, max_height, -1, (size_t)budget_bytes));
+    if (!b->eng || !b->eng->ok() || cudaEventCreate(&b->ev0) != cudaSuccess ||
+        cudaEventCreate(&b->ev1) != cudaSuccess) {
+        delete b;
+        return nullptr;
+    }
+    return b;
+}
+
+int fastrrt_batch_memory(void *batch, uint64_t *budget, uint64_t *used, uint64_t *peak)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b) {
+        set_error("batch memory: bad arguments");
+        return -1;
+    }
+    if (budget)
+        *budget = b->eng->budget();
+    if (used)
+        *used = b->eng->used();
+    if (peak)
+        *peak = b->eng->peak_used();
+    return 0;
+}
+
+uint64_t fastrrt_slot_bytes(int width, int height)
+{
+    return width > 0 && height > 0 ? (uint64_t)Engine::slot_bytes(width, height) : 0;
+}
+
 void fastrrt_batch_destroy(void *batch) { delete static_cast<Batch *>(batch); }
 
 int fastrrt_batch_admit_many(void *batch, int n, const fastrrt_request *reqs, int timeout_ms)
@@ -1032,9 +1099,11 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
     // slots left live by an earlier call take no part
     if (!e.fetch_states(true))
         return -1;
-    for (int s = 0; s < n_slots; s++)
+    for (int s = 0; s < n_slots; s++) {
         if (e.state(s).active && !e.state(s).done && !e.deactivate(s))
             return -1;
+        e.release_storage(s);  // budget mode: the whole arena for this call
+    }
     // device clock -> host clock: one read bracketed by host reads
     long long dev0 = 0;
     const double ha = now_ms();
@@ -1056,6 +1125,17 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
         list.clear();
         while (next < n && !free_slots.empty() && (!arrival_ms || arrival_ms[next] <= now)) {
             const int s = free_slots.back();
+            // admission by device memory: the request waits (in arrival
+            // order) until the arena has room for its frame's storage
+            if (!e.ensure_storage(s, reqs[next].width, reqs[next].height)) {
+                if (!e.out_of_budget())
+                    return -1;
+                if (in_flight == 0 && list.empty()) {
+                    set_error("batch serve: a request needs more memory than the whole budget");
+                    return -1;
+                }
+                break;
+            }
             free_slots.pop_back();
             if (!load_request(e, s, reqs[next], timeout_ms))
                 return -1;
@@ -1114,6 +1194,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                 loops[r] = S.loops;
             owner[s] = -1;
             free_slots.push_back(s);
+            e.release_storage(s);  // budget mode: back to the arena
             in_flight--;
             finished++;
         }
@@ -1251,7 +1332,10 @@ int fastrrt_batch_release(void *batch, int slot)
     auto *b = static_cast<Batch *>(batch);
     if (!b || slot < 0 || slot >= b->eng->n_slots())
         return -1;
-    return b->eng->deactivate(slot) ? 0 : -1;
+    if (!b->eng->deactivate(slot))
+        return -1;
+    b->eng->release_storage(slot);
+    return 0;
 }
 
 }  // extern "C"

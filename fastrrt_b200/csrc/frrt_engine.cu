@@ -109,7 +109,179 @@ bool Engine::check(cudaError_t e, const char *what)
     return false;
 }
 
-Engine::Engine(int n_slots, int max_w, int max_h, int device)
+// byte sizes of the parts of one slot's storage for a W x H frame (C = cells
+// rounded up to a sweep chunk), each part 256-byte aligned
+namespace {
+constexpr int kParts = 37;
+void slot_parts(int W, int H, size_t parts[kParts])
+{
+    const size_t C = align_up((size_t)W * H, kSweepCells);
+    const size_t mw = align_up((size_t)((W + 31) / 32) * H, 4);
+    const size_t p[kParts] = {
+        C,                                  // 0 type
+        4 * C, 4 * C,                       // 1 parent, 2 child
+        4 * C, 4 * C, 4 * C, 4 * C,         // 3 heading, 4 cost, 5 intrinsic, 6 direct
+        C, 4 * C, 4 * C,                    // 7 gd flag, 8 heading, 9 cost
+        4 * C,                              // 10 claim
+        4 * C, 4 * C, 4 * C, 4 * C,         // 11 cand, 12 end, 13 heading, 14 cost
+        4 * C, 8 * C, 4 * C, 4 * C,         // 15 nodes, 16 best key, 17 pending, 18 pruned
+        C,                                  // 19 own class ids
+        4 * mw,                             // 20 blocked
+        4 * mw,                             // 21 clear
+        4 * (size_t)kMaxRegions,            // 22 region_count
+        4 * (size_t)kMaxRegions,            // 23 region_new
+        4 * mw,                             // 24 clear-mask scratch
+        C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
+        8 * C, 8 * C,                       // 27 memo key, 28 memo result
+        2 * (size_t)(W + 1) * (H + 1),      // 29 obstacle summed-area table
+        4 * C, 4 * C, 4 * C, 4 * C, 4 * C,  // 30 cand steer, 31 cand len, 32 prop row, 33/34 prop
+        4 * C, 4 * C,                       // 35 exp steer, 36 exp len
+    };
+    for (int k = 0; k < kParts; k++)
+        parts[k] = align_up(p[k], 256);
+}
+}  // namespace
+
+size_t Engine::slot_bytes(int W, int H)
+{
+    size_t parts[kParts], total = 0;
+    slot_parts(W, H, parts);
+    for (size_t b : parts)
+        total += b;
+    return align_up(total, 4096);
+}
+
+// points the slot's record at its storage (store_off_ in the arena) laid out
+// for a W x H frame; the claim array starts free
+bool Engine::layout_slot(int s, int W, int H)
+{
+    size_t parts[kParts];
+    slot_parts(W, H, parts);
+    void *ptr[kParts];
+    char *base = (char *)arena_ + store_off_[s];
+    for (int k = 0; k < kParts; k++) {
+        ptr[k] = base;
+        base += parts[k];
+    }
+    Inst &I = h_inst_[s];
+    I.type = (int8_t *)ptr[0];
+    I.parent = (int32_t *)ptr[1];
+    I.child = (int32_t *)ptr[2];
+    I.heading = (float *)ptr[3];
+    I.cost = (float *)ptr[4];
+    intrinsic_[s] = (float *)ptr[5];
+    I.intrinsic = nullptr;  // zero intrinsic costs: the reference's default
+    I.direct = (float *)ptr[6];
+    I.gd_flag = (uint8_t *)ptr[7];
+    I.gd_heading = (float *)ptr[8];
+    I.gd_cost = (float *)ptr[9];
+    I.claim = (int32_t *)ptr[10];
+    I.cand = (int32_t *)ptr[11];
+    I.cand_end = (int32_t *)ptr[12];
+    I.cand_heading = (float *)ptr[13];
+    I.cand_cost = (float *)ptr[14];
+    I.nodes = (int32_t *)ptr[15];
+    I.node_key = (unsigned long long *)ptr[16];
+    I.node_pending = (int32_t *)ptr[17];
+    I.node_pruned = (int32_t *)ptr[18];
+    own_cls_[s] = (uint8_t *)ptr[19];
+    I.cls = own_cls_[s];
+    I.blocked = (const uint32_t *)ptr[20];
+    I.clear = (const uint32_t *)ptr[21];
+    I.region_count = (unsigned *)ptr[22];
+    I.region_new = (unsigned *)ptr[23];
+    I.rowdil = (uint32_t *)ptr[24];
+    I.gd_req = (uint32_t *)ptr[25];
+    I.gd_list = (int32_t *)ptr[26];
+    I.memo_key = (unsigned long long *)ptr[27];
+    I.memo_result = (unsigned long long *)ptr[28];
+    I.sat = (const uint16_t *)ptr[29];
+    I.cand_steer = (float *)ptr[30];
+    I.cand_len = (float *)ptr[31];
+    I.prop_row = (int32_t *)ptr[32];
+    I.prop_steer = (float *)ptr[33];
+    I.prop_len = (float *)ptr[34];
+    I.exp_steer = (float *)ptr[35];
+    I.exp_len = (float *)ptr[36];
+    dirty_ = true;
+    return check(cudaMemsetAsync(I.claim, 0x7F, parts[10], stream_), "claim init");
+}
+
+bool Engine::ensure_storage(int slot, int W, int H)
+{
+    out_of_budget_ = false;
+    if (!budget_)
+        return W <= max_w_ && H <= max_h_;
+    if (store_bytes_[slot] && store_w_[slot] == W && store_h_[slot] == H)
+        return true;
+    release_storage(slot);
+    const size_t need = slot_bytes(W, H);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+        if (it->second < need)
+            continue;
+        const size_t off = it->first, len = it->second;
+        free_.erase(it);
+        if (len > need)
+            free_[off + need] = len - need;
+        store_off_[slot] = off;
+        store_bytes_[slot] = need;
+        store_w_[slot] = W;
+        store_h_[slot] = H;
+        used_ += need;
+        peak_used_ = std::max(peak_used_, used_);
+        return layout_slot(slot, W, H);
+    }
+    out_of_budget_ = true;
+    set_error("admission: device memory budget exhausted (" + std::to_string(need) + " bytes needed, " +
+              std::to_string(budget_ - used_) + " of " + std::to_string(budget_) + " free)");
+    return false;
+}
+
+void Engine::release_storage(int slot)
+{
+    if (!budget_ || !store_bytes_[slot])
+        return;
+    size_t off = store_off_[slot], len = store_bytes_[slot];
+    used_ -= len;
+    // merge with the free neighbours
+    auto next = free_.lower_bound(off);
+    if (next != free_.end() && off + len == next->first) {
+        len += next->second;
+        next = free_.erase(next);
+    }
+    if (next != free_.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+            off = prev->first;
+            len += prev->second;
+            free_.erase(prev);
+        }
+    }
+    free_[off] = len;
+    store_bytes_[slot] = 0;
+    store_w_[slot] = store_h_[slot] = 0;
+    // no frame: no sweep chunks, no pointers
+    Inst &I = h_inst_[slot];
+    const Physical ph = h_phys_[slot];
+    const double ms = I.max_steer, lr = I.lr;
+    const float mc = I.max_curvature;
+    const float *costs = I.class_costs;
+    memset(&I, 0, sizeof(Inst));
+    I.class_costs = costs;
+    I.max_steer = ms;
+    I.lr = lr;
+    I.max_curvature = mc;
+    I.lbx = ph.lbx;
+    I.lbz = ph.lbz;
+    I.ubx = ph.ubx;
+    I.ubz = ph.ubz;
+    I.stop_on_goal = 1;
+    own_cls_[slot] = nullptr;
+    intrinsic_[slot] = nullptr;
+    dirty_ = true;
+}
+
+Engine::Engine(int n_slots, int max_w, int max_h, int device, size_t budget_bytes)
 {
     if (n_slots <= 0 || max_w <= 0 || max_h <= 0 || max_w > 4095 || max_h > 4095) {
         set_error("engine: bad slot count or frame size (frames up to 4095 x 4095)");
@@ -129,95 +301,46 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device)
     if (!check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))
         return;
 
-    const size_t C = align_up((size_t)max_cells_, kSweepCells);
     const int rw = (max_w + 31) / 32;
     mask_words_ = (int)align_up((size_t)rw * max_h, 4);
-    const size_t parts[] = {
-        C,                                  // 0 type
-        4 * C, 4 * C,                       // 1 parent, 2 child
-        4 * C, 4 * C, 4 * C, 4 * C,         // 3 heading, 4 cost, 5 intrinsic, 6 direct
-        C, 4 * C, 4 * C,                    // 7 gd flag, 8 heading, 9 cost
-        4 * C,                              // 10 claim
-        4 * C, 4 * C, 4 * C, 4 * C,         // 11 cand, 12 end, 13 heading, 14 cost
-        4 * C, 8 * C, 4 * C, 4 * C,         // 15 nodes, 16 best key, 17 pending, 18 pruned
-        C,                                  // 19 own class ids
-        4 * (size_t)mask_words_,            // 20 blocked
-        4 * (size_t)mask_words_,            // 21 clear
-        4 * (size_t)kMaxRegions,            // 22 region_count
-        4 * (size_t)kMaxRegions,            // 23 region_new
-        4 * (size_t)mask_words_,            // 24 clear-mask scratch
-        C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
-        8 * C, 8 * C,                       // 27 memo key, 28 memo result
-        2 * (size_t)(max_w + 1) * (max_h + 1),  // 29 obstacle summed-area table
-        4 * C, 4 * C, 4 * C, 4 * C, 4 * C,  // 30 cand steer, 31 cand len, 32 prop row, 33/34 prop
-        4 * C, 4 * C,                       // 35 exp steer, 36 exp len
-    };
-    constexpr int kParts = sizeof(parts) / sizeof(parts[0]);
-    size_t per_slot = 0;
-    for (size_t b : parts)
-        per_slot += align_up(b, 256);
-    arena_bytes_ = per_slot * n_slots;
-    if (!check(cudaMalloc(&arena_, arena_bytes_), "arena cudaMalloc"))
-        return;
-    if (!check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "arena memset"))
-        return;
     h_inst_.assign(n_slots, Inst{});
     h_phys_.assign(n_slots, Physical{});
     own_cls_.assign(n_slots, nullptr);
     intrinsic_.assign(n_slots, nullptr);
     ncls_.assign(n_slots, 0);
-    char *base = (char *)arena_;
+    store_off_.assign(n_slots, 0);
+    store_bytes_.assign(n_slots, 0);
+    store_w_.assign(n_slots, 0);
+    store_h_.assign(n_slots, 0);
     for (int s = 0; s < n_slots; s++) {
-        void *ptr[kParts];
-        for (int k = 0; k < kParts; k++) {
-            ptr[k] = base;
-            base += align_up(parts[k], 256);
-        }
         Inst &I = h_inst_[s];
         memset(&I, 0, sizeof(Inst));
-        I.type = (int8_t *)ptr[0];
-        I.parent = (int32_t *)ptr[1];
-        I.child = (int32_t *)ptr[2];
-        I.heading = (float *)ptr[3];
-        I.cost = (float *)ptr[4];
-        intrinsic_[s] = (float *)ptr[5];
-        I.intrinsic = nullptr;  // zero intrinsic costs: the reference's default
-        I.direct = (float *)ptr[6];
-        I.gd_flag = (uint8_t *)ptr[7];
-        I.gd_heading = (float *)ptr[8];
-        I.gd_cost = (float *)ptr[9];
-        I.claim = (int32_t *)ptr[10];
-        I.cand = (int32_t *)ptr[11];
-        I.cand_end = (int32_t *)ptr[12];
-        I.cand_heading = (float *)ptr[13];
-        I.cand_cost = (float *)ptr[14];
-        I.nodes = (int32_t *)ptr[15];
-        I.node_key = (unsigned long long *)ptr[16];
-        I.node_pending = (int32_t *)ptr[17];
-        I.node_pruned = (int32_t *)ptr[18];
-        own_cls_[s] = (uint8_t *)ptr[19];
-        I.cls = own_cls_[s];
-        I.blocked = (const uint32_t *)ptr[20];
-        I.clear = (const uint32_t *)ptr[21];
-        I.region_count = (unsigned *)ptr[22];
-        I.region_new = (unsigned *)ptr[23];
-        I.rowdil = (uint32_t *)ptr[24];
-        I.gd_req = (uint32_t *)ptr[25];
-        I.gd_list = (int32_t *)ptr[26];
-        I.memo_key = (unsigned long long *)ptr[27];
-        I.memo_result = (unsigned long long *)ptr[28];
-        I.sat = (const uint16_t *)ptr[29];
-        I.cand_steer = (float *)ptr[30];
-        I.cand_len = (float *)ptr[31];
-        I.prop_row = (int32_t *)ptr[32];
-        I.prop_steer = (float *)ptr[33];
-        I.prop_len = (float *)ptr[34];
-        I.exp_steer = (float *)ptr[35];
-        I.exp_len = (float *)ptr[36];
         I.lbx = I.lbz = I.ubx = I.ubz = -1;
         I.stop_on_goal = 1;
-        if (!check(cudaMemsetAsync(I.claim, 0x7F, 4 * C, stream_), "claim init"))
+    }
+    if (budget_bytes > 0) {
+        // slots get their storage on admission, sized by the frame
+        budget_ = align_up(budget_bytes, 4096);
+        arena_bytes_ = budget_;
+        if (!check(cudaMalloc(&arena_, arena_bytes_), "arena cudaMalloc"))
             return;
+        free_[0] = budget_;
+    } else {
+        // every slot holds the largest frame, for good
+        const size_t per_slot = slot_bytes(max_w, max_h);
+        arena_bytes_ = per_slot * n_slots;
+        if (!check(cudaMalloc(&arena_, arena_bytes_), "arena cudaMalloc"))
+            return;
+        if (!check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "arena memset"))
+            return;
+        for (int s = 0; s < n_slots; s++) {
+            store_off_[s] = per_slot * s;
+            store_bytes_[s] = per_slot;
+            store_w_[s] = max_w;
+            store_h_[s] = max_h;
+            if (!layout_slot(s, max_w, max_h))
+                return;
+        }
     }
     bool ok = check(cudaMalloc(&d_inst_, sizeof(Inst) * n_slots), "inst table") &&
               check(cudaMalloc(&d_state_, sizeof(State) * n_slots), "state table") &&
@@ -344,6 +467,8 @@ bool Engine::bind_frame(int slot, const Frame *f)
         set_error("frame larger than the engine's slots");
         return false;
     }
+    if (!ensure_storage(slot, f->W, f->H))
+        return false;
     Inst &I = h_inst_[slot];
     set_geometry(I, f->W, f->H);
     I.cls = f->d_cls;  // read in place
@@ -363,6 +488,8 @@ bool Engine::copy_frame(int slot, int W, int H, const uint8_t *cls, const float 
         set_error("frame larger than the engine's slots or bad class table");
         return false;
     }
+    if (!ensure_storage(slot, W, H))
+        return false;
     Inst &I = h_inst_[slot];
     set_geometry(I, W, H);
     I.cls = own_cls_[slot];
@@ -707,6 +834,43 @@ bool Engine::extract_and_validate(const std::vector<int> &slots, int cap, bool c
             check(cudaMemcpyAsync(h_paths_.data(), d_paths_, sizeof(float) * 3 * (size_t)cap_ * n,
                                   cudaMemcpyDeviceToHost, stream_), "paths")) &&
            sync();
+}
+
+bool Engine::check_graph(int slot, int &ok)
+{
+    ok = 0;
+    // the path buffers hold the validity flags and node counts
+    if (!extract_and_validate({}, 64) || !upload_slots_list({slot}))
+        return false;
+    launch_check_graphs(d_inst_, d_slots_, 1, h_inst_[slot].W * h_inst_[slot].H, d_counts_, d_valid_,
+                        stream_);
+    return check(cudaGetLastError(), "graph check launch") &&
+           check(cudaMemcpyAsync(h_small_, d_valid_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                 "graph check") &&
+           sync() && ((ok = h_small_[0]), true);
+}
+
+bool Engine::check_path(int slot, const float *xyh, int m, int &ok)
+{
+    ok = 0;
+    if (m < 0 || (m > 0 && !xyh)) {
+        set_error("path check: bad path");
+        return false;
+    }
+    if (!extract_and_validate({}, std::max(m, 64)) || !upload_slots_list({slot}))
+        return false;
+    h_small_[0] = m;
+    if (!check(cudaMemcpyAsync(d_path_n_, h_small_, sizeof(int), cudaMemcpyHostToDevice, stream_),
+               "path upload") ||
+        (m > 0 && !check(cudaMemcpyAsync(d_paths_, xyh, sizeof(float) * 3 * (size_t)m,
+                                         cudaMemcpyHostToDevice, stream_),
+                         "path upload")))
+        return false;
+    launch_check_paths(d_inst_, d_slots_, 1, d_paths_, d_path_n_, cap_, d_valid_, d_length_, stream_);
+    return check(cudaGetLastError(), "path check launch") &&
+           check(cudaMemcpyAsync(h_small_ + 1, d_valid_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                 "path check") &&
+           sync() && ((ok = h_small_[1]), true);
 }
 
 int Engine::extract_path(int slot, std::vector<float> &xyh)

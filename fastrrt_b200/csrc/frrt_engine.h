@@ -7,6 +7,7 @@
 // Engine with one slot; the batched and served planners use many.
 #pragma once
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -66,7 +67,11 @@ struct Physical {
 
 class Engine {
 public:
-    Engine(int n_slots, int max_w, int max_h, int device = -1);
+    // budget_bytes == 0: every slot holds storage for the largest frame for
+    // the engine's life.  budget_bytes > 0: slots hold no storage until a
+    // frame is bound to them; each then gets storage sized by its frame from
+    // one arena of budget_bytes, and gives it back when released.
+    Engine(int n_slots, int max_w, int max_h, int device = -1, size_t budget_bytes = 0);
     ~Engine();
     bool ok() const { return ok_; }
 
@@ -74,6 +79,20 @@ public:
     int max_cells() const { return max_cells_; }
     cudaStream_t stream() const { return stream_; }
     const Launch &launch() const { return L_; }
+
+    // device memory of one slot's storage (node grid, frame copy, masks,
+    // scratch) for a W x H frame
+    static size_t slot_bytes(int W, int H);
+    // budget mode: storage for a W x H frame in `slot` (kept when it already
+    // holds that layout); false with out_of_budget() when the arena has no
+    // room.  Without a budget: whether the frame fits the preallocated slots.
+    bool ensure_storage(int slot, int W, int H);
+    bool out_of_budget() const { return out_of_budget_; }
+    // budget mode: gives the slot's storage back to the arena
+    void release_storage(int slot);
+    size_t budget() const { return budget_; }
+    size_t used() const { return budget_ ? used_ : arena_bytes_; }
+    size_t peak_used() const { return budget_ ? peak_used_ : arena_bytes_; }
 
     // slot configuration (host side; uploaded by commit())
     void set_physical(int slot, const Physical &p);
@@ -150,6 +169,12 @@ public:
     // made the child) appended at X[offset..], labels[offset..] (device, at
     // most cap rows in all); returns the rows added or -1
     int log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap);
+    // the validator's halves on one slot: checkGraphIsConsistent of its
+    // graph (graph_check_dag_consistency.cpp:33-76), and the per-path checks
+    // of a host path [x, z, heading] * m against its frame, grid and goal;
+    // `ok` gets 1 (passes) or 0
+    bool check_graph(int slot, int &ok);
+    bool check_path(int slot, const float *xyh, int m, int &ok);
     const std::vector<int> &paths_n() const { return h_path_n_; }
     const std::vector<int> &valid() const { return h_valid_; }
     const std::vector<float> &lengths() const { return h_length_; }
@@ -176,6 +201,7 @@ private:
     int *d_log_count_ = nullptr;
     int log_cap_ = 0;
     bool check(cudaError_t e, const char *what);
+    bool layout_slot(int slot, int W, int H);
     bool ensure_graph();
     bool upload_slots_list(const std::vector<int> &slots);
 
@@ -186,6 +212,13 @@ private:
     Launch L_{};
     void *arena_ = nullptr;
     size_t arena_bytes_ = 0;
+    // slot storage: offset and bytes in the arena, the frame size it is laid
+    // out for; budget mode keeps the arena's free ranges (offset -> bytes)
+    size_t budget_ = 0, used_ = 0, peak_used_ = 0;
+    bool out_of_budget_ = false;
+    std::map<size_t, size_t> free_;
+    std::vector<size_t> store_off_, store_bytes_;
+    std::vector<int> store_w_, store_h_;
     std::vector<Inst> h_inst_;
     std::vector<Physical> h_phys_;
     Inst *d_inst_ = nullptr;

@@ -1881,7 +1881,6 @@ __device__ __forceinline__ float wrap_pi(float a)
     return a;
 }
 
-// per-path checks, one thread per slot (the path is short)
 // The validator on one path per warp: lane k checks waypoints k, k + 32, ...
 // (cell in the frame, parent link, no repeated cell, heading change within
 // the curvature bound, footprint feasible outside the ego box); footprints
@@ -2035,6 +2034,26 @@ void launch_validate(const Inst *d_inst, State *d_state, const int *d_slots, int
     k_fill_int<<<(n + 255) / 256, 256, 0, st>>>(d_valid, n, 1);
     launch_count(d_inst, d_slots, n, max_cells, T_NODE, d_counts, st);
     k_dag<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, d_counts, d_valid);
+    k_path_check<<<(n * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_slots, n, d_paths, d_path_n, cap,
+                                                       d_valid, d_length);
+}
+
+void launch_check_graphs(const Inst *d_inst, const int *d_slots, int n, int max_cells, unsigned *d_counts,
+                         int *d_valid, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_fill_int<<<(n + 255) / 256, 256, 0, st>>>(d_valid, n, 1);
+    launch_count(d_inst, d_slots, n, max_cells, T_NODE, d_counts, st);
+    k_dag<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, d_counts, d_valid);
+}
+
+void launch_check_paths(const Inst *d_inst, const int *d_slots, int n, const float *d_paths,
+                        const int *d_path_n, int cap, int *d_valid, float *d_length, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_fill_int<<<(n + 255) / 256, 256, 0, st>>>(d_valid, n, 1);
     k_path_check<<<(n * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_slots, n, d_paths, d_path_n, cap,
                                                        d_valid, d_length);
 }

@@ -103,6 +103,12 @@ void launch_log_paths(const Inst *d_inst, const State *d_state, const int *d_slo
 // count cells of `type` (type < 0: all non-NULL) for listed slots into d_out[k]
 void launch_count(const Inst *d_inst, const int *d_slots, int n, int max_cells, int type,
                   unsigned *d_out, cudaStream_t st);
+// the two halves of launch_validate on their own: the DAG consistency of the
+// listed slots' graphs, and the per-path checks of given paths
+void launch_check_graphs(const Inst *d_inst, const int *d_slots, int n, int max_cells, unsigned *d_counts,
+                         int *d_valid, cudaStream_t st);
+void launch_check_paths(const Inst *d_inst, const int *d_slots, int n, const float *d_paths,
+                        const int *d_path_n, int cap, int *d_valid, float *d_length, cudaStream_t st);
 
 // per-candidate microbenchmarks over one frame slot
 void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, const int32_t *sz,

@@ -164,6 +164,18 @@ class FastRRT:
     def load_graph_state(self, filename):
         _lib.lib().load_graph_state(self._ptr, filename.encode("utf-8"))
 
+    # -- validation (on the device) --------------------------------------------
+    def check_graph_is_consistent(self):
+        """CudaGraph::checkGraphIsConsistent of the planner's graph"""
+        return bool(_lib.check(_lib.lib().fastrrt_check_graph_consistent(self._ptr),
+                               "check_graph_consistent"))
+
+    def validate_path(self, path):
+        """the device path validator on an (n, 3) array of (x, z, heading)"""
+        p = np.ascontiguousarray(np.asarray(path, np.float32).reshape(-1, 3))
+        return bool(_lib.check(_lib.lib().fastrrt_validate_path(self._ptr, p.reshape(-1), len(p)),
+                               "validate_path"))
+
     # -- instrumentation -------------------------------------------------------
     def probe_count(self):
         v = C.c_uint64(0)

@@ -55,6 +55,21 @@ bool path_optimize(void *ptr);
 int *export_graph_nodes(void *ptr);
 /* replaces release_export_graph_nodes (src/python_bind.cpp:109-112) */
 void release_export_graph_nodes(int *ptr);
+/* CudaGraph::checkGraphIsConsistent (src/graph_check_dag_consistency.cpp:33-76)
+ * on the planner's graph, on the device: every node's parent chain ends at a
+ * root within count(NODE) + 4 hops, no node is its own parent, and every
+ * parent is a NODE, COLLISION or CONNECT_TO_GOAL cell.  1 consistent, 0 not,
+ * -1 error.  (The reference exposes it to its unit tests only.) */
+int fastrrt_check_graph_consistent(void *ptr);
+/* The path validator of the batched planner on a given path
+ * [x0, z0, h0, x1, ...] of n waypoints against the planner's frame, graph
+ * and plan data: it starts at the start cell and reaches the goal within
+ * the distance and heading tolerances, every waypoint lies in the frame, is
+ * a graph cell whose parent is the previous waypoint, repeats no cell,
+ * turns within the curvature bound and has a feasible footprint outside the
+ * ego box.  1 valid, 0 not, -1 error.  No counterpart in the reference (its
+ * tests check paths by hand). */
+int fastrrt_validate_path(void *ptr, const float *xyh, int n);
 /* replace get_planned_path / interpolate_planned_path (src/python_bind.cpp:138-150):
  * [n, x0, z0, heading0, ...] */
 float *get_planned_path(void *ptr);
@@ -192,6 +207,21 @@ typedef struct {
 } fastrrt_request;
 
 void *fastrrt_batch_create(int n_slots, int max_width, int max_height);
+/* A batched planner whose slots take device memory by their frame's size:
+ * one arena of budget_bytes (allocated here) from which a slot gets its
+ * storage (node grid, frame copy, masks, scratch: fastrrt_slot_bytes of its
+ * frame) when a request is admitted, and to which it returns the storage when
+ * the slot is released or, in fastrrt_batch_serve, harvested.  Admission
+ * fails with a "budget exhausted" error when the arena has no room;
+ * fastrrt_batch_serve then keeps the request (and those after it) waiting
+ * until finished requests free memory.  No counterpart in the reference
+ * (one CudaGraph of fixed size per planner, src/cuda/graph.cu:249-280). */
+void *fastrrt_batch_create_budget(int max_slots, int max_width, int max_height, uint64_t budget_bytes);
+/* device memory of one slot's storage for a width x height frame */
+uint64_t fastrrt_slot_bytes(int width, int height);
+/* the arena's budget, the bytes slots hold now and the most they held (a
+ * batch created without a budget reports its preallocated arena for all) */
+int fastrrt_batch_memory(void *batch, uint64_t *budget, uint64_t *used, uint64_t *peak);
 void fastrrt_batch_destroy(void *batch);
 /* loads a request into a slot (frame upload, masks, goal precompute, start) */
 int fastrrt_batch_admit(void *batch, int slot, const fastrrt_request *req, int timeout_ms);
@@ -210,7 +240,8 @@ int fastrrt_batch_collect(void *batch, int n, const int32_t *slots, int32_t *val
                           float *length, int32_t *path_n);
 /* copies the last collected path of list entry k: up to cap (x, z, heading) */
 int fastrrt_batch_path(void *batch, int k, float *xyh, int cap);
-/* frees a slot */
+/* deactivates a slot; in a batch with a memory budget its storage returns to
+ * the arena */
 int fastrrt_batch_release(void *batch, int slot);
 /* device time of the last fastrrt_batch_run, milliseconds */
 float fastrrt_batch_last_ms(void *batch);

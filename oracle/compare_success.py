@@ -1,22 +1,33 @@
 """Whole-planner statistics against the reference's own planner (test
-infrastructure; needs oracle/_ref and a GPU): success rate and coarse path
-length of C0 plans over a range of seeds, for the reference's FastRRT
+infrastructure; needs oracle/_ref and a GPU): success rate, path length and
+path cost of C0 plans over a range of seeds, for the reference's FastRRT
 (src/fastrrt.cpp through its C ABI, its clock-seeded curand) and for this
-library's batched planner, both capped at the same number of loop() calls.
+library's drop-in FastRRT (the same seeds through the reference API), both
+capped at the same number of loop() calls and without a timeout.
 
-    python -m oracle.compare_success [--seeds N] [--loops L] [--out file.json]
+Path cost is the accumulated node cost the planner's own graph holds at the
+last waypoint before the goal (the goal-connected cell): the parent's cost
+plus (intrinsic + 1) per cell along the curves (kinematics.cu:184-221,
+graph_direct_goal_connection.cu:16-167), with the base-cost addition of the
+goal connection (fastrrt.cpp:145-167).  It is read from each planner's graph
+dump (CudaGraph::dumpGraph, graph.cu:496-520: the same text format on both
+sides).  The reference runs in several processes on the GPU at once.
+
+    python -m oracle.compare_success [--seeds N] [--loops L] [--workers W] [--out file.json]
 """
 import argparse
 import json
 import math
 import os
 import sys
+import tempfile
 import time
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
+W = H = 256
 
 
 def path_length(p):
@@ -26,55 +37,118 @@ def path_length(p):
     return float(np.sqrt(((p[1:, :2] - p[:-1, :2]) ** 2).sum(1)).sum())
 
 
+def dump_cost(filename, x, z):
+    """the cost column of cell (x, z) in a graph dump"""
+    with open(filename) as f:
+        for k, line in enumerate(f):
+            if k == z * W + x:
+                return float(line.split()[5])
+    return float("nan")
+
+
+def path_cost(planner_dump, path):
+    """accumulated cost at the goal-connected cell (the waypoint before the goal)"""
+    if len(path) < 2:
+        return float("nan")
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "graph.txt")
+        planner_dump(f)
+        return dump_cost(f, int(path[-2][0]), int(path[-2][1]))
+
+
+def run_mine(seeds, loops):
+    import fastrrt_b200 as F
+    from fastrrt_b200 import synth
+    out = []
+    for s in seeds:
+        cls, st, gl = synth.c0_request(s)
+        fr = F.SearchFrame(class_ids=cls, class_costs=synth.CLASS_COSTS)
+        p = F.FastRRT(search_frame=fr, perception_width_m=34.56, perception_height_m=34.56,
+                      max_steering_angle_deg=40, vehicle_length_m=5.4, timeout_ms=-1,
+                      min_dist_x=22, min_dist_z=40, path_costs=synth.CLASS_COSTS, seed=s)
+        p.set_plan_data(fr, st, gl, 2.0)
+        p.search_init()
+        n = 0
+        while not p.goal_reached() and n < loops:
+            n += 1
+            if not p.loop(False):
+                break
+        ok = bool(p.goal_reached())
+        path = p.get_planned_path_array() if ok else np.zeros((0, 3), np.float32)
+        valid = ok and p.validate_path(path)
+        out.append((int(ok and valid), path_length(path) if ok else float("nan"),
+                    path_cost(p.save_current_graph_state, path) if ok else float("nan")))
+    return out
+
+
+def run_reference(seeds, loops):
+    """the reference planner on `seeds` (a worker process)"""
+    from fastrrt_b200 import synth
+    from oracle import oracle as O
+    out = []
+    for s in seeds:
+        cls, st, gl = synth.c0_request(s)
+        rp = O.RefPlanner(cls, synth.CLASS_COSTS, 34.56, 34.56, 40.0, 5.4)
+        rp.set_plan_data(st, gl, 2.0, (22, 40))
+        ok, _ = rp.plan(False, loops)
+        path = rp.path() if ok else np.zeros((0, 3), np.float32)
+        out.append((int(ok), path_length(path) if ok else float("nan"),
+                    path_cost(rp.save_graph, path) if ok else float("nan")))
+        del rp
+    return out
+
+
+def _ref_worker(args):
+    return run_reference(*args)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--seeds", type=int, default=1000)
     ap.add_argument("--loops", type=int, default=50)
     ap.add_argument("--seed0", type=int, default=0)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
-    import fastrrt_b200 as F
-    from fastrrt_b200 import synth
-    from oracle import oracle as O
+    import concurrent.futures as cf
+    import multiprocessing as mp
     seeds = list(range(a.seed0, a.seed0 + a.seeds))
-    # this library, batched
-    B = F.BatchPlanner(256, 256, 256)
-    mine_ok, mine_len = [], []
     t0 = time.time()
-    for b0 in range(0, len(seeds), 256):
-        chunk = seeds[b0:b0 + 256]
-        reqs = [F.make_request(*[synth.c0_request(s)[0], synth.CLASS_COSTS, *synth.c0_request(s)[1:]],
-                               seed=s, max_iterations=a.loops) for s in chunk]
-        v, length, _, _ = B.plan(reqs, max_launches=a.loops + 8, check_every=4)
-        for k in range(len(chunk)):
-            mine_ok.append(int(v[k]))
-            mine_len.append(path_length(B.path(k)) if v[k] else float("nan"))
+    # the reference in spawned processes (started before this process uses the GPU)
+    parts = [seeds[k::a.workers] for k in range(a.workers)]
+    ex = cf.ProcessPoolExecutor(a.workers, mp_context=mp.get_context("spawn"))
+    futs = [ex.submit(_ref_worker, (p, a.loops)) for p in parts]
+    mine = run_mine(seeds, a.loops)
     t_mine = time.time() - t0
-    # the reference's planner
-    ref_ok, ref_len = [], []
-    t0 = time.time()
-    for s in seeds:
-        cls, st, gl = synth.c0_request(s)
-        rp = O.RefPlanner(cls, synth.CLASS_COSTS, 34.56, 34.56, 40.0, 5.4)
-        rp.set_plan_data(st, gl, 2.0, (22, 40))
-        ok, _ = rp.plan(False, a.loops)
-        ref_ok.append(int(ok))
-        ref_len.append(path_length(rp.path()) if ok else float("nan"))
-        del rp
+    ref_parts = [f.result() for f in futs]
+    ex.shutdown()
     t_ref = time.time() - t0
-    mo, ro = np.array(mine_ok), np.array(ref_ok)
-    ml, rl = np.array(mine_len), np.array(ref_len)
+    ref = [None] * len(seeds)
+    for k, part in enumerate(ref_parts):
+        for j, r in enumerate(part):
+            ref[k + j * a.workers] = r
+    mo, ml, mc = (np.array([m[i] for m in mine], np.float64) for i in range(3))
+    ro, rl, rc = (np.array([r[i] for r in ref], np.float64) for i in range(3))
 
     def ci(p, n):
         return 1.96 * math.sqrt(max(p * (1 - p), 1e-12) / n)
 
     both = (mo > 0) & (ro > 0)
-    res = {"seeds": a.seeds, "loop_cap": a.loops,
+    res = {"seeds": [a.seed0, a.seed0 + a.seeds - 1], "loop_cap": a.loops, "timeout": "none",
+           "workload": "C0: seeded 256x256 frames, start (128,128,0), goal (128,0,0), 40 deg, 5.4 m, "
+                       "min_dist 22x40 px, 2 m/s",
            "success_mine": float(mo.mean()), "success_reference": float(ro.mean()),
            "success_ci95": [ci(mo.mean(), len(mo)), ci(ro.mean(), len(ro))],
+           "success_diff_points": 100 * float(mo.mean() - ro.mean()),
            "mean_path_len_mine": float(np.nanmean(ml)), "mean_path_len_reference": float(np.nanmean(rl)),
+           "mean_path_cost_mine": float(np.nanmean(mc)), "mean_path_cost_reference": float(np.nanmean(rc)),
+           "path_cost_rel_diff": float(np.nanmean(mc) / np.nanmean(rc) - 1),
+           "path_len_rel_diff": float(np.nanmean(ml) / np.nanmean(rl) - 1),
+           "both_solved": int(both.sum()),
            "mean_path_len_both_solved": [float(ml[both].mean()), float(rl[both].mean())],
-           "seconds": {"mine": t_mine, "reference": t_ref}}
+           "mean_path_cost_both_solved": [float(mc[both].mean()), float(rc[both].mean())],
+           "mine_validated_by": "the device path validator (fastrrt_validate_path)",
+           "seconds": {"mine": t_mine, "reference_wall": t_ref, "reference_workers": a.workers}}
     print(json.dumps(res))
     if a.out:
         json.dump(res, open(a.out, "w"), indent=1)

@@ -579,7 +579,8 @@ class RefPlanner:
             ("loop", C.c_bool, [C.c_void_p, C.c_bool]),
             ("path_optimize", C.c_bool, [C.c_void_p]),
             ("get_planned_path", C.POINTER(C.c_float), [C.c_void_p]),
-            ("release_planned_path_data", None, [C.POINTER(C.c_float)])]:
+            ("release_planned_path_data", None, [C.POINTER(C.c_float)]),
+            ("save_current_graph_state", None, [C.c_void_p, C.c_char_p])]:
             getattr(L, name).restype = res
             getattr(L, name).argtypes = args
         cls = np.ascontiguousarray(cls, np.uint8)
@@ -615,6 +616,10 @@ class RefPlanner:
             if not self.L.loop(self.p, smart):
                 break
         return bool(self.L.goal_reached(self.p)), it
+
+    def save_graph(self, filename):
+        """the reference's graph dump (CudaGraph::dumpGraph, graph.cu:496-520)"""
+        self.L.save_current_graph_state(self.p, filename.encode("utf-8"))
 
     def path(self):
         ptr = self.L.get_planned_path(self.p)

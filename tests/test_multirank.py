@@ -70,3 +70,23 @@ def test_two_ranks_shard_requests(tmp_path, orc):
             p.set_plan_data((64, 64, 0.0), (64, 0, 0.0), 2.0, (22, 40), seed=s)
             g2, it2 = p.plan(False, 30)
             assert (int(g2), it2, len(p.path())) == (good, it, n)
+
+
+def test_bench_starts_its_own_ranks():
+    """`bench.py --gpus 2` without a torchrun environment starts two ranks
+    itself (torch.distributed.run on 127.0.0.1, gloo without a GPU); the
+    reference arm runs on rank 0 alone and prints one line for both ranks,
+    the other rank exits 0 without work."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--impl",
+                        "reference", "--steps", "1", "--warmup", "0", "--ref-plans", "1"],
+                       capture_output=True, text=True, timeout=600, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
