@@ -42,16 +42,20 @@ EXPORTS = [
     "loop", "path_optimize", "export_graph_nodes", "release_export_graph_nodes",
     "get_planned_path", "interpolate_planned_path", "release_planned_path_data",
     "interpolate_planned_path_p", "ideal_curve", "compute_region_debug_performance",
-    "save_current_graph_state", "load_graph_state", "fastrrt_check_graph_consistent",
+    "save_current_graph_state", "load_graph_state", "fastrrt_apf_repulsion", "fastrrt_apf_attraction",
+    "fastrrt_intrinsic_costs", "fastrrt_check_graph_consistent",
     "fastrrt_validate_path",
     # frames, seeding, errors
     "fastrrt_last_error", "fastrrt_frame_create", "fastrrt_frame_create_f3",
-    "fastrrt_frame_destroy", "fastrrt_set_seed", "fastrrt_probe_count", "fastrrt_loop_count",
+    "fastrrt_frame_destroy", "fastrrt_frame_process_distance_to_goal",
+    "fastrrt_frame_process_safe_zone", "fastrrt_frame_flags", "fastrrt_frame_channels",
+    "fastrrt_set_frame_preprocessing", "fastrrt_set_seed", "fastrrt_probe_count", "fastrrt_loop_count",
     # per-candidate kernels
     "fastrrt_candidates_create", "fastrrt_candidates_destroy", "fastrrt_candidates_kinematic",
     "fastrrt_candidates_kinematic_device", "fastrrt_candidates_hermite",
     "fastrrt_candidates_hermite_device", "fastrrt_candidates_feasible",
-    "fastrrt_candidates_kinematic_noalloc",
+    "fastrrt_candidates_kinematic_noalloc", "fastrrt_debug_set_stage_wait_limit",
+    "fastrrt_debug_stage_timeouts",
     # batched planner
     "fastrrt_batch_create", "fastrrt_batch_create_budget", "fastrrt_slot_bytes",
     "fastrrt_batch_memory", "fastrrt_batch_destroy", "fastrrt_batch_admit",
@@ -59,7 +63,7 @@ EXPORTS = [
     "fastrrt_batch_collect", "fastrrt_batch_path", "fastrrt_batch_release",
     "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
     "fastrrt_batch_kernel_times", "fastrrt_kernel_count", "fastrrt_kernel_name",
-    "fastrrt_batch_probes", "fastrrt_batch_direct_connections", "fastrrt_batch_serve",
+    "fastrrt_batch_probes", "fastrrt_batch_interpolate", "fastrrt_batch_interpolated_path", "fastrrt_batch_direct_connections", "fastrrt_batch_serve",
     # learned expansion proposal
     "fastrrt_mlp_create", "fastrrt_mlp_destroy", "fastrrt_mlp_get_weights",
     "fastrrt_mlp_set_weights", "fastrrt_mlp_forward", "fastrrt_mlp_gradients", "fastrrt_mlp_train",
@@ -104,12 +108,20 @@ def lib():
         "compute_region_debug_performance": (None, [vp]),
         "save_current_graph_state": (None, [vp, C.c_char_p]),
         "load_graph_state": (None, [vp, C.c_char_p]),
+        "fastrrt_apf_repulsion": (C.c_int, [vp, vp, C.c_float, C.c_int]),
+        "fastrrt_apf_attraction": (C.c_int, [vp, vp, C.c_float, C.c_int, C.c_int]),
+        "fastrrt_intrinsic_costs": (C.c_int, [vp, f32p]),
         "fastrrt_check_graph_consistent": (C.c_int, [vp]),
         "fastrrt_validate_path": (C.c_int, [vp, f32p, C.c_int]),
         "fastrrt_last_error": (C.c_char_p, []),
         "fastrrt_frame_create": (vp, [C.c_int, C.c_int, u8p, f32p, C.c_int, vp]),
         "fastrrt_frame_create_f3": (vp, [C.c_int, C.c_int, f32p, f32p, C.c_int]),
         "fastrrt_frame_destroy": (None, [vp]),
+        "fastrrt_frame_process_distance_to_goal": (C.c_int, [vp, C.c_int, C.c_int]),
+        "fastrrt_frame_process_safe_zone": (C.c_int, [vp, C.c_int, C.c_int]),
+        "fastrrt_frame_flags": (C.c_int, [vp, P(C.c_int), P(C.c_int)]),
+        "fastrrt_frame_channels": (C.c_int, [vp, vp, vp]),
+        "fastrrt_set_frame_preprocessing": (C.c_int, [vp, C.c_int]),
         "fastrrt_set_seed": (C.c_int, [vp, C.c_uint64]),
         "fastrrt_probe_count": (C.c_int, [vp, P(C.c_uint64)]),
         "fastrrt_loop_count": (C.c_int, [vp]),
@@ -131,6 +143,8 @@ def lib():
                                                            C.c_int, C.c_int, C.c_double,
                                                            C.c_double, C.c_int, vp, vp, vp, vp,
                                                            C.c_float, vp, vp, vp]),
+        "fastrrt_debug_set_stage_wait_limit": (C.c_int, [C.c_int64]),
+        "fastrrt_debug_stage_timeouts": (C.c_int, [P(C.c_uint64)]),
         "fastrrt_batch_create": (vp, [C.c_int, C.c_int, C.c_int]),
         "fastrrt_batch_create_budget": (vp, [C.c_int, C.c_int, C.c_int, C.c_uint64]),
         "fastrrt_slot_bytes": (C.c_uint64, [C.c_int, C.c_int]),
@@ -153,6 +167,8 @@ def lib():
         "fastrrt_kernel_count": (C.c_int, []),
         "fastrrt_kernel_name": (C.c_char_p, [C.c_int]),
         "fastrrt_batch_probes": (C.c_int, [vp, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+        "fastrrt_batch_interpolate": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+        "fastrrt_batch_interpolated_path": (C.c_int, [vp, C.c_int, f32p, C.c_int]),
         "fastrrt_batch_direct_connections": (C.c_int, [vp, C.c_int, vp, vp, vp]),
         "fastrrt_mlp_create": (vp, [C.c_uint64, C.c_int]),
         "fastrrt_mlp_destroy": (None, [vp]),

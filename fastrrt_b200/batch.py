@@ -135,6 +135,26 @@ class BatchPlanner:
                    "batch_collect")
         return valid, length, path_n
 
+    def interpolate(self, cap=8192):
+        """GPU interpolation of the last collected paths and their curve
+        quality: (length, jerk, tangential discontinuity) arrays"""
+        L = _lib.lib()
+        n = self.n_slots  # the last list has at most this many paths
+        length = np.zeros(n, np.float32)
+        jerk = np.zeros(n, np.float32)
+        disc = np.zeros(n, np.int32)
+        m = _lib.check(L.fastrrt_batch_interpolate(self._h, int(cap), length.ctypes.data, jerk.ctypes.data,
+                                                   disc.ctypes.data), "batch_interpolate")
+        self._interp_cap = cap
+        return length[:m], jerk[:m], disc[:m]
+
+    def interpolated_path(self, k):
+        cap = getattr(self, "_interp_cap", 8192)
+        buf = np.zeros(3 * cap, np.float32)
+        m = _lib.check(_lib.lib().fastrrt_batch_interpolated_path(self._h, k, buf, cap),
+                       "batch_interpolated_path")
+        return buf[:3 * m].reshape(m, 3)
+
     def path(self, k, cap=1024):
         buf = np.zeros(3 * cap, np.float32)
         m = _lib.check(_lib.lib().fastrrt_batch_path(self._h, k, buf, cap), "batch_path")

@@ -103,12 +103,32 @@ struct Batch {
     std::vector<int> admitted;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.0f;
+    // two pinned state snapshots of the serving loop and their events
+    State *snap[2] = {nullptr, nullptr};
+    cudaEvent_t snap_ev[2] = {nullptr, nullptr};
+    bool snapshots()
+    {
+        const size_t b = sizeof(State) * (size_t)eng->n_slots();
+        for (int k = 0; k < 2; k++) {
+            if (!snap[k] && cudaMallocHost(&snap[k], b) != cudaSuccess)
+                return false;
+            if (!snap_ev[k] && cudaEventCreateWithFlags(&snap_ev[k], cudaEventDisableTiming) != cudaSuccess)
+                return false;
+        }
+        return true;
+    }
     ~Batch()
     {
         if (ev0)
             cudaEventDestroy(ev0);
         if (ev1)
             cudaEventDestroy(ev1);
+        for (int k = 0; k < 2; k++) {
+            if (snap[k])
+                cudaFreeHost(snap[k]);
+            if (snap_ev[k])
+                cudaEventDestroy(snap_ev[k]);
+        }
     }
 };
 
@@ -171,6 +191,50 @@ void *fastrrt_frame_create_f3(int width, int height, const float *xyz, const flo
 
 void fastrrt_frame_destroy(void *frame) { delete static_cast<Frame *>(frame); }
 
+int fastrrt_frame_process_distance_to_goal(void *frame, int goal_x, int goal_z)
+{
+    return frame_process_distance_to_goal(static_cast<Frame *>(frame), goal_x, goal_z) ? 0 : -1;
+}
+
+int fastrrt_frame_process_safe_zone(void *frame, int min_dist_x, int min_dist_z)
+{
+    return frame_process_safe_zone(static_cast<Frame *>(frame), min_dist_x, min_dist_z) ? 0 : -1;
+}
+
+int fastrrt_frame_flags(void *frame, int *safe_zone_checked, int *distance_to_goal_processed)
+{
+    const Frame *f = static_cast<const Frame *>(frame);
+    if (!f) {
+        set_error("frame: null");
+        return -1;
+    }
+    if (safe_zone_checked)
+        *safe_zone_checked = f->safe_zone_checked;
+    if (distance_to_goal_processed)
+        *distance_to_goal_processed = f->distance_processed;
+    return 0;
+}
+
+int fastrrt_frame_channels(void *frame, float *distance, int32_t *traversability)
+{
+    const Frame *f = static_cast<const Frame *>(frame);
+    if (!f) {
+        set_error("frame: null");
+        return -1;
+    }
+    const size_t n = (size_t)f->W * f->H;
+    bool ok = true;
+    if (distance)
+        ok = f->d_dist ? cudaMemcpy(distance, f->d_dist, 4 * n, cudaMemcpyDeviceToHost) == cudaSuccess
+                       : (memset(distance, 0, 4 * n), true);
+    if (traversability && ok)
+        ok = f->d_trav ? cudaMemcpy(traversability, f->d_trav, 4 * n, cudaMemcpyDeviceToHost) == cudaSuccess
+                       : (memset(traversability, 0, 4 * n), true);
+    if (!ok)
+        set_error("frame: channel download failed");
+    return ok ? 0 : -1;
+}
+
 // ---------------------------------------------------------------------------
 // planner
 // ---------------------------------------------------------------------------
@@ -216,6 +280,40 @@ void *fastrrt_initialize(int width, int height, float perceptionWidthSize_m,
 }
 
 void fastrrt_destroy(void *ptr) { delete static_cast<Planner *>(ptr); }
+
+int fastrrt_debug_set_stage_wait_limit(int64_t rounds)
+{
+    if (rounds < 0) {
+        set_error("stage wait limit: negative");
+        return -1;
+    }
+    if (!set_stage_wait_limit((long)rounds)) {
+        set_error("stage wait limit: symbol copy failed");
+        return -1;
+    }
+    return 0;
+}
+
+int fastrrt_debug_stage_timeouts(uint64_t *count)
+{
+    unsigned long long c = 0;
+    if (!take_stage_timeouts(c)) {
+        set_error("stage timeouts: symbol copy failed");
+        return -1;
+    }
+    if (count)
+        *count = c;
+    return 0;
+}
+
+int fastrrt_set_frame_preprocessing(void *ptr, int use)
+{
+    Planner *p = as_planner(ptr);
+    if (!p)
+        return -1;
+    p->eng->set_use_frame_preprocessing(0, use != 0);
+    return 0;
+}
 
 int fastrrt_set_seed(void *ptr, uint64_t seed)
 {
@@ -423,6 +521,36 @@ int *export_graph_nodes(void *ptr)
 }
 
 void release_export_graph_nodes(int *ptr) { delete[] ptr; }
+
+int fastrrt_apf_repulsion(void *ptr, void *frame, float kr, int radius)
+{
+    Planner *p = as_planner(ptr);
+    if (!p)
+        return -1;
+    return p->eng->apf_repulsion(0, static_cast<const Frame *>(frame), kr, radius) ? 0 : -1;
+}
+
+int fastrrt_apf_attraction(void *ptr, void *frame, float ka, int goal_x, int goal_z)
+{
+    Planner *p = as_planner(ptr);
+    if (!p)
+        return -1;
+    return p->eng->apf_attraction(0, static_cast<const Frame *>(frame), ka, goal_x, goal_z) ? 0 : -1;
+}
+
+int fastrrt_intrinsic_costs(void *ptr, float *out)
+{
+    Planner *p = as_planner(ptr);
+    if (!p || !out) {
+        set_error("intrinsic costs: bad arguments");
+        return -1;
+    }
+    std::vector<float> v;
+    if (!p->eng->intrinsic_download(0, v))
+        return -1;
+    std::copy(v.begin(), v.end(), out);
+    return (int)v.size();
+}
 
 int fastrrt_check_graph_consistent(void *ptr)
 {
@@ -995,6 +1123,43 @@ int fastrrt_batch_path(void *batch, int k, float *xyh, int cap)
     return m;
 }
 
+int fastrrt_batch_interpolate(void *batch, int cap, float *length, float *jerk, int32_t *tan_disc)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || cap <= 0) {
+        set_error("batch interpolate: bad arguments");
+        return -1;
+    }
+    Engine &e = *b->eng;
+    if (!e.interpolate_last(cap))
+        return -1;
+    const int n = (int)e.interp_n().size();
+    for (int k = 0; k < n; k++) {
+        if (length)
+            length[k] = e.interp_length()[k];
+        if (jerk)
+            jerk[k] = e.interp_jerk()[k];
+        if (tan_disc)
+            tan_disc[k] = e.interp_disc()[k];
+    }
+    return n;
+}
+
+int fastrrt_batch_interpolated_path(void *batch, int k, float *xyh, int cap)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || k < 0 || k >= (int)b->eng->interp_n().size() || !xyh || cap < 0) {
+        set_error("batch interpolated path: bad index");
+        return -1;
+    }
+    const Engine &e = *b->eng;
+    const int m = std::min(e.interp_n()[k], cap);
+    const size_t stride = (size_t)3 * e.interp_cap();
+    for (int i = 0; i < 3 * m; i++)
+        xyh[i] = e.interp_points()[(size_t)k * stride + i];
+    return m;
+}
+
 int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_launches,
                        int check_every, int32_t *valid, float *length, float *latency_ms,
                        float *device_ms)
@@ -1118,6 +1283,20 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
     for (int s = n_slots - 1; s >= 0; s--)
         free_slots.push_back(s);
     std::vector<double> admitted_at(n, 0.0);
+    if (!b->snapshots()) {
+        set_error("batch serve: pinned snapshot allocation failed");
+        return -1;
+    }
+    // One batch of iterations stays in flight: the loop launches the next
+    // batch and a copy of the states after it, then reads the states of the
+    // batch before.  A slot's finish time is on the device clock, so reading
+    // it a batch late changes no latency; a finished slot only takes part in
+    // that extra batch as a no-op.  admit_batch[s]: the first batch whose
+    // snapshot shows the request admitted to slot s.
+    std::vector<long> admit_batch(n_slots, 0);
+    long batch_idx = 0, pend_batch = -1;
+    int cur = 0;
+    bool pending = false;
     int next = 0, finished = 0, in_flight = 0, good = 0;
     while (finished < n) {
         // admit every request that has arrived while a slot is free
@@ -1130,7 +1309,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
             if (!e.ensure_storage(s, reqs[next].width, reqs[next].height)) {
                 if (!e.out_of_budget())
                     return -1;
-                if (in_flight == 0 && list.empty()) {
+                if (in_flight == 0 && list.empty() && !pending) {
                     set_error("batch serve: a request needs more memory than the whole budget");
                     return -1;
                 }
@@ -1141,6 +1320,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                 return -1;
             owner[s] = next;
             admitted_at[next] = now;
+            admit_batch[s] = batch_idx;
             list.push_back(s);
             next++;
         }
@@ -1149,7 +1329,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                 return -1;
             in_flight += (int)list.size();
         }
-        if (in_flight == 0) {
+        if (in_flight == 0 && !pending) {
             if (!arrival_ms || next >= n) {
                 set_error("batch serve: no free slot");
                 return -1;
@@ -1161,43 +1341,61 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                     (long long)std::min(wait * 1000.0, 200.0)));
             continue;
         }
-        for (int k = 0; k < check_every; k++)
-            if (!e.iterate())
+        bool launched = false;
+        long this_batch = -1;
+        if (in_flight > 0) {
+            for (int k = 0; k < check_every; k++)
+                if (!e.iterate())
+                    return -1;
+            if (!e.snapshot_states(b->snap[cur], b->snap_ev[cur]))
                 return -1;
-        if (!e.fetch_states(true))
-            return -1;
-        // harvest finished slots and free them
-        list.clear();
-        for (int s = 0; s < n_slots; s++)
-            if (owner[s] >= 0 && e.state(s).done)
-                list.push_back(s);
-        if (list.empty())
-            continue;
-        if (!e.extract_and_validate(list, 1024, false))
-            return -1;
-        for (size_t k = 0; k < list.size(); k++) {
-            const int s = list[k];
-            const int r = owner[s];
-            const State &S = e.state(s);
-            const int v = e.valid()[k] && S.goal_reached;
-            good += v;
-            const double fin = finish_ms(S.finish_ns);
-            if (valid)
-                valid[r] = v;
-            if (length)
-                length[r] = e.lengths()[k];
-            if (latency_ms)
-                latency_ms[r] = (float)(fin - (arrival_ms ? arrival_ms[r] : 0.0));
-            if (service_ms)
-                service_ms[r] = (float)(fin - admitted_at[r]);
-            if (loops)
-                loops[r] = S.loops;
-            owner[s] = -1;
-            free_slots.push_back(s);
-            e.release_storage(s);  // budget mode: back to the arena
-            in_flight--;
-            finished++;
+            launched = true;
+            this_batch = batch_idx++;
         }
+        if (pending) {
+            // harvest the finished slots of the batch before
+            const int pb = cur ^ 1;
+            if (cudaEventSynchronize(b->snap_ev[pb]) != cudaSuccess) {
+                set_error(std::string("batch serve: ") + cudaGetErrorString(cudaGetLastError()));
+                return -1;
+            }
+            const State *snap = b->snap[pb];
+            list.clear();
+            for (int s = 0; s < n_slots; s++)
+                if (owner[s] >= 0 && admit_batch[s] <= pend_batch && snap[s].done)
+                    list.push_back(s);
+            if (!list.empty()) {
+                if (!e.extract_and_validate(list, 1024, false))
+                    return -1;
+                for (size_t k = 0; k < list.size(); k++) {
+                    const int s = list[k];
+                    const int r = owner[s];
+                    const State &S = snap[s];
+                    const int v = e.valid()[k] && S.goal_reached;
+                    good += v;
+                    const double fin = finish_ms(S.finish_ns);
+                    if (valid)
+                        valid[r] = v;
+                    if (length)
+                        length[r] = e.lengths()[k];
+                    if (latency_ms)
+                        latency_ms[r] = (float)(fin - (arrival_ms ? arrival_ms[r] : 0.0));
+                    if (service_ms)
+                        service_ms[r] = (float)(fin - admitted_at[r]);
+                    if (loops)
+                        loops[r] = S.loops;
+                    owner[s] = -1;
+                    free_slots.push_back(s);
+                    e.release_storage(s);  // budget mode: back to the arena
+                    in_flight--;
+                    finished++;
+                }
+            }
+        }
+        pending = launched;
+        pend_batch = this_batch;
+        if (launched)
+            cur ^= 1;
     }
     cudaEventRecord(b->ev1, e.stream());
     cudaEventSynchronize(b->ev1);

@@ -107,6 +107,13 @@ struct Inst {
     double lr;                 // vehicle length / 2 (m)
     float max_curvature;       // PHYSICAL_MAX_CURVATURE as float
     float gd_max_curvature;    // curvature limit of the goal direct connections
+    // SearchFrame preprocessing used by the goal direct connections: the
+    // frame's distance-to-goal channel (nullptr: computed) and the safe-zone
+    // skip of the traversability bit 0x100 (isDistanceToGoalProcessed,
+    // isSafeZoneChecked; graph_direct_goal_connection.cu:16-36, 124-135)
+    const float *gd_dist;
+    int gd_safe;
+    const float *frame_dist;   // the frame's distance-to-goal channel or nullptr
     int win_chunks;            // 32-cell chunks covering a node's goal-search window
     float velocity, max_path, dist_tol, heading_tol;
     int start_x, start_z;

@@ -345,7 +345,7 @@ struct HermTask {
 
     __device__ void init(const Inst &I, const Foot &f, float max_curv, int x_, int z_,
                          float local_heading, int gx, int gz, float goal_heading, int safe_zone,
-                         float start_cost)
+                         float start_cost, const float *dist_channel = nullptr)
     {
         W = f.W;
         H = f.H;
@@ -358,7 +358,8 @@ struct HermTask {
         const long pos = (long)z * W + x;
         const int dx = goal_x - x;
         const int dz = goal_z - z;
-        distance = sqrtf(dx * dx + dz * dz);
+        // isDistanceToGoalProcessed: the frame's distance channel
+        distance = dist_channel ? dist_channel[pos] : sqrtf(dx * dx + dz * dz);
         numPoints = (int)(distance);
         const float a1 = local_heading - kHalfPi;
         const float a2 = goal_heading - kHalfPi;
@@ -639,12 +640,15 @@ __device__ inline KinResult kin_warp(const Inst &I, const Foot &f, int sx, int s
 // walked in order.  Every argument is the same in all lanes, and so is the
 // result: the reference's return value (the cost, or -1 for no connection;
 // callers treat any negative value as none, as the reference's do).
+// `dist_channel` (isDistanceToGoalProcessed) takes the curve's distance from
+// the frame's distance channel at the start cell instead of computing it.
 __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv, int x, int z,
                                    float local_heading, int gx, int gz, float goal_heading, int safe,
-                                   float start_cost, int coarse, int lane, unsigned long long &probes)
+                                   float start_cost, int coarse, int lane, unsigned long long &probes,
+                                   const float *dist_channel = nullptr)
 {
     HermTask h;
-    h.init(I, f, max_curv, x, z, local_heading, gx, gz, goal_heading, safe, start_cost);
+    h.init(I, f, max_curv, x, z, local_heading, gx, gz, goal_heading, safe, start_cost, dist_channel);
     const int np = h.numPoints;
     const bool skip_foot = safe && (h.trav & 0x100);
     const unsigned lower = (1u << lane) - 1u;
@@ -860,9 +864,11 @@ constexpr long kWaitLimit = 1L << 22;  // try_wait rounds before giving up
 
 // Loads `words` 32-bit words of the two masks into shared memory.  Called by
 // the whole block; returns false (and the caller falls back to the global
-// copies) if the copy did not complete within the wait limit.
+// copies, after draining the copy with a second bounded wait) if the copy did
+// not complete within `limit` rounds.
 __device__ inline bool stage_masks(uint32_t *s_blk, uint32_t *s_clr, const uint32_t *g_blk,
-                                   const uint32_t *g_clr, int words, uint64_t *bar, unsigned &phase)
+                                   const uint32_t *g_clr, int words, uint64_t *bar, unsigned &phase,
+                                   long limit = kWaitLimit)
 {
     __syncthreads();  // every warp finished reading the previous masks
     if (threadIdx.x == 0) {
@@ -873,7 +879,7 @@ __device__ inline bool stage_masks(uint32_t *s_blk, uint32_t *s_clr, const uint3
         bulk_g2s(s_clr, g_clr, bytes, bar);
     }
     bool done = false;
-    for (long k = 0; k < kWaitLimit; k++)
+    for (long k = 0; k < limit; k++)
         if (mbar_try_wait(bar, phase)) {
             done = true;
             break;

@@ -32,6 +32,59 @@ Frame::~Frame()
     cudaFree(d_cls);
     cudaFree(d_costs);
     cudaFree(d_trav);
+    cudaFree(d_dist);
+}
+
+bool frame_process_distance_to_goal(Frame *f, int goal_x, int goal_z)
+{
+    if (!f) {
+        set_error("frame: null");
+        return false;
+    }
+    if (!f->d_dist && cudaMalloc(&f->d_dist, sizeof(float) * (size_t)f->W * f->H) != cudaSuccess) {
+        set_error("frame: distance channel allocation failed");
+        return false;
+    }
+    launch_frame_distance(f->W, f->H, goal_x, goal_z, f->d_dist, 0);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        set_error(std::string("frame: distance to goal: ") + cudaGetErrorString(cudaGetLastError()));
+        return false;
+    }
+    f->distance_processed = true;
+    return true;
+}
+
+bool frame_process_safe_zone(Frame *f, int min_dist_x, int min_dist_z)
+{
+    if (!f || min_dist_x < 0 || min_dist_z < 0) {
+        set_error("frame: bad safe-zone arguments");
+        return false;
+    }
+    const size_t n = (size_t)f->W * f->H;
+    if (!f->d_trav) {
+        if (cudaMalloc(&f->d_trav, sizeof(int32_t) * n) != cudaSuccess ||
+            cudaMemset(f->d_trav, 0, sizeof(int32_t) * n) != cudaSuccess) {
+            set_error("frame: traversability channel allocation failed");
+            return false;
+        }
+    }
+    uint8_t *rows = nullptr;
+    if (cudaMalloc(&rows, n) != cudaSuccess) {
+        set_error("frame: safe-zone scratch allocation failed");
+        return false;
+    }
+    // setSearchParams (graph.cu:306-314): half extents TO_INT((float)min / 2)
+    const int mdx = (int)((float)min_dist_x / 2), mdz = (int)((float)min_dist_z / 2);
+    const int rc = (int)std::floor(std::sqrt((double)mdx * mdx + (double)mdz * mdz)) + 2;
+    launch_frame_safe_zone(f->W, f->H, f->d_cls, f->d_costs, f->n_classes, rc, rows, f->d_trav, 0);
+    const cudaError_t e = cudaDeviceSynchronize();
+    cudaFree(rows);
+    if (e != cudaSuccess) {
+        set_error(std::string("frame: safe zone: ") + cudaGetErrorString(e));
+        return false;
+    }
+    f->safe_zone_checked = true;
+    return true;
 }
 
 Frame *frame_create(int W, int H, const uint8_t *cls, const float *costs, int n_classes,
@@ -94,7 +147,20 @@ Frame *frame_create_f3(int W, int H, const float *xyz, const float *costs, int n
         trav[i] = (int32_t)xyz[3 * i + 2];  // TO_INT(frame.z)
         any_trav = any_trav || trav[i] != 0;
     }
-    return frame_create(W, H, cls.data(), costs, n_classes, any_trav ? trav.data() : nullptr);
+    Frame *f = frame_create(W, H, cls.data(), costs, n_classes, any_trav ? trav.data() : nullptr);
+    if (!f)
+        return nullptr;
+    // the distance channel (frame.y), kept for isDistanceToGoalProcessed
+    std::vector<float> dist((size_t)n);
+    for (long i = 0; i < n; i++)
+        dist[i] = xyz[3 * i + 1];
+    if (cudaMalloc(&f->d_dist, sizeof(float) * (size_t)n) != cudaSuccess ||
+        cudaMemcpy(f->d_dist, dist.data(), sizeof(float) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_error("frame: distance channel upload failed");
+        delete f;
+        return nullptr;
+    }
+    return f;
 }
 
 // ---------------------------------------------------------------------------
@@ -308,6 +374,7 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device, size_t budget_byte
     own_cls_.assign(n_slots, nullptr);
     intrinsic_.assign(n_slots, nullptr);
     ncls_.assign(n_slots, 0);
+    use_preproc_.assign(n_slots, 0);
     store_off_.assign(n_slots, 0);
     store_bytes_.assign(n_slots, 0);
     store_w_.assign(n_slots, 0);
@@ -422,6 +489,12 @@ Engine::~Engine()
         cudaEventDestroy(stage_ev_);
     cudaFree(d_paths_);
     cudaFree(d_path_n_);
+    cudaFree(d_interp_);
+    cudaFree(d_interp_n_);
+    cudaFree(d_qscratch_);
+    cudaFree(d_qlen_);
+    cudaFree(d_qjerk_);
+    cudaFree(d_qdisc_);
     cudaFree(d_keys_);
     cudaFree(d_counts_);
     cudaFree(d_valid_);
@@ -473,6 +546,10 @@ bool Engine::bind_frame(int slot, const Frame *f)
     set_geometry(I, f->W, f->H);
     I.cls = f->d_cls;  // read in place
     I.trav = f->d_trav;
+    const bool pre = use_preproc_[slot] != 0;
+    I.frame_dist = f->d_dist;
+    I.gd_dist = pre && f->distance_processed ? f->d_dist : nullptr;
+    I.gd_safe = pre && f->safe_zone_checked ? 1 : 0;
     ncls_[slot] = f->n_classes;
     I.n_classes = f->n_classes;
     dirty_ = true;
@@ -494,6 +571,9 @@ bool Engine::copy_frame(int slot, int W, int H, const uint8_t *cls, const float 
     set_geometry(I, W, H);
     I.cls = own_cls_[slot];
     I.trav = nullptr;
+    I.frame_dist = nullptr;
+    I.gd_dist = nullptr;
+    I.gd_safe = 0;
     ncls_[slot] = n_classes;
     I.n_classes = n_classes;
     dirty_ = true;
@@ -756,6 +836,13 @@ bool Engine::fetch_states(bool synchronous)
     return !synchronous || sync();
 }
 
+bool Engine::snapshot_states(State *dst, cudaEvent_t done)
+{
+    return check(cudaMemcpyAsync(dst, d_state_, sizeof(State) * n_slots_, cudaMemcpyDeviceToHost, stream_),
+                 "state snapshot") &&
+           check(cudaEventRecord(done, stream_), "state snapshot event");
+}
+
 bool Engine::deactivate(int slot)
 {
     const int zero = 0;
@@ -809,6 +896,7 @@ bool Engine::extract_and_validate(const std::vector<int> &slots, int cap, bool c
     }
     if (n == 0)
         return true;
+    last_list_ = slots;
     int max_cells = 0;
     for (int s : slots)
         max_cells = std::max(max_cells, h_inst_[s].W * h_inst_[s].H);
@@ -833,6 +921,122 @@ bool Engine::extract_and_validate(const std::vector<int> &slots, int cap, bool c
            (!copy_paths ||
             check(cudaMemcpyAsync(h_paths_.data(), d_paths_, sizeof(float) * 3 * (size_t)cap_ * n,
                                   cudaMemcpyDeviceToHost, stream_), "paths")) &&
+           sync();
+}
+
+// the slot's intrinsic-cost array made current (zeroed when the costs were
+// all zero) after the deferred goal connections that read the old costs
+bool Engine::intrinsic_for_update(int slot, const Frame *f)
+{
+    Inst &I = h_inst_[slot];
+    if (!f || I.W == 0 || f->W != I.W || f->H != I.H) {
+        set_error("apf: the frame must have the planner's size (set_plan_data first)");
+        return false;
+    }
+    if (!gd_complete(slot) ||
+        !check(cudaMemsetAsync(I.memo_key, 0xFF, 8 * (size_t)I.W * I.H, stream_), "memo reset"))
+        return false;
+    if (!I.intrinsic) {
+        if (!check(cudaMemsetAsync(intrinsic_[slot], 0, 4 * (size_t)I.W * I.H, stream_), "intrinsic init"))
+            return false;
+        I.intrinsic = intrinsic_[slot];
+        dirty_ = true;
+    }
+    return true;
+}
+
+bool Engine::apf_repulsion(int slot, const Frame *f, float kr, int radius)
+{
+    if (radius < 1) {
+        set_error("apf: radius must be at least 1");
+        return false;
+    }
+    if (!intrinsic_for_update(slot, f))
+        return false;
+    const Inst &I = h_inst_[slot];
+    uint8_t *scratch = nullptr;
+    if (!check(cudaMallocAsync((void **)&scratch, (size_t)I.W * I.H, stream_), "apf scratch"))
+        return false;
+    launch_apf_repulsion(I.W, I.H, f->d_cls, f->d_costs, f->n_classes, I.lbx, I.lbz, I.ubx, I.ubz, kr, radius,
+                         scratch, intrinsic_[slot], stream_);
+    const bool ok = check(cudaGetLastError(), "apf launch");
+    cudaFreeAsync(scratch, stream_);
+    return ok && commit() && sync();
+}
+
+bool Engine::apf_attraction(int slot, const Frame *f, float ka, int goal_x, int goal_z)
+{
+    if (!intrinsic_for_update(slot, f))
+        return false;
+    const Inst &I = h_inst_[slot];
+    launch_apf_attraction(I.W, I.H, f->d_cls, f->d_costs, f->n_classes, ka, goal_x, goal_z, intrinsic_[slot],
+                          stream_);
+    return check(cudaGetLastError(), "apf launch") && commit() && sync();
+}
+
+bool Engine::intrinsic_download(int slot, std::vector<float> &out)
+{
+    const Inst &I = h_inst_[slot];
+    out.assign((size_t)I.W * I.H, 0.0f);
+    if (!I.intrinsic || out.empty())
+        return true;
+    return check(cudaMemcpyAsync(out.data(), I.intrinsic, 4 * out.size(), cudaMemcpyDeviceToHost, stream_),
+                 "intrinsic download") &&
+           sync();
+}
+
+bool Engine::interpolate_last(int out_cap)
+{
+    const int n = (int)last_list_.size();
+    if (n == 0 || !d_paths_) {
+        set_error("interpolate: no extracted paths");
+        return false;
+    }
+    if (out_cap <= 0) {
+        set_error("interpolate: bad capacity");
+        return false;
+    }
+    if (out_cap > interp_cap_) {
+        cudaFree(d_interp_);
+        cudaFree(d_interp_n_);
+        cudaFree(d_qscratch_);
+        cudaFree(d_qlen_);
+        cudaFree(d_qjerk_);
+        cudaFree(d_qdisc_);
+        d_interp_ = d_qlen_ = d_qjerk_ = nullptr;
+        d_interp_n_ = d_qdisc_ = nullptr;
+        d_qscratch_ = nullptr;
+        interp_cap_ = 0;
+        const size_t ns = (size_t)n_slots_;
+        if (!check(cudaMalloc(&d_interp_, sizeof(float) * 3 * (size_t)out_cap * ns), "interpolation buffers") ||
+            !check(cudaMalloc(&d_interp_n_, sizeof(int) * ns), "interpolation counts") ||
+            !check(cudaMalloc(&d_qscratch_, sizeof(double) * 2 * (size_t)out_cap * ns), "quality scratch") ||
+            !check(cudaMalloc(&d_qlen_, sizeof(float) * ns), "quality") ||
+            !check(cudaMalloc(&d_qjerk_, sizeof(float) * ns), "quality") ||
+            !check(cudaMalloc(&d_qdisc_, sizeof(int) * ns), "quality"))
+            return false;
+        interp_cap_ = out_cap;
+    }
+    if (!upload_slots_list(last_list_))
+        return false;
+    launch_interpolate(d_inst_, d_slots_, n, d_paths_, d_path_n_, cap_, d_interp_, d_interp_n_, interp_cap_,
+                       d_qscratch_, d_qlen_, d_qjerk_, d_qdisc_, stream_);
+    h_interp_.resize((size_t)3 * interp_cap_ * n);
+    h_interp_n_.resize(n);
+    h_qlen_.resize(n);
+    h_qjerk_.resize(n);
+    h_qdisc_.resize(n);
+    return check(cudaGetLastError(), "interpolate launch") &&
+           check(cudaMemcpyAsync(h_interp_.data(), d_interp_, sizeof(float) * h_interp_.size(),
+                                 cudaMemcpyDeviceToHost, stream_), "interpolated points") &&
+           check(cudaMemcpyAsync(h_interp_n_.data(), d_interp_n_, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                                 stream_), "interpolated counts") &&
+           check(cudaMemcpyAsync(h_qlen_.data(), d_qlen_, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_),
+                 "quality") &&
+           check(cudaMemcpyAsync(h_qjerk_.data(), d_qjerk_, sizeof(float) * n, cudaMemcpyDeviceToHost, stream_),
+                 "quality") &&
+           check(cudaMemcpyAsync(h_qdisc_.data(), d_qdisc_, sizeof(int) * n, cudaMemcpyDeviceToHost, stream_),
+                 "quality") &&
            sync();
 }
 

@@ -31,9 +31,23 @@ struct Frame {
     float *d_costs = nullptr;
     int n_classes = 0;
     int32_t *d_trav = nullptr;
+    float *d_dist = nullptr;         // distance-to-goal channel or nullptr
+    bool safe_zone_checked = false;  // the SearchFrame's isSafeZoneChecked()
+    bool distance_processed = false; // the SearchFrame's isDistanceToGoalProcessed()
     std::vector<float> h_costs;
     ~Frame();
 };
+
+// SearchFrame preprocessing on the device (the driveless SearchFrame's
+// processDistanceToGoal / processSafeDistanceZone, whose sources are not in
+// the reference tree; semantics from their uses in the reference):
+// the distance channel gets the Euclidean distance of every cell to the goal
+// as checkDirectConnectionToGoal computes it, sqrtf(dx * dx + dz * dz); the
+// safe zone sets traversability bit 0x100 on every cell whose footprint of
+// half extents (min_dist_x / 2, min_dist_z / 2) holds no obstacle at any
+// heading (no obstacle within the Chebyshev radius that bounds every probe).
+bool frame_process_distance_to_goal(Frame *f, int goal_x, int goal_z);
+bool frame_process_safe_zone(Frame *f, int min_dist_x, int min_dist_z);
 
 Frame *frame_create(int W, int H, const uint8_t *cls, const float *costs, int n_classes,
                     const int32_t *trav);
@@ -94,6 +108,11 @@ public:
     size_t used() const { return budget_ ? used_ : arena_bytes_; }
     size_t peak_used() const { return budget_ ? peak_used_ : arena_bytes_; }
 
+    // the goal direct connections of the slot follow its frame's
+    // preprocessing flags (the reference's processDirectGoalConnection passes
+    // false for both, fastrrt.cpp:79 -> graph_direct_goal_connection.cu:222)
+    void set_use_frame_preprocessing(int slot, bool on) { use_preproc_[slot] = on; }
+
     // slot configuration (host side; uploaded by commit())
     void set_physical(int slot, const Physical &p);
     // frame owned by the caller (must outlive its use) or copied into the slot
@@ -128,6 +147,9 @@ public:
     bool sync();
     // copy the small head of the state of every slot to host memory
     bool fetch_states(bool synchronous = true);
+    // the same copy into `dst` (pinned host memory, n_slots states) on the
+    // stream, completion marked by `done`; no host wait
+    bool snapshot_states(State *dst, cudaEvent_t done);
     const State &state(int slot) const { return h_state_[slot]; }
     bool deactivate(int slot);
 
@@ -151,6 +173,12 @@ public:
     bool gd_download(int slot, std::vector<uint8_t> &flag, std::vector<float> &heading,
                      std::vector<float> &cost);
     bool regions_upload(int slot, const std::vector<unsigned> &counts);
+    // artificial potential fields (apf.cu:23-154) of frame f added to the
+    // slot's intrinsic costs (the deferred goal direct connections of the
+    // current plan are evaluated first, with the costs they were set up with)
+    bool apf_repulsion(int slot, const Frame *f, float kr, int radius);
+    bool apf_attraction(int slot, const Frame *f, float ka, int goal_x, int goal_z);
+    bool intrinsic_download(int slot, std::vector<float> &out);
     bool set_state_field_last_expanded(int slot, int v);
     bool clear_goal_flag(int slot);
 
@@ -175,6 +203,16 @@ public:
     // `ok` gets 1 (passes) or 0
     bool check_graph(int slot, int &ok);
     bool check_path(int slot, const float *xyh, int m, int &ok);
+    // interpolation of the paths of the last extract_and_validate list and
+    // their curve-quality metrics, on the device; up to out_cap points per
+    // path; results in interp_* (host copies)
+    bool interpolate_last(int out_cap);
+    const std::vector<float> &interp_points() const { return h_interp_; }
+    const std::vector<int> &interp_n() const { return h_interp_n_; }
+    const std::vector<float> &interp_length() const { return h_qlen_; }
+    const std::vector<float> &interp_jerk() const { return h_qjerk_; }
+    const std::vector<int> &interp_disc() const { return h_qdisc_; }
+    int interp_cap() const { return interp_cap_; }
     const std::vector<int> &paths_n() const { return h_path_n_; }
     const std::vector<int> &valid() const { return h_valid_; }
     const std::vector<float> &lengths() const { return h_length_; }
@@ -202,6 +240,7 @@ private:
     int log_cap_ = 0;
     bool check(cudaError_t e, const char *what);
     bool layout_slot(int slot, int W, int H);
+    bool intrinsic_for_update(int slot, const Frame *f);
     bool ensure_graph();
     bool upload_slots_list(const std::vector<int> &slots);
 
@@ -240,6 +279,7 @@ private:
     std::vector<uint8_t *> own_cls_;  // per slot frame copies
     std::vector<float *> intrinsic_;  // per slot intrinsic-cost arrays
     std::vector<int> ncls_;           // class count of each slot's frame
+    std::vector<char> use_preproc_;   // set_use_frame_preprocessing
     // path extraction / validation scratch
     int cap_ = 0;
     float *d_paths_ = nullptr;
@@ -254,6 +294,13 @@ private:
     long long *d_clock_ = nullptr;    // device clock read-out
     std::vector<int> h_path_n_, h_valid_;
     std::vector<float> h_length_, h_paths_;
+    std::vector<int> last_list_;      // slots of the last extraction
+    int interp_cap_ = 0;
+    float *d_interp_ = nullptr, *d_qlen_ = nullptr, *d_qjerk_ = nullptr;
+    int *d_interp_n_ = nullptr, *d_qdisc_ = nullptr;
+    double *d_qscratch_ = nullptr;
+    std::vector<float> h_interp_, h_qlen_, h_qjerk_;
+    std::vector<int> h_interp_n_, h_qdisc_;
     bool profiling_ = false;
     std::vector<cudaEvent_t> prof_ev_;
     std::vector<double> prof_ms_;

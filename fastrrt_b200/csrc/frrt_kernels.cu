@@ -28,6 +28,7 @@
 // Concurrent claims on one target cell are resolved by atomicMin on the
 // expanding cell index, which makes every iteration deterministic for a
 // given seed.
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 
@@ -53,6 +54,12 @@ __device__ __forceinline__ int find_slot(const int *prefix, int n, int chunk)
 }
 
 __device__ __forceinline__ bool live(const State &S) { return S.active && !S.done; }
+
+// rounds the per-candidate kernels wait for their staged masks before they
+// give up and read the global copies (a test hook lowers it), and how many
+// blocks gave up
+__device__ long g_stage_wait_limit = kWaitLimit;
+__device__ unsigned long long g_stage_timeouts = 0;
 
 // Items a warp of the warp-per-item kernels takes from its work counter at
 // once: one while the items are few next to the grid's warps (every item on
@@ -341,8 +348,8 @@ __device__ void gd_eval_cell(const Inst &I, const Foot &f, int pos, int lane, un
     const int z = pos / I.W;
     const int x = pos - z * I.W;
     const float lh = compute_heading(x, z, I.goal_x, I.goal_z);
-    const float c = curve_warp(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading, 0,
-                               I.gd_cost[pos], kCoarseStride, lane, probes);
+    const float c = curve_warp(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading,
+                               I.gd_safe, I.gd_cost[pos], kCoarseStride, lane, probes, I.gd_dist);
     if (lane == 0) {
         if (c >= 0) {
             I.gd_heading[pos] = lh;
@@ -680,11 +687,16 @@ __global__ void __launch_bounds__(256) k_post(const Inst *insts, State *states, 
         const int cells = I.W * I.H;
         const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
         int nodes = 0;
+        // the last two (region, count) runs of the thread's 16 cells (a run
+        // before those, possible when the cells span a row end, is added
+        // directly)
+        int reg[2] = {-1, -1};
+        unsigned cnt[2] = {0u, 0u};
         if (base < cells) {
             int8_t t[16];
             load16(I.type + base, t);
             const int dw = I.W / kRegion + 1;
-            int reg = -1, rc = 0;
+            int run = -1;
             for (int k = 0; k < 16; k++) {
                 const int pos = base + k;
                 if (pos >= cells)
@@ -693,17 +705,35 @@ __global__ void __launch_bounds__(256) k_post(const Inst *insts, State *states, 
                 if (I.smart && t[k] != T_NULL && t[k] != T_PROCESSING) {
                     const int z = pos / I.W, x = pos - z * I.W;
                     const int r = (z / kRegion) * dw + x / kRegion;
-                    if (r != reg) {
-                        if (rc)
-                            atomicAdd(&I.region_new[reg], (unsigned)rc);
-                        reg = r;
-                        rc = 0;
+                    if (run < 0 || r != reg[run]) {
+                        if (run == 1) {
+                            atomicAdd(&I.region_new[reg[0]], cnt[0]);
+                            reg[0] = reg[1];
+                            cnt[0] = cnt[1];
+                            cnt[1] = 0u;
+                            run = 0;
+                        }
+                        reg[++run] = r;
                     }
-                    rc++;
+                    cnt[run]++;
                 }
             }
-            if (rc)
-                atomicAdd(&I.region_new[reg], (unsigned)rc);
+        }
+        // density of the new nodes by region (graph_expansion_search_zones.cu:
+        // 42-66): the warp's 512 consecutive cells fall in a few regions; the
+        // lanes of each region sum their counts and one adds them
+        if (I.smart) {
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const bool has = cnt[q] > 0;
+                const unsigned act = __ballot_sync(kFull, has);
+                if (has) {
+                    const unsigned m = __match_any_sync(act, reg[q]);
+                    const unsigned sum = __reduce_add_sync(m, cnt[q]);
+                    if ((threadIdx.x & 31) == __ffs(m) - 1)
+                        atomicAdd(&I.region_new[reg[q]], sum);
+                }
+            }
         }
         nodes = warp_sum(nodes);
         if ((threadIdx.x & 31) == 0 && nodes)
@@ -1029,7 +1059,7 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
         const float lh = compute_heading(x, z, I.goal_x, I.goal_z);
         unsigned long long probes = 0;
         const float c = curve_warp(I, f, I.gd_max_curvature, x, z, lh, I.goal_x, I.goal_z, I.goal_heading,
-                                   0, I.gd_cost[pos], kCoarseStride, lane, probes);
+                                   I.gd_safe, I.gd_cost[pos], kCoarseStride, lane, probes, I.gd_dist);
         probes = warp_sum64(probes);
         if (lane == 0) {
             // __CUDA_direct_connection (graph_direct_goal_connection.cu:169-193)
@@ -1410,14 +1440,9 @@ __global__ void __launch_bounds__(256) k_prop_list(const Inst *insts, const Stat
 // softmax of the network's logits (fourth word, inverse CDF) and the value
 // uniformly inside the bin (first two words); otherwise prop_len = -1 and
 // the expansion draws uniformly as without the network.
-__global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const State *states,
-                                                     ProposalBufs pb)
+__device__ void prop_sample_row(const Inst *insts, const State *states, const ProposalBufs &pb, int r,
+                                int lane)
 {
-    const int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    const int rows = min(*pb.count, pb.cap);
-    if (r >= rows)
-        return;
     const int slot = pb.slot_of[r], idx = pb.idx[r], pos = pb.cells[r];
     const Inst &I = insts[slot];
     const State &S = states[slot];
@@ -1483,6 +1508,17 @@ __global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const St
     I.prop_len[idx] = fmaxf(5.0f, lo + (lb + u01(w[1])) * lw);
 }
 
+// rows grid-strided over a machine-sized grid (the row count is on the device)
+__global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const State *states,
+                                                     ProposalBufs pb)
+{
+    const int lane = threadIdx.x & 31;
+    const int rows = min(*pb.count, pb.cap);
+    const int warps = (int)((gridDim.x * (long)blockDim.x) >> 5);
+    for (int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); r < rows; r += warps)
+        prop_sample_row(insts, states, pb, r, lane);
+}
+
 void launch_proposal(const Inst *d_inst, State *d_state, const Sched *d_sched, const ProposalBufs &pb,
                      const Launch &L, cudaStream_t st)
 {
@@ -1490,7 +1526,7 @@ void launch_proposal(const Inst *d_inst, State *d_state, const Sched *d_sched, c
     k_prop_list<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched, pb);
     launch_features(d_inst, pb.cells, pb.slot_of, pb.cap, pb.X, st, pb.count);
     launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, pb.h1, pb.h2, pb.logits, st);
-    k_prop_sample<<<(pb.cap * 32 + 255) / 256, 256, 0, st>>>(d_inst, d_state, pb);
+    k_prop_sample<<<std::min((pb.cap * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st>>>(d_inst, d_state, pb);
 }
 
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
@@ -1973,6 +2009,206 @@ __global__ void __launch_bounds__(128) k_path_check(const Inst *insts, const int
     length[k] = len;
 }
 
+// ---------------------------------------------------------------------------
+// interpolation of extracted paths and curve quality, one warp per path
+// ---------------------------------------------------------------------------
+
+// interpolate (interpolation.cpp:112-135) of the listed paths: for every pair
+// of consecutive waypoints, interpolateHermiteCurve (interpolation.cpp:36-110)
+// with the reference's float arithmetic, each product and sum rounded on its
+// own (the reference is host code: no fused multiply-adds), samples across
+// the lanes; a sample keeps its rounded cell when it lies in the frame and
+// the cell differs from the last kept one (a ballot over the chunk, the last
+// kept cell carried).  Then the curve-quality metrics of the interpolated
+// curve (tests/python_dataset/curve_quality.py:92-99, 179-294, in double as
+// the reference's Python): length, jerk of the windowed direction, and the
+// tangential discontinuity against the path's start heading.
+__global__ void __launch_bounds__(128) k_interp(const Inst *insts, const int *slots, int n,
+                                                const float *paths, const int *path_n, int cap,
+                                                float *out, int *out_n, int out_cap, double *scratch,
+                                                float *length, float *jerk, int *tan_disc)
+{
+    const int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= n)
+        return;  // uniform across the warp
+    const Inst &I = insts[slots[k]];
+    const float *p = paths + (long)k * cap * 3;
+    const int m = path_n[k];
+    float *o = out + (long)k * out_cap * 3;
+    const unsigned lower = (1u << lane) - 1u;
+    int cnt = 0, last_x = -1, last_z = -1;
+    bool full = false;
+    for (int s = 1; s < m && !full; s++) {
+        const int p1x = (int)p[3 * (s - 1)], p1z = (int)p[3 * (s - 1) + 1];
+        const int p2x = (int)p[3 * s], p2z = (int)p[3 * s + 1];
+        const float p1h = p[3 * (s - 1) + 2], p2h = p[3 * s + 2];
+        const double dxd = p2x - p1x, dzd = p2z - p1z;
+        const int numPoints = (int)sqrt(dxd * dxd + dzd * dzd);
+        const float dx = (float)(p2x - p1x), dz = (float)(p2z - p1z);
+        const float d = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)));
+        const float a1 = (float)(p1h - kPi / 2), a2 = (float)(p2h - kPi / 2);
+        const float t1x = __fmul_rn(d, cosf(a1)), t1y = __fmul_rn(d, sinf(a1));
+        const float t2x = __fmul_rn(d, cosf(a2)), t2y = __fmul_rn(d, sinf(a2));
+        const float fx1 = (float)p1x, fz1 = (float)p1z, fx2 = (float)p2x, fz2 = (float)p2z;
+        // x = h00 p1 + h10 tan1 + h01 p2 + h11 tan2, summed left to right
+        auto mix = [](float a, float b, float c, float d4, float u, float v, float w, float q) {
+            return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a, u), __fmul_rn(b, v)), __fmul_rn(c, w)),
+                             __fmul_rn(d4, q));
+        };
+        for (int base = 0; base < numPoints && !full; base += 32) {
+            const int i = base + lane;
+            const float t = __fdiv_rn((float)i, (float)(numPoints - 1));
+            const float t2 = __fmul_rn(t, t), t3 = __fmul_rn(t2, t);
+            const float h00 = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, t3), __fmul_rn(3.0f, t2)), 1.0f);
+            const float h10 = __fadd_rn(__fsub_rn(t3, __fmul_rn(2.0f, t2)), t);
+            const float h01 = __fadd_rn(__fmul_rn(-2.0f, t3), __fmul_rn(3.0f, t2));
+            const float h11 = __fsub_rn(t3, t2);
+            const float x = mix(h00, h10, h01, h11, fx1, t1x, fx2, t2x);
+            const float z = mix(h00, h10, h01, h11, fz1, t1y, fz2, t2y);
+            int cx = 0, cz = 0;
+            bool valid = false;
+            if (i < numPoints && !(x < 0 || x >= I.W) && !(z < 0 || z >= I.H)) {
+                cx = (int)roundf(x);
+                cz = (int)roundf(z);
+                valid = cx >= 0 && cx < I.W && cz >= 0 && cz < I.H;
+            }
+            const unsigned vm = __ballot_sync(kFull, valid);
+            const unsigned below = vm & lower;
+            const int src = below ? 31 - __clz(below) : lane;
+            const int qx = __shfl_sync(kFull, cx, src), qz = __shfl_sync(kFull, cz, src);
+            const bool keep = valid && !(cx == (below ? qx : last_x) && cz == (below ? qz : last_z));
+            const unsigned km = __ballot_sync(kFull, keep);
+            if (keep) {
+                const float t00 = __fsub_rn(__fmul_rn(6.0f, t2), __fmul_rn(6.0f, t));
+                const float t10 = __fadd_rn(__fsub_rn(__fmul_rn(3.0f, t2), __fmul_rn(4.0f, t)), 1.0f);
+                const float t01 = __fadd_rn(__fmul_rn(-6.0f, t2), __fmul_rn(6.0f, t));
+                const float t11 = __fsub_rn(__fmul_rn(3.0f, t2), __fmul_rn(2.0f, t));
+                const float ddx = mix(t00, t10, t01, t11, fx1, t1x, fx2, t2x);
+                const float ddz = mix(t00, t10, t01, t11, fz1, t1y, fz2, t2y);
+                const float heading = (float)(atan2f(ddz, ddx) + kPi / 2);
+                const int at = cnt + __popc(km & lower);
+                if (at < out_cap) {
+                    o[3 * at] = (float)cx;
+                    o[3 * at + 1] = (float)cz;
+                    o[3 * at + 2] = heading;
+                }
+            }
+            if (vm) {
+                const int hi = 31 - __clz(vm);
+                last_x = __shfl_sync(kFull, cx, hi);
+                last_z = __shfl_sync(kFull, cz, hi);
+            }
+            cnt += __popc(km);
+            full = cnt >= out_cap;
+        }
+    }
+    cnt = min(cnt, out_cap);
+    __syncwarp();
+    // curve quality of the cnt interpolated cells
+    double len = 0.0;
+    for (int i = 1 + lane; i < cnt; i += 32) {
+        const double ex = o[3 * i] - o[3 * (i - 1)], ez = o[3 * i + 1] - o[3 * (i - 1) + 1];
+        len += sqrt(ex * ex + ez * ez);
+    }
+    for (int q = 16; q; q >>= 1)
+        len += __shfl_xor_sync(kFull, len, q);
+    // the window of point `pos` (curve_quality.py:191-201), positions below
+    // zero wrap to the curve's end as Python's do; below -cnt they fail
+    auto window = [cnt](int pos, int &i0, int &j0) {
+        int i = pos - 4, j = pos + 4;
+        if (i < 0) {
+            j -= i;
+            i = 0;
+        }
+        if (j >= cnt) {
+            i = i - (j - cnt) - 1;
+            j = cnt - 1;
+        }
+        i0 = i;
+        j0 = j;
+    };
+    double *v = scratch + (long)k * out_cap * 2, *g = v + out_cap;
+    bool ok = cnt >= 3, disc = false;
+    const double thr = 15.0 * kPi / 180.0;
+    const float sh = m > 0 ? p[2] : 0.0f;
+    for (int i = lane; i < cnt && ok; i += 32) {
+        int i0, j0;
+        window(i, i0, j0);
+        if (i0 < -cnt) {
+            ok = false;
+            break;
+        }
+        const double px = o[3 * i], pz = o[3 * i + 1];
+        double dv = 0.0, mh = 0.0;
+        int c = 0;
+        for (int q = i0; q <= j0; q++) {
+            if (q == i)
+                continue;
+            const int r = q < 0 ? q + cnt : q;
+            const double rx = o[3 * r], rz = o[3 * r + 1];
+            // direction (curve_quality.py:243-246), from the earlier point
+            const double ax = q < i ? px - rx : rx - px, az = q < i ? pz - rz : rz - pz;
+            dv += atan2(az, ax);
+            // heading (curve_quality.py:179-189): 0 for a repeated point
+            double hd = 0.0;
+            if (!(ax == 0.0 && az == 0.0)) {
+                hd = kPi / 2 - atan2(-az, ax);
+                if (hd > kPi)
+                    hd -= 2 * kPi;
+            }
+            mh += hd;
+            c++;
+        }
+        v[i] = c ? dv / c : 0.0;
+        g[i] = c ? mh / c : 0.0;
+    }
+    ok = __all_sync(kFull, ok);
+    __syncwarp();
+    // tangential discontinuity (curve_quality.py:227-241): any step of the
+    // windowed heading above 15 degrees, from the start heading on
+    for (int i = 1 + lane; i < cnt && ok; i += 32) {
+        const double before = i == 1 ? (double)sh : g[i - 1];
+        if (fabs(g[i] - before) > thr)
+            disc = true;
+    }
+    disc = __any_sync(kFull, disc);
+    __syncwarp();
+    // jerk (curve_quality.py:290-294): np.gradient twice (one-sided at the
+    // ends), then the sum of magnitudes
+    auto grad = [cnt](const double *f, int i) {
+        if (i == 0)
+            return f[1] - f[0];
+        if (i == cnt - 1)
+            return f[cnt - 1] - f[cnt - 2];
+        return (f[i + 1] - f[i - 1]) / 2.0;
+    };
+    for (int i = lane; i < cnt && ok; i += 32)
+        g[i] = grad(v, i);
+    __syncwarp();
+    double js = 0.0;
+    for (int i = lane; i < cnt && ok; i += 32)
+        js += fabs(grad(g, i));
+    for (int q = 16; q; q >>= 1)
+        js += __shfl_xor_sync(kFull, js, q);
+    if (lane == 0) {
+        out_n[k] = cnt;
+        length[k] = (float)len;
+        jerk[k] = ok ? (float)fabs(js) : __int_as_float(0x7fc00000);
+        tan_disc[k] = ok ? (disc ? 1 : 0) : -1;
+    }
+}
+
+void launch_interpolate(const Inst *d_inst, const int *d_slots, int n, const float *d_paths,
+                        const int *d_path_n, int cap, float *d_out, int *d_out_n, int out_cap,
+                        double *d_scratch, float *d_length, float *d_jerk, int *d_disc, cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_interp<<<(n * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_slots, n, d_paths, d_path_n, cap, d_out,
+                                                   d_out_n, out_cap, d_scratch, d_length, d_jerk, d_disc);
+}
+
 // Training rows of valid paths: one per expansion on the path (waypoints 1 ..
 // m - 3; the last two are the goal connection and the goal): the parent cell,
 // its slot, and the bin of the draw that made the child.  One warp per path.
@@ -2078,13 +2314,19 @@ __global__ void __launch_bounds__(256) k_candidates(const Inst *insts, int slot,
         if (threadIdx.x == 0)
             mbar_init(&bar, 1);
         __syncthreads();
-        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase)) {
+        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase,
+                        g_stage_wait_limit)) {
             blk = smem;
             clr = smem + smem_words;
         } else {
+            // the copy did not land in time: count it, let it finish (its
+            // shared memory must outlive it) and read the global masks
+            if (threadIdx.x == 0)
+                atomicAdd(&g_stage_timeouts, 1ull);
             for (long k = 0; k < kWaitLimit; k++)
                 if (mbar_try_wait(&bar, phase ^ 1u))
                     break;
+            __syncthreads();
         }
     }
     const Foot f = foot_of(I, blk, clr);
@@ -2149,13 +2391,19 @@ __global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, in
         if (threadIdx.x == 0)
             mbar_init(&bar, 1);
         __syncthreads();
-        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase)) {
+        if (stage_masks(smem, smem + smem_words, I.blocked, I.clear, I.mask_words, &bar, phase,
+                        g_stage_wait_limit)) {
             blk = smem;
             clr = smem + smem_words;
         } else {
+            // the copy did not land in time: count it, let it finish (its
+            // shared memory must outlive it) and read the global masks
+            if (threadIdx.x == 0)
+                atomicAdd(&g_stage_timeouts, 1ull);
             for (long k = 0; k < kWaitLimit; k++)
                 if (mbar_try_wait(&bar, phase ^ 1u))
                     break;
+            __syncthreads();
         }
     }
     const Foot f = foot_of(I, blk, clr);
@@ -2169,8 +2417,9 @@ __global__ void __launch_bounds__(256) k_hermite(const Inst *insts, int slot, in
         const int cx = x[i], cz = z[i];
         float r = -1.0f;
         if (cx >= 0 && cx < I.W && cz >= 0 && cz < I.H)
-            r = curve_warp(I, f, maxc, cx, cz, lh[i], gx[i], gz[i], gh[i], safe, I.cost[(long)cz * I.W + cx],
-                           0, lane, probes);
+            r = curve_warp(I, f, maxc, cx, cz, lh[i], gx[i], gz[i], gh[i], safe & 1,
+                           I.cost[(long)cz * I.W + cx], 0, lane, probes,
+                           (safe & 2) ? I.frame_dist : nullptr);
         if (lane == 0)
             out[i] = r;
     }
@@ -2212,10 +2461,187 @@ __global__ void k_feasible(const Inst *insts, int slot, int n, const int32_t *x,
         atomicAdd(probes_out, pr);
 }
 
+// ---------------------------------------------------------------------------
+// SearchFrame preprocessing
+// ---------------------------------------------------------------------------
+
+// distance channel: the distance of every cell to the goal as
+// checkDirectConnectionToGoal computes it (graph_direct_goal_connection.cu:33-35)
+__global__ void k_frame_distance(int W, int H, int gx, int gz, float *dist)
+{
+    const long n = (long)W * H;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < n; pos += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(pos / W), x = (int)(pos - (long)z * W);
+        const int dx = gx - x, dz = gz - z;
+        dist[pos] = sqrtf(dx * dx + dz * dz);
+    }
+}
+
+void launch_frame_distance(int W, int H, int gx, int gz, float *dist, cudaStream_t st)
+{
+    const long n = (long)W * H;
+    k_frame_distance<<<(int)std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(W, H, gx, gz, dist);
+}
+
+// safe zone, pass 1: per cell, an obstacle (class cost < 0) within rc cells
+// of it in its row
+__global__ void k_frame_rows(int W, int H, const uint8_t *cls, const float *costs, int ncls, int rc,
+                             uint8_t *rows)
+{
+    const long n = (long)W * H;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < n; pos += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(pos / W), x = (int)(pos - (long)z * W);
+        uint8_t hit = 0;
+        for (int xx = max(0, x - rc); xx <= min(W - 1, x + rc) && !hit; xx++) {
+            const int c = cls[(long)z * W + xx];
+            hit = (c < ncls && costs[c] < 0) ? 1 : 0;
+        }
+        rows[pos] = hit;
+    }
+}
+
+// pass 2: no row hit within rc rows -> no obstacle within Chebyshev radius
+// rc -> every footprint probe at every heading misses: bit 0x100
+__global__ void k_frame_safe(int W, int H, int rc, const uint8_t *rows, int32_t *trav)
+{
+    const long n = (long)W * H;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < n; pos += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(pos / W), x = (int)(pos - (long)z * W);
+        bool hit = false;
+        for (int zz = max(0, z - rc); zz <= min(H - 1, z + rc) && !hit; zz++)
+            hit = rows[(long)zz * W + x] != 0;
+        trav[pos] = hit ? (trav[pos] & ~0x100) : (trav[pos] | 0x100);
+    }
+}
+
+void launch_frame_safe_zone(int W, int H, const uint8_t *cls, const float *costs, int ncls, int rc,
+                            uint8_t *rows, int32_t *trav, cudaStream_t st)
+{
+    const long n = (long)W * H;
+    const int grid = (int)std::min<long>((n + 255) / 256, 148 * 16);
+    k_frame_rows<<<grid, 256, 0, st>>>(W, H, cls, costs, ncls, rc, rows);
+    k_frame_safe<<<grid, 256, 0, st>>>(W, H, rc, rows, trav);
+}
+
+// ---------------------------------------------------------------------------
+// artificial potential field intrinsic costs (apf.cu:23-154)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ bool apf_obstacle(const uint8_t *cls, const float *costs, int ncls, int W, int H,
+                                             int x, int z)
+{
+    if (x < 0 || x >= W || z < 0 || z >= H)
+        return true;  // check_is_obstacle (apf.cu:17-21): outside is an obstacle
+    const int c = cls[(long)z * W + x];
+    return c < ncls && costs[c] < 0;
+}
+
+__device__ __forceinline__ bool apf_ego(int x, int z, int lbx, int lbz, int ubx, int ubz)
+{
+    return x >= lbx && x <= ubx && z >= ubz && z <= lbz;
+}
+
+// sources of the repulsive field: obstacle cells outside the ego box with a
+// free 4-neighbour (apf.cu:37-57)
+__global__ void k_apf_sources(int W, int H, const uint8_t *cls, const float *costs, int ncls, int lbx, int lbz,
+                              int ubx, int ubz, uint8_t *src)
+{
+    const long n = (long)W * H;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < n; pos += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(pos / W), x = (int)(pos - (long)z * W);
+        bool s = false;
+        if (!apf_ego(x, z, lbx, lbz, ubx, ubz) && apf_obstacle(cls, costs, ncls, W, H, x, z))
+            s = !(apf_obstacle(cls, costs, ncls, W, H, x - 1, z) && apf_obstacle(cls, costs, ncls, W, H, x + 1, z) &&
+                  apf_obstacle(cls, costs, ncls, W, H, x, z - 1) && apf_obstacle(cls, costs, ncls, W, H, x, z + 1));
+        src[pos] = s ? 1 : 0;
+    }
+}
+
+// __CUDA_KERNEL_repulsive_force (apf.cu:23-91) as a gather, one cell per
+// thread: an obstacle cell outside the ego box is set to 100 Kr/2 (apf.cu:49),
+// then every cell outside the ego box adds Kr/2 (1/p - 1/r)^2 for each source
+// within distance r (p = the distance, not the cell itself; apf.cu:59-89), one
+// source after another in the sources' row-major order, each product and sum
+// rounded on its own.  The reference scatters these adds with float atomics
+// and its obstacle sets race with them; this order is one it can produce.
+__global__ void k_apf_repulse(int W, int H, const uint8_t *cls, const float *costs, int ncls, int lbx, int lbz,
+                              int ubx, int ubz, const uint8_t *src, float kr_half, int radius, float *intr)
+{
+    const long n = (long)W * H;
+    const float p0 = (float)radius;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < n; pos += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(pos / W), x = (int)(pos - (long)z * W);
+        if (apf_ego(x, z, lbx, lbz, ubx, ubz))
+            continue;
+        float v = apf_obstacle(cls, costs, ncls, W, H, x, z) ? __fmul_rn(100.0f, kr_half) : intr[pos];
+        for (int sz = z - radius; sz <= z + radius; sz++) {
+            if (sz < 0 || sz >= H)
+                continue;
+            for (int sx = x - radius; sx <= x + radius; sx++) {
+                if (sx < 0 || sx >= W || (sx == x && sz == z) || !src[(long)sz * W + sx])
+                    continue;
+                const float p = __fsqrt_rn((float)((x - sx) * (x - sx) + (z - sz) * (z - sz)));
+                if (p > p0)
+                    continue;
+                const float f = __fsub_rn(__fdiv_rn(1.0f, p), __fdiv_rn(1.0f, p0));
+                v = __fadd_rn(v, __fmul_rn(__fmul_rn(kr_half, f), f));
+            }
+        }
+        intr[pos] = v;
+    }
+}
+
+// __CUDA_KERNEL_attractive_force (apf.cu:93-121): every free cell loses
+// Ka/2 times its squared distance to the goal
+__global__ void k_apf_attract(int W, int H, const uint8_t *cls, const float *costs, int ncls, float ka_half,
+                              int gx, int gz, float *intr)
+{
+    const long n = (long)W * H;
+    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < n; pos += (long)gridDim.x * blockDim.x) {
+        const int z = (int)(pos / W), x = (int)(pos - (long)z * W);
+        const int c = cls[pos];
+        if (c < ncls && costs[c] < 0)
+            continue;  // obstacle
+        const int dx = gx - x, dz = gz - z;
+        const float dcost = (float)(dx * dx + dz * dz) * ka_half;
+        const float current_cost = intr[pos];
+        intr[pos] = current_cost - dcost;
+    }
+}
+
+void launch_apf_repulsion(int W, int H, const uint8_t *cls, const float *costs, int ncls, int lbx, int lbz, int ubx,
+                          int ubz, float kr, int radius, uint8_t *scratch, float *intr, cudaStream_t st)
+{
+    const long n = (long)W * H;
+    const int grid = (int)std::min<long>((n + 255) / 256, 148 * 16);
+    k_apf_sources<<<grid, 256, 0, st>>>(W, H, cls, costs, ncls, lbx, lbz, ubx, ubz, scratch);
+    k_apf_repulse<<<grid, 256, 0, st>>>(W, H, cls, costs, ncls, lbx, lbz, ubx, ubz, scratch, kr * 0.5f, radius, intr);
+}
+
+void launch_apf_attraction(int W, int H, const uint8_t *cls, const float *costs, int ncls, float ka, int gx, int gz,
+                           float *intr, cudaStream_t st)
+{
+    const long n = (long)W * H;
+    k_apf_attract<<<(int)std::min<long>((n + 255) / 256, 148 * 16), 256, 0, st>>>(W, H, cls, costs, ncls, ka * 0.5f,
+                                                                                gx, gz, intr);
+}
+
 // the device clock that the state timestamps use (%globaltimer, ns)
 __global__ void k_clock(long long *out) { *out = global_ns(); }
 
 void launch_clock(long long *d_out, cudaStream_t st) { k_clock<<<1, 1, 0, st>>>(d_out); }
+
+bool set_stage_wait_limit(long rounds)
+{
+    return cudaMemcpyToSymbol(g_stage_wait_limit, &rounds, sizeof(long)) == cudaSuccess;
+}
+
+bool take_stage_timeouts(unsigned long long &count)
+{
+    const unsigned long long zero = 0;
+    return cudaMemcpyFromSymbol(&count, g_stage_timeouts, sizeof(count)) == cudaSuccess &&
+           cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof(zero)) == cudaSuccess;
+}
 
 void configure_kernels(int smem_bytes)
 {

@@ -94,6 +94,15 @@ void launch_optimize(const Inst *d_inst, int slot, int cells, float *d_path, int
 void launch_validate(const Inst *d_inst, State *d_state, const int *d_slots, int n, int max_cells,
                      const float *d_paths, const int *d_path_n, int cap, unsigned *d_counts,
                      int *d_valid, float *d_length, cudaStream_t st);
+// interpolation of extracted paths (interpolation.cpp:36-135) and the
+// curve-quality metrics of the interpolated curves (the reference's
+// tests/python_dataset/curve_quality.py): out_cap points of (x, z, heading)
+// per path, their count, length, jerk (NaN where undefined) and tangential
+// discontinuity (1, 0, or -1 where undefined); scratch holds 2 * out_cap
+// doubles per path
+void launch_interpolate(const Inst *d_inst, const int *d_slots, int n, const float *d_paths,
+                        const int *d_path_n, int cap, float *d_out, int *d_out_n, int out_cap,
+                        double *d_scratch, float *d_length, float *d_jerk, int *d_disc, cudaStream_t st);
 // training rows (parent cell, slot, label) of the valid paths of the last
 // extraction, appended through *count (at most cap_rows)
 void launch_log_paths(const Inst *d_inst, const State *d_state, const int *d_slots, int n,
@@ -109,6 +118,26 @@ void launch_check_graphs(const Inst *d_inst, const int *d_slots, int n, int max_
                          int *d_valid, cudaStream_t st);
 void launch_check_paths(const Inst *d_inst, const int *d_slots, int n, const float *d_paths,
                         const int *d_path_n, int cap, int *d_valid, float *d_length, cudaStream_t st);
+
+// SearchFrame preprocessing: the distance-to-goal channel and the safe-zone
+// bit (0x100) of the traversability channel
+void launch_frame_distance(int W, int H, int gx, int gz, float *dist, cudaStream_t st);
+void launch_frame_safe_zone(int W, int H, const uint8_t *cls, const float *costs, int ncls, int rc,
+                            uint8_t *rows, int32_t *trav, cudaStream_t st);
+
+// the bounded wait of the per-candidate kernels for their staged masks: its
+// limit in rounds (a test hook; the default is kWaitLimit) and the number of
+// blocks that gave up since the last call (reset by the read)
+bool set_stage_wait_limit(long rounds);
+bool take_stage_timeouts(unsigned long long &count);
+
+// artificial potential field intrinsic costs (apf.cu:23-154): the repulsive
+// field of the frame's obstacles within `radius` cells (scratch: W*H bytes)
+// and the attractive field of the goal, added to intr (W*H floats)
+void launch_apf_repulsion(int W, int H, const uint8_t *cls, const float *costs, int ncls, int lbx, int lbz, int ubx,
+                          int ubz, float kr, int radius, uint8_t *scratch, float *intr, cudaStream_t st);
+void launch_apf_attraction(int W, int H, const uint8_t *cls, const float *costs, int ncls, float ka, int gx, int gz,
+                           float *intr, cudaStream_t st);
 
 // per-candidate microbenchmarks over one frame slot
 void launch_candidates(const Inst *d_inst, int slot, int n, const int32_t *sx, const int32_t *sz,

@@ -3,6 +3,7 @@
 #include "frrt_mlp.cuh"
 #include "frrt_device.cuh"
 
+#include <algorithm>
 #include <cmath>
 
 namespace frrt {
@@ -36,12 +37,13 @@ __global__ void __launch_bounds__(128) k_gemm(GemmArgs g)
         const int cnt = *g.dM;
         g.M = cnt < g.M ? cnt : g.M;
     }
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    if (m0 >= g.M)
-        return;  // uniform across the block
+    const int n0 = blockIdx.x * kBN;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     const int gq = lane >> 2, tq = lane & 3;
+    // row tiles grid-strided: the grid is sized for the machine, the rows (a
+    // device-side count in the planner) may be few (uniform across the block)
+    for (int m0 = blockIdx.y * kBM; m0 < g.M; m0 += gridDim.y * kBM) {
     float acc[2][4][4];
 #pragma unroll
     for (int i = 0; i < 2; i++)
@@ -130,6 +132,7 @@ __global__ void __launch_bounds__(128) k_gemm(GemmArgs g)
                 else
                     g.cb[(long)m * g.ldc + n] = __float2bfloat16(v);
             }
+    }
 }
 
 // one warp per row of 128 logits
@@ -221,46 +224,47 @@ __global__ void k_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, con
 __global__ void k_features(const Inst *insts, const int32_t *cells, const int32_t *slot_of, int n,
                            __nv_bfloat16 *X, const int *d_count)
 {
-    const int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (d_count && *d_count < n)
         n = *d_count;
-    if (k >= n)
-        return;
-    const Inst &I = insts[slot_of[k]];
-    const int pos = cells[k];
-    const int z = pos / I.W, x = pos - z * I.W;
-    const float h = I.heading[pos];
-    float sh, ch;
-    sincosf(h, &sh, &ch);
-    // pixel offsets: forward (sin h, -cos h), right (cos h, sin h)
-    __nv_bfloat16 *row = X + (long)k * kMlpInPad;
-    const int half = kMlpPatch / 2;
-    for (int s = lane; s < kMlpPatch * kMlpPatch; s += 32) {
-        const int iu = s / kMlpPatch, iv = s % kMlpPatch;
-        const float u = (float)((half - 1 - iu) * kMlpPatchStride);  // forward, row 0 ahead
-        const float v = (float)((iv - half) * kMlpPatchStride);      // right
-        const int px = (int)floorf(x + u * sh + v * ch + 0.5f);
-        const int pz = (int)floorf(z - u * ch + v * sh + 0.5f);
-        float val = 0.5f;  // outside the frame
-        if (px >= 0 && px < I.W && pz >= 0 && pz < I.H)
-            val = bit_xz(I.blocked, I.mask_rw, px, pz) ? 1.0f : 0.0f;
-        row[s] = __float2bfloat16(val);
-    }
-    if (lane < kMlpInPad - kMlpPatch * kMlpPatch) {
-        const float dx = (float)(I.goal_x - x), dz = (float)(I.goal_z - z);
-        const float scale = 1.0f / (float)max(I.W, I.H);
-        float val = 0.0f;
-        switch (lane) {
-        case 0: val = (dx * sh - dz * ch) * scale; break;  // goal ahead
-        case 1: val = (dx * ch + dz * sh) * scale; break;  // goal to the right
-        case 2: val = sqrtf(dx * dx + dz * dz) * scale; break;
-        case 3: val = sh; break;
-        case 4: val = ch; break;
-        case 5: val = (float)I.max_steer; break;
-        default: val = 0.0f;
+    // rows grid-strided over a machine-sized grid (the count is on the device)
+    const int warps = (int)((gridDim.x * (long)blockDim.x) >> 5);
+    for (int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); k < n; k += warps) {
+        const Inst &I = insts[slot_of[k]];
+        const int pos = cells[k];
+        const int z = pos / I.W, x = pos - z * I.W;
+        const float h = I.heading[pos];
+        float sh, ch;
+        sincosf(h, &sh, &ch);
+        // pixel offsets: forward (sin h, -cos h), right (cos h, sin h)
+        __nv_bfloat16 *row = X + (long)k * kMlpInPad;
+        const int half = kMlpPatch / 2;
+        for (int s = lane; s < kMlpPatch * kMlpPatch; s += 32) {
+            const int iu = s / kMlpPatch, iv = s % kMlpPatch;
+            const float u = (float)((half - 1 - iu) * kMlpPatchStride);  // forward, row 0 ahead
+            const float v = (float)((iv - half) * kMlpPatchStride);      // right
+            const int px = (int)floorf(x + u * sh + v * ch + 0.5f);
+            const int pz = (int)floorf(z - u * ch + v * sh + 0.5f);
+            float val = 0.5f;  // outside the frame
+            if (px >= 0 && px < I.W && pz >= 0 && pz < I.H)
+                val = bit_xz(I.blocked, I.mask_rw, px, pz) ? 1.0f : 0.0f;
+            row[s] = __float2bfloat16(val);
         }
-        row[kMlpPatch * kMlpPatch + lane] = __float2bfloat16(val);
+        if (lane < kMlpInPad - kMlpPatch * kMlpPatch) {
+            const float dx = (float)(I.goal_x - x), dz = (float)(I.goal_z - z);
+            const float scale = 1.0f / (float)max(I.W, I.H);
+            float val = 0.0f;
+            switch (lane) {
+            case 0: val = (dx * sh - dz * ch) * scale; break;  // goal ahead
+            case 1: val = (dx * ch + dz * sh) * scale; break;  // goal to the right
+            case 2: val = sqrtf(dx * dx + dz * dz) * scale; break;
+            case 3: val = sh; break;
+            case 4: val = ch; break;
+            case 5: val = (float)I.max_steer; break;
+            default: val = 0.0f;
+            }
+            row[kMlpPatch * kMlpPatch + lane] = __float2bfloat16(val);
+        }
     }
 }
 
@@ -270,8 +274,10 @@ void launch_gemm(const GemmArgs &g, cudaStream_t st)
 {
     if (g.M <= 0 || g.N <= 0)
         return;
-    const dim3 grid((g.N + kBN - 1) / kBN, (g.M + kBM - 1) / kBM);
-    k_gemm<<<grid, 128, 0, st>>>(g);
+    // at most kMlpGridBlocks blocks (the row tiles loop beyond that)
+    const int nx = (g.N + kBN - 1) / kBN;
+    const int ny = std::min((g.M + kBM - 1) / kBM, std::max(1, kMlpGridBlocks / nx));
+    k_gemm<<<dim3(nx, ny), 128, 0, st>>>(g);
 }
 
 void launch_softmax_xent(const float *logits, const int32_t *labels, int M, float scale,
@@ -311,7 +317,8 @@ void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *sl
 {
     if (n <= 0)
         return;
-    k_features<<<(n * 32 + 255) / 256, 256, 0, st>>>(d_inst, cells, slot_of, n, X, d_count);
+    k_features<<<std::min((n * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st>>>(d_inst, cells, slot_of, n, X,
+                                                                                 d_count);
 }
 
 void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,

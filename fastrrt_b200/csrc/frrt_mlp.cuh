@@ -20,6 +20,12 @@ constexpr int kMlpHidden = 256;
 constexpr int kSteerBins = 16;
 constexpr int kLenBins = 8;
 constexpr int kMlpOut = kSteerBins * kLenBins;    // 128
+// blocks of the planner-side network kernels, whose row count is a device
+// value below the row capacity (a build-time knob for measurement)
+#ifndef FRRT_MLP_GRID_BLOCKS
+#define FRRT_MLP_GRID_BLOCKS 1184
+#endif
+constexpr int kMlpGridBlocks = FRRT_MLP_GRID_BLOCKS;
 
 // Weights of the three layers: W[l] is out x in (row-major, bf16), b[l] f32.
 struct MlpWeights {

@@ -100,6 +100,40 @@ class SearchFrame:
             raise _lib.FastRRTError("SearchFrame has no data")
         return self._handle
 
+    # -- preprocessing (the driveless SearchFrame's, on the device) -------------
+    def process_distance_to_goal(self, goal_x, goal_z):
+        """fills the distance channel with every cell's distance to the goal"""
+        _lib.check(_lib.lib().fastrrt_frame_process_distance_to_goal(self.get_cuda_ptr(), int(goal_x),
+                                                                     int(goal_z)),
+                   "process_distance_to_goal")
+
+    def process_safe_distance_zone(self, min_dist):
+        """sets traversability bit 0x100 where the (min_dist_x, min_dist_z)
+        footprint holds no obstacle at any heading"""
+        _lib.check(_lib.lib().fastrrt_frame_process_safe_zone(self.get_cuda_ptr(), int(min_dist[0]),
+                                                              int(min_dist[1])),
+                   "process_safe_distance_zone")
+
+    def _flags(self):
+        a, b = _lib.C.c_int(), _lib.C.c_int()
+        _lib.check(_lib.lib().fastrrt_frame_flags(self.get_cuda_ptr(), _lib.C.byref(a), _lib.C.byref(b)),
+                   "frame_flags")
+        return bool(a.value), bool(b.value)
+
+    def is_safe_zone_checked(self):
+        return self._flags()[0]
+
+    def is_distance_to_goal_processed(self):
+        return self._flags()[1]
+
+    def channels(self):
+        """(distance, traversability) host copies, H x W each"""
+        d = np.zeros((self.height, self.width), np.float32)
+        t = np.zeros((self.height, self.width), np.int32)
+        _lib.check(_lib.lib().fastrrt_frame_channels(self.get_cuda_ptr(), d.ctypes.data, t.ctypes.data),
+                   "frame_channels")
+        return d, t
+
     def _release(self):
         if self._handle is not None and _lib._lib is not None:
             _lib.lib().fastrrt_frame_destroy(self._handle)

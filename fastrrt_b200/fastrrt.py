@@ -66,6 +66,12 @@ class FastRRT:
             self._ptr = None
 
     # -- planner API (fastrrt.py:172-290) --------------------------------------
+    def set_frame_preprocessing(self, use=True):
+        """the goal direct connections follow the frame's preprocessing flags
+        (distance channel, safe zone) from the next set_plan_data on"""
+        _lib.check(_lib.lib().fastrrt_set_frame_preprocessing(self._ptr, int(bool(use))),
+                   "set_frame_preprocessing")
+
     def set_seed(self, seed):
         _lib.check(_lib.lib().fastrrt_set_seed(self._ptr, int(seed)), "set_seed")
 
@@ -163,6 +169,23 @@ class FastRRT:
 
     def load_graph_state(self, filename):
         _lib.lib().load_graph_state(self._ptr, filename.encode("utf-8"))
+
+    # -- artificial potential fields (on the device) ---------------------------
+    def compute_apf_repulsion(self, search_frame, kr, radius):
+        """the repulsive field of the frame's obstacles added to the intrinsic costs"""
+        _lib.check(_lib.lib().fastrrt_apf_repulsion(self._ptr, search_frame.get_cuda_ptr(), float(kr),
+                                                    int(radius)), "apf_repulsion")
+
+    def compute_apf_attraction(self, search_frame, ka, goal_x, goal_z):
+        """the goal's attractive field added to the intrinsic costs"""
+        _lib.check(_lib.lib().fastrrt_apf_attraction(self._ptr, search_frame.get_cuda_ptr(), float(ka),
+                                                     int(goal_x), int(goal_z)), "apf_attraction")
+
+    def get_intrinsic_costs(self):
+        w, h = self._ego.search_frame_dimensions
+        out = np.zeros(w * h, np.float32)
+        _lib.check(_lib.lib().fastrrt_intrinsic_costs(self._ptr, out), "intrinsic_costs")
+        return out.reshape(h, w)
 
     # -- validation (on the device) --------------------------------------------
     def check_graph_is_consistent(self):

@@ -45,6 +45,13 @@ void set_plan_data(void *ptr, void *frame, int start_x, int start_z, float start
                    float distToGoalTolerance, float headingErrorTolerance_rad);
 /* replaces goal_reached (src/python_bind.cpp:66-70) */
 bool goal_reached(void *ptr);
+/* The planner's goal direct connections (processDirectGoalConnection) follow
+ * the frame's preprocessing flags from the next set_plan_data on: the
+ * distance channel when isDistanceToGoalProcessed, the safe-zone skip when
+ * isSafeZoneChecked.  Off by default, as the reference's FastRRT passes false
+ * for both (fastrrt.cpp:79 -> graph_direct_goal_connection.cu:222, the
+ * frame's flags commented out there).  0 or -1. */
+int fastrrt_set_frame_preprocessing(void *ptr, int use);
 /* replaces search_init (src/python_bind.cpp:72-76) */
 void search_init(void *ptr, bool copyIntrinsicCostsFromFrame);
 /* replaces loop (src/python_bind.cpp:77-81) */
@@ -55,6 +62,23 @@ bool path_optimize(void *ptr);
 int *export_graph_nodes(void *ptr);
 /* replaces release_export_graph_nodes (src/python_bind.cpp:109-112) */
 void release_export_graph_nodes(int *ptr);
+/* replace compute_apf_repulsion / compute_apf_attraction
+ * (src/python_cuda_graph_bind.cpp:41-54 -> CudaGraph::computeRepulsiveFieldAPF /
+ * computeAttractiveFieldAPF, src/cuda/apf.cu:123-154) on the planner's
+ * intrinsic costs, for the planner's frame size (set_plan_data first).
+ * Repulsion: every obstacle cell outside the ego box is set to 100 kr / 2,
+ * then every cell outside it adds kr / 2 (1/p - 1/radius)^2 for each obstacle
+ * with a free 4-neighbour at distance p <= radius, in the obstacles' row-major
+ * order (the reference adds them with float atomics in an arbitrary order, its
+ * sets racing with them).  Attraction: every free cell loses ka / 2 times its
+ * squared distance to the goal.  The plan's remaining deferred goal direct
+ * connections are evaluated first with the costs they were set up with.
+ * 0 or -1. */
+int fastrrt_apf_repulsion(void *ptr, void *frame, float kr, int radius);
+int fastrrt_apf_attraction(void *ptr, void *frame, float ka, int goal_x, int goal_z);
+/* replaces get_intrinsic_costs (src/python_cuda_graph_bind.cpp:56-72): the
+ * width*height intrinsic costs into out; returns the count or -1 */
+int fastrrt_intrinsic_costs(void *ptr, float *out);
 /* CudaGraph::checkGraphIsConsistent (src/graph_check_dag_consistency.cpp:33-76)
  * on the planner's graph, on the device: every node's parent chain ends at a
  * root within count(NODE) + 4 hops, no node is its own parent, and every
@@ -99,6 +123,22 @@ void *fastrrt_frame_create(int width, int height, const uint8_t *class_ids,
 void *fastrrt_frame_create_f3(int width, int height, const float *xyz, const float *class_costs,
                               int n_classes);
 void fastrrt_frame_destroy(void *frame);
+/* SearchFrame preprocessing on the device, in place of the driveless
+ * SearchFrame's processDistanceToGoal / processSafeDistanceZone (not in the
+ * reference tree; their outputs are read at graph_direct_goal_connection.cu:
+ * 28-36 and 124-135).  The distance channel gets every cell's distance to
+ * (goal_x, goal_z), sqrtf(dx * dx + dz * dz) as checkDirectConnectionToGoal
+ * computes it, and the frame counts as isDistanceToGoalProcessed.  The safe
+ * zone sets traversability bit 0x100 on every cell whose footprint of half
+ * extents (min_dist / 2) holds no obstacle at any heading, and the frame
+ * counts as isSafeZoneChecked.  0 or -1. */
+int fastrrt_frame_process_distance_to_goal(void *frame, int goal_x, int goal_z);
+int fastrrt_frame_process_safe_zone(void *frame, int min_dist_x, int min_dist_z);
+/* the frame's isSafeZoneChecked / isDistanceToGoalProcessed flags */
+int fastrrt_frame_flags(void *frame, int *safe_zone_checked, int *distance_to_goal_processed);
+/* host copies of the distance and traversability channels (W*H each, NULL
+ * to skip one; zeros when the frame has none) */
+int fastrrt_frame_channels(void *frame, float *distance, int32_t *traversability);
 /* expansion RNG seed (default: wall-clock milliseconds, like the reference) */
 int fastrrt_set_seed(void *ptr, uint64_t seed);
 /* footprint probes of the reference algorithm run so far (instrumentation) */
@@ -128,7 +168,10 @@ int fastrrt_candidates_kinematic_device(void *ctx, int n, const int32_t *sx, con
                                         float velocity_m_s, float *out4, uint64_t *probes,
                                         void *stream);
 /* checkDirectConnectionToGoal (src/cuda/graph_direct_goal_connection.cu:16-167);
- * out = cost or -1.  Host buffers. */
+ * out = cost or -1.  safe_zone_checked: bit 0 isSafeZoneChecked (skip the
+ * footprints when the start cell has traversability bit 0x100), bit 1
+ * isDistanceToGoalProcessed (the distance from the frame's distance
+ * channel).  Host buffers. */
 int fastrrt_candidates_hermite(void *ctx, int n, const int32_t *x, const int32_t *z,
                                const float *local_heading, const int32_t *goal_x,
                                const int32_t *goal_z, const float *goal_heading,
@@ -170,6 +213,15 @@ int fastrrt_candidates_kinematic_noalloc(int width, int height, const uint8_t *c
                                          const int32_t *sx, const int32_t *sz, const float *steer,
                                          const float *length, float velocity_m_s, float *out4,
                                          uint64_t *probes, void *stream);
+/* Test hooks of the bounded waits, no counterpart in the reference.  The
+ * per-candidate kernels stage the frame masks in shared memory with a bulk
+ * copy and wait for it at most `rounds` mbarrier polls (default 4194304);
+ * a block that gives up counts a timeout, lets its copy finish (a second
+ * bounded wait) and reads the global masks, with the same results.
+ * fastrrt_debug_stage_timeouts returns the count since its last call and
+ * resets it.  0 or -1. */
+int fastrrt_debug_set_stage_wait_limit(int64_t rounds);
+int fastrrt_debug_stage_timeouts(uint64_t *count);
 /* __computeFeasibleForAngle (src/cuda/path_feasible.cu:18-78). Host buffers. */
 int fastrrt_candidates_feasible(void *ctx, int n, const int32_t *x, const int32_t *z,
                                 const float *angle, int32_t *out, uint64_t *probes);
@@ -240,6 +292,22 @@ int fastrrt_batch_collect(void *batch, int n, const int32_t *slots, int32_t *val
                           float *length, int32_t *path_n);
 /* copies the last collected path of list entry k: up to cap (x, z, heading) */
 int fastrrt_batch_path(void *batch, int k, float *xyh, int cap);
+/* interpolate (src/interpolation.cpp:112-135) of the paths of the last
+ * collected list, on the device: interpolateHermiteCurve between consecutive
+ * waypoints with the reference's float arithmetic (cells from round(), the
+ * heading of the curve's tangent), at most `cap` points per path; and the
+ * curve-quality metrics of each interpolated curve as the reference's
+ * tests/python_dataset/curve_quality.py computes them (length, jerk of the
+ * windowed direction, tangential discontinuity of the windowed heading above
+ * 15 degrees from the start heading; jerk NaN and discontinuity -1 where its
+ * arithmetic is undefined: fewer than 3 points or a window beyond the
+ * curve).  length / jerk / tan_disc get one value per path (NULL to skip);
+ * returns the number of paths or -1.  No counterpart in the reference ABI
+ * (its interpolation runs on the host, interpolate_planned_path). */
+int fastrrt_batch_interpolate(void *batch, int cap, float *length, float *jerk, int32_t *tan_disc);
+/* the k-th interpolated path of the last fastrrt_batch_interpolate:
+ * [x, z, heading] * m into xyh (at most cap points); returns m */
+int fastrrt_batch_interpolated_path(void *batch, int k, float *xyh, int cap);
 /* deactivates a slot; in a batch with a memory budget its storage returns to
  * the arena */
 int fastrrt_batch_release(void *batch, int slot);

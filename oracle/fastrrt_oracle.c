@@ -436,7 +436,11 @@ float orc_direct_connection(const orc_graph *g, const orc_frame *f, const orc_se
     const int W = sp->W, H = sp->H;
     const long pos = (long)z * W + x;
     const int dxi = goal_x - x, dzi = goal_z - z;
-    const float distance = sqrtf((float)(dxi * dxi + dzi * dzi));
+    /* isDistanceToGoalProcessed: the frame's distance channel
+     * (graph_direct_goal_connection.cu:28-36) */
+    const float distance = ((safe_zone_checked & ORC_DISTANCE_PROCESSED) && f->dist)
+                               ? f->dist[pos]
+                               : sqrtf((float)(dxi * dxi + dzi * dzi));
     const int numPoints = toi_f(distance);
     const float a1 = (float)(local_heading - ORC_HALF_PI);
     const float a2 = (float)(goal_heading - ORC_HALF_PI);
@@ -487,7 +491,7 @@ float orc_direct_connection(const orc_graph *g, const orc_frame *f, const orc_se
         }
         last_x = cx;
         last_z = cz;
-        if (safe_zone_checked && (trav & 0x100))
+        if ((safe_zone_checked & ORC_SAFE_ZONE_CHECKED) && (trav & 0x100))
             continue;
         if (!orc_feasible(f, sp, last_x, last_z, heading, probes))
             return -1;
@@ -1462,6 +1466,7 @@ int orc_plan_batch(int n, int W, int H, const uint8_t *cls, const float *class_c
         f.class_costs = class_costs;
         f.n_classes = n_classes;
         f.trav = NULL;
+        f.dist = NULL;
         orc_planner *p = orc_planner_new(W, H, pw_m, ph_m, max_steer_deg, vehicle_len,
                                          -1, -1, -1, -1, -1.0f);
         orc_plan_params pp;

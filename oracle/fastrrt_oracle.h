@@ -49,14 +49,22 @@ typedef struct { float x, y, z, w; } orc_f4;
 
 /* BEV frame: the reference's SearchFrame stores float3 per pixel
  * (class id, distance to goal, traversability bits).  The class id is held
- * as uint8 here; `trav` is the third channel (NULL = all zero). */
+ * as uint8 here; `trav` is the third channel (NULL = all zero), `dist` the
+ * second (NULL = none). */
 typedef struct {
     int W, H;
     const uint8_t *cls;
     const float *class_costs;
     int n_classes;
     const int32_t *trav;
+    const float *dist;
 } orc_frame;
+
+/* flag bits of orc_direct_connection's `safe_zone_checked` argument: the
+ * reference's isSafeZoneChecked and isDistanceToGoalProcessed
+ * (graph_direct_goal_connection.cu:16) */
+#define ORC_SAFE_ZONE_CHECKED 1
+#define ORC_DISTANCE_PROCESSED 2
 
 /* search-space parameters (graph.cu:306-314, FRAME_PARAM_*) */
 typedef struct {

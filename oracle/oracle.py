@@ -20,7 +20,7 @@ FP_HOST, FP_DEVICE = 0, 1
 class OrcFrame(C.Structure):
     _fields_ = [("W", C.c_int), ("H", C.c_int), ("cls", C.POINTER(C.c_uint8)),
                 ("class_costs", C.POINTER(C.c_float)), ("n_classes", C.c_int),
-                ("trav", C.POINTER(C.c_int32))]
+                ("trav", C.POINTER(C.c_int32)), ("dist", C.POINTER(C.c_float))]
 
 
 class OrcSearch(C.Structure):
@@ -188,22 +188,27 @@ def set_fp_mode(mode):
 class Frame:
     """Class-id frame + class-cost table (+ optional traversability bits)."""
 
-    def __init__(self, cls, class_costs, trav=None):
+    def __init__(self, cls, class_costs, trav=None, dist=None):
         self.cls = np.ascontiguousarray(cls, dtype=np.uint8)
         self.H, self.W = self.cls.shape
         self.costs = np.ascontiguousarray(class_costs, dtype=np.float32)
         self.trav = None if trav is None else np.ascontiguousarray(trav, dtype=np.int32)
+        self.dist = None if dist is None else np.ascontiguousarray(dist, dtype=np.float32)
         self.s = OrcFrame(self.W, self.H, self.cls.ctypes.data_as(C.POINTER(C.c_uint8)),
                           self.costs.ctypes.data_as(C.POINTER(C.c_float)), len(self.costs),
                           None if self.trav is None else
-                          self.trav.ctypes.data_as(C.POINTER(C.c_int32)))
+                          self.trav.ctypes.data_as(C.POINTER(C.c_int32)),
+                          None if self.dist is None else
+                          self.dist.ctypes.data_as(C.POINTER(C.c_float)))
 
     def xyz(self):
         """float3 frame as the reference's SearchFrame stores it"""
         out = np.zeros((self.H, self.W, 3), np.float32)
         out[..., 0] = self.cls
+        if self.dist is not None:
+            out[..., 1] = self.dist.reshape(self.H, self.W)
         if self.trav is not None:
-            out[..., 2] = self.trav
+            out[..., 2] = self.trav.reshape(self.H, self.W)
         return out
 
 

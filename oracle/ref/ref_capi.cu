@@ -145,8 +145,9 @@ __global__ void k_ref_direct(DevPtrs d, float maxc, int n, const int *x, const i
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    // safe: bit 0 isSafeZoneChecked, bit 1 isDistanceToGoalProcessed
     out[i] = checkDirectConnectionToGoal(d.data, d.frame, d.costs, d.sp, maxc, x[i], z[i], lh[i],
-                                         gx[i], gz[i], gh[i], safe != 0, false);
+                                         gx[i], gz[i], gh[i], (safe & 1) != 0, (safe & 2) != 0);
 }
 
 __global__ void k_ref_heading(int n, const int *x, const int *z, const int *gx, const int *gz,
@@ -204,7 +205,7 @@ int ref_h_direct(REF_COMMON_ARGS, float maxc, int n, const int *x, const int *z,
     for (int i = 0; i < n; i++)
         out[i] = checkDirectConnectionToGoal(in.data.data(), in.frame.data(), in.costs.data(), in.sp,
                                              maxc, x[i], z[i], lh[i], gx[i], gz[i], gh[i],
-                                             safe != 0, false);
+                                             (safe & 1) != 0, (safe & 2) != 0);
     return 0;
 }
 

@@ -24,8 +24,9 @@ def ctx_for(F, cls, heading=None, min_dist=(22, 40)):
 
 @pytest.mark.parametrize("coverage", [0.05, 0.15, 0.30])
 def test_kinematic_bit_exact_vs_reference_kernel(gpu, ref, coverage):
+    # the per-candidate microbench at full size: 2^20 candidates per density
     cls = synth.make_frame(100 + int(coverage * 100), 256, coverage=coverage)
-    heading, sx, sz, steer, seg = synth.candidates(20000, W, H, int(coverage * 1000))
+    heading, sx, sz, steer, seg = synth.candidates(1 << 20, W, H, int(coverage * 1000))
     fr, ctx = ctx_for(gpu, cls, heading)
     out, probes = ctx.kinematic(sx, sz, steer, seg, 2.0)
     rc = ref.RefCase(ref.Frame(cls, synth.CLASS_COSTS), heading=heading, max_steer_rad=MS, lr=LR,
@@ -116,8 +117,9 @@ def test_hermite_bit_exact_vs_reference_kernel(gpu, ref):
     cls, _, _ = synth.c0_request(4)
     fr, ctx = ctx_for(gpu, cls)
     rc = ref.RefCase(ref.Frame(cls, synth.CLASS_COSTS), mdx=11, mdz=20)
-    for npts in (2, 40, 64):
-        x, z, lh, gx, gz, gh = synth.hermite_pairs(8192, W, H, npts, num_points=npts)
+    # 65,536 pose pairs at the microbench's 64 samples, and short curves
+    for npts, n in ((64, 65536), (2, 8192), (40, 8192)):
+        x, z, lh, gx, gz, gh = synth.hermite_pairs(n, W, H, npts, num_points=npts)
         out, _ = ctx.hermite(x, z, lh, gx, gz, gh, 0.8)
         r = rc.direct(0.8, x, z, lh, gx, gz, gh, device=True)
         assert np.array_equal(out.view(np.uint32), r.view(np.uint32)), npts
