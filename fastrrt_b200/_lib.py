@@ -63,11 +63,13 @@ EXPORTS = [
     "fastrrt_batch_collect", "fastrrt_batch_path", "fastrrt_batch_release",
     "fastrrt_batch_last_ms", "fastrrt_batch_plan", "fastrrt_batch_profile",
     "fastrrt_batch_kernel_times", "fastrrt_kernel_count", "fastrrt_kernel_name",
-    "fastrrt_batch_probes", "fastrrt_batch_interpolate", "fastrrt_batch_interpolated_path", "fastrrt_batch_direct_connections", "fastrrt_batch_serve",
+    "fastrrt_batch_probes", "fastrrt_batch_interpolate", "fastrrt_batch_interpolated_path",
+    "fastrrt_batch_direct_connections", "fastrrt_batch_serve",
     # learned expansion proposal
     "fastrrt_mlp_create", "fastrrt_mlp_destroy", "fastrrt_mlp_get_weights",
     "fastrrt_mlp_set_weights", "fastrrt_mlp_forward", "fastrrt_mlp_gradients", "fastrrt_mlp_train",
     "fastrrt_batch_set_proposal", "fastrrt_batch_log_paths", "fastrrt_batch_set_launch",
+    "fastrrt_gemm_bf16", "fastrrt_batch_log_nodes",
 ]
 
 
@@ -179,8 +181,11 @@ def lib():
         "fastrrt_mlp_train": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64,
                                         P(C.c_float)]),
         "fastrrt_batch_set_proposal": (C.c_int, [vp, vp, C.c_float, C.c_int]),
+        "fastrrt_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int,
+                                        C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
         "fastrrt_batch_set_launch": (C.c_int, [vp, C.c_int, C.c_int]),
         "fastrrt_batch_log_paths": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
+        "fastrrt_batch_log_nodes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
         "fastrrt_batch_serve": (C.c_int, [vp, C.c_int, P(Request), vp, C.c_int, C.c_int, i32p, f32p,
                                           f32p, f32p, i32p, P(C.c_double), P(C.c_float)]),
     }

@@ -214,6 +214,13 @@ class BatchPlanner:
                                                              labels_dev.data_ptr(), int(offset),
                                                              int(cap)), "batch_log_paths")
 
+    def log_nodes(self, X_dev, labels_dev, offset, cap):
+        """training rows of every accepted expansion (node of the final graph
+        but the start) of the last collected list's solved requests"""
+        return _lib.check(_lib.lib().fastrrt_batch_log_nodes(self._h, X_dev.data_ptr(),
+                                                             labels_dev.data_ptr(), int(offset),
+                                                             int(cap)), "batch_log_nodes")
+
     def profile(self, on=True):
         _lib.check(_lib.lib().fastrrt_batch_profile(self._h, int(on)), "batch_profile")
 

@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfastrrt_b200.so")
 OBJ = os.path.join(HERE, "_obj")
 SOURCES = ["frrt_kernels.cu", "frrt_engine.cu", "frrt_capi.cu", "frrt_noalloc.cu", "frrt_mlp.cu",
-           "frrt_mlp_capi.cu"]
+           "frrt_mlp_capi.cu", "frrt_umma.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC]

@@ -103,32 +103,12 @@ struct Batch {
     std::vector<int> admitted;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.0f;
-    // two pinned state snapshots of the serving loop and their events
-    State *snap[2] = {nullptr, nullptr};
-    cudaEvent_t snap_ev[2] = {nullptr, nullptr};
-    bool snapshots()
-    {
-        const size_t b = sizeof(State) * (size_t)eng->n_slots();
-        for (int k = 0; k < 2; k++) {
-            if (!snap[k] && cudaMallocHost(&snap[k], b) != cudaSuccess)
-                return false;
-            if (!snap_ev[k] && cudaEventCreateWithFlags(&snap_ev[k], cudaEventDisableTiming) != cudaSuccess)
-                return false;
-        }
-        return true;
-    }
     ~Batch()
     {
         if (ev0)
             cudaEventDestroy(ev0);
         if (ev1)
             cudaEventDestroy(ev1);
-        for (int k = 0; k < 2; k++) {
-            if (snap[k])
-                cudaFreeHost(snap[k]);
-            if (snap_ev[k])
-                cudaEventDestroy(snap_ev[k]);
-        }
     }
 };
 
@@ -1283,20 +1263,6 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
     for (int s = n_slots - 1; s >= 0; s--)
         free_slots.push_back(s);
     std::vector<double> admitted_at(n, 0.0);
-    if (!b->snapshots()) {
-        set_error("batch serve: pinned snapshot allocation failed");
-        return -1;
-    }
-    // One batch of iterations stays in flight: the loop launches the next
-    // batch and a copy of the states after it, then reads the states of the
-    // batch before.  A slot's finish time is on the device clock, so reading
-    // it a batch late changes no latency; a finished slot only takes part in
-    // that extra batch as a no-op.  admit_batch[s]: the first batch whose
-    // snapshot shows the request admitted to slot s.
-    std::vector<long> admit_batch(n_slots, 0);
-    long batch_idx = 0, pend_batch = -1;
-    int cur = 0;
-    bool pending = false;
     int next = 0, finished = 0, in_flight = 0, good = 0;
     while (finished < n) {
         // admit every request that has arrived while a slot is free
@@ -1309,7 +1275,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
             if (!e.ensure_storage(s, reqs[next].width, reqs[next].height)) {
                 if (!e.out_of_budget())
                     return -1;
-                if (in_flight == 0 && list.empty() && !pending) {
+                if (in_flight == 0 && list.empty()) {
                     set_error("batch serve: a request needs more memory than the whole budget");
                     return -1;
                 }
@@ -1320,7 +1286,6 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                 return -1;
             owner[s] = next;
             admitted_at[next] = now;
-            admit_batch[s] = batch_idx;
             list.push_back(s);
             next++;
         }
@@ -1329,7 +1294,7 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                 return -1;
             in_flight += (int)list.size();
         }
-        if (in_flight == 0 && !pending) {
+        if (in_flight == 0) {
             if (!arrival_ms || next >= n) {
                 set_error("batch serve: no free slot");
                 return -1;
@@ -1341,61 +1306,43 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
                     (long long)std::min(wait * 1000.0, 200.0)));
             continue;
         }
-        bool launched = false;
-        long this_batch = -1;
-        if (in_flight > 0) {
-            for (int k = 0; k < check_every; k++)
-                if (!e.iterate())
-                    return -1;
-            if (!e.snapshot_states(b->snap[cur], b->snap_ev[cur]))
+        for (int k = 0; k < check_every; k++)
+            if (!e.iterate())
                 return -1;
-            launched = true;
-            this_batch = batch_idx++;
+        if (!e.fetch_states(true))
+            return -1;
+        // harvest finished slots and free them
+        list.clear();
+        for (int s = 0; s < n_slots; s++)
+            if (owner[s] >= 0 && e.state(s).done)
+                list.push_back(s);
+        if (list.empty())
+            continue;
+        if (!e.extract_and_validate(list, 1024, false))
+            return -1;
+        for (size_t k = 0; k < list.size(); k++) {
+            const int s = list[k];
+            const int r = owner[s];
+            const State &S = e.state(s);
+            const int v = e.valid()[k] && S.goal_reached;
+            good += v;
+            const double fin = finish_ms(S.finish_ns);
+            if (valid)
+                valid[r] = v;
+            if (length)
+                length[r] = e.lengths()[k];
+            if (latency_ms)
+                latency_ms[r] = (float)(fin - (arrival_ms ? arrival_ms[r] : 0.0));
+            if (service_ms)
+                service_ms[r] = (float)(fin - admitted_at[r]);
+            if (loops)
+                loops[r] = S.loops;
+            owner[s] = -1;
+            free_slots.push_back(s);
+            e.release_storage(s);  // budget mode: back to the arena
+            in_flight--;
+            finished++;
         }
-        if (pending) {
-            // harvest the finished slots of the batch before
-            const int pb = cur ^ 1;
-            if (cudaEventSynchronize(b->snap_ev[pb]) != cudaSuccess) {
-                set_error(std::string("batch serve: ") + cudaGetErrorString(cudaGetLastError()));
-                return -1;
-            }
-            const State *snap = b->snap[pb];
-            list.clear();
-            for (int s = 0; s < n_slots; s++)
-                if (owner[s] >= 0 && admit_batch[s] <= pend_batch && snap[s].done)
-                    list.push_back(s);
-            if (!list.empty()) {
-                if (!e.extract_and_validate(list, 1024, false))
-                    return -1;
-                for (size_t k = 0; k < list.size(); k++) {
-                    const int s = list[k];
-                    const int r = owner[s];
-                    const State &S = snap[s];
-                    const int v = e.valid()[k] && S.goal_reached;
-                    good += v;
-                    const double fin = finish_ms(S.finish_ns);
-                    if (valid)
-                        valid[r] = v;
-                    if (length)
-                        length[r] = e.lengths()[k];
-                    if (latency_ms)
-                        latency_ms[r] = (float)(fin - (arrival_ms ? arrival_ms[r] : 0.0));
-                    if (service_ms)
-                        service_ms[r] = (float)(fin - admitted_at[r]);
-                    if (loops)
-                        loops[r] = S.loops;
-                    owner[s] = -1;
-                    free_slots.push_back(s);
-                    e.release_storage(s);  // budget mode: back to the arena
-                    in_flight--;
-                    finished++;
-                }
-            }
-        }
-        pending = launched;
-        pend_batch = this_batch;
-        if (launched)
-            cur ^= 1;
     }
     cudaEventRecord(b->ev1, e.stream());
     cudaEventSynchronize(b->ev1);
@@ -1440,6 +1387,16 @@ int fastrrt_batch_log_paths(void *batch, void *X_bf16, int32_t *labels, int offs
         return -1;
     }
     return b->eng->log_paths(static_cast<__nv_bfloat16 *>(X_bf16), labels, offset, cap);
+}
+
+int fastrrt_batch_log_nodes(void *batch, void *X_bf16, int32_t *labels, int offset, int cap)
+{
+    auto *b = static_cast<Batch *>(batch);
+    if (!b || !X_bf16 || !labels || offset < 0 || cap < offset) {
+        set_error("batch log_nodes: bad arguments");
+        return -1;
+    }
+    return b->eng->log_paths(static_cast<__nv_bfloat16 *>(X_bf16), labels, offset, cap, true);
 }
 
 int fastrrt_batch_probes(void *batch, uint64_t *expand, uint64_t *goal, uint64_t *precompute)

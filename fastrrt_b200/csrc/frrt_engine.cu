@@ -833,14 +833,17 @@ bool Engine::fetch_states(bool synchronous)
                                stream_),
                "state download"))
         return false;
-    return !synchronous || sync();
-}
-
-bool Engine::snapshot_states(State *dst, cudaEvent_t done)
-{
-    return check(cudaMemcpyAsync(dst, d_state_, sizeof(State) * n_slots_, cudaMemcpyDeviceToHost, stream_),
-                 "state snapshot") &&
-           check(cudaEventRecord(done, stream_), "state snapshot event");
+    if (!synchronous)
+        return true;
+    if (!sync())
+        return false;
+    // the proposal network's GEMMs of the iterations since the last check
+    if (use_proposal_)
+        if (const char *e = gemm_take_error()) {
+            set_error(std::string("proposal: ") + e);
+            return false;
+        }
+    return true;
 }
 
 bool Engine::deactivate(int slot)
@@ -1207,6 +1210,11 @@ bool Engine::set_launch(int sweep_per_sm, int work_per_sm)
 
 bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
 {
+    if (w && !umma_init()) {
+        const char *e = gemm_take_error();
+        set_error(std::string("proposal: ") + (e ? e : "tensor-core GEMM unavailable"));
+        return false;
+    }
     if (w && cap > 0 && cap != pb_.cap) {
         cudaFree(pb_.cells);
         cudaFree(pb_.slot_of);
@@ -1249,7 +1257,7 @@ bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
     return commit();
 }
 
-int Engine::log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap)
+int Engine::log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap, bool all_nodes)
 {
     const int n = (int)h_path_n_.size();
     if (n == 0 || cap <= offset)
@@ -1267,8 +1275,12 @@ int Engine::log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap)
     }
     if (!check(cudaMemsetAsync(d_log_count_, 0, sizeof(int), stream_), "log counter"))
         return -1;
-    launch_log_paths(d_inst_, d_state_, d_slots_, n, d_paths_, d_path_n_, d_valid_, cap_, d_log_cells_,
-                     d_log_slots_, labels + offset, d_log_count_, rows_max, stream_);
+    if (all_nodes)
+        launch_log_nodes(d_inst_, d_state_, d_slots_, n, d_valid_, d_log_cells_, d_log_slots_, labels + offset,
+                         d_log_count_, rows_max, stream_);
+    else
+        launch_log_paths(d_inst_, d_state_, d_slots_, n, d_paths_, d_path_n_, d_valid_, cap_, d_log_cells_,
+                         d_log_slots_, labels + offset, d_log_count_, rows_max, stream_);
     int rows = 0;
     if (!check(cudaMemcpyAsync(&h_small_[4], d_log_count_, sizeof(int), cudaMemcpyDeviceToHost, stream_),
                "log counter") ||

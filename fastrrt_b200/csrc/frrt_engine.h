@@ -147,9 +147,6 @@ public:
     bool sync();
     // copy the small head of the state of every slot to host memory
     bool fetch_states(bool synchronous = true);
-    // the same copy into `dst` (pinned host memory, n_slots states) on the
-    // stream, completion marked by `done`; no host wait
-    bool snapshot_states(State *dst, cudaEvent_t done);
     const State &state(int slot) const { return h_state_[slot]; }
     bool deactivate(int slot);
 
@@ -195,8 +192,9 @@ public:
     // training rows of the last extracted list: for each valid path, one row
     // per expansion on it (features of the parent, the bin of the draw that
     // made the child) appended at X[offset..], labels[offset..] (device, at
-    // most cap rows in all); returns the rows added or -1
-    int log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap);
+    // most cap rows in all); returns the rows added or -1.  all_nodes: one
+    // row per node of each solved graph but the start instead
+    int log_paths(__nv_bfloat16 *X, int32_t *labels, int offset, int cap, bool all_nodes = false);
     // the validator's halves on one slot: checkGraphIsConsistent of its
     // graph (graph_check_dag_consistency.cpp:33-76), and the per-path checks
     // of a host path [x, z, heading] * m against its frame, grid and goal;

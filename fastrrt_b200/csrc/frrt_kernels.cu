@@ -1416,14 +1416,23 @@ __global__ void __launch_bounds__(256) k_prop_list(const Inst *insts, const Stat
 {
     const int n = sc->n_slots;
     const int total = sc->cand_start[n];
+    const int lane = threadIdx.x & 31;
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
         const int slot = find_slot(sc->cand_start, n, c);
         const Inst &I = insts[slot];
         const State &S = states[slot];
         const int idx = (c - sc->cand_start[slot]) * kCandChunk + threadIdx.x;
-        if (idx >= S.n_cand || !I.proposal)
+        const bool is = idx < S.n_cand && I.proposal;
+        const unsigned m = __ballot_sync(kFull, is);
+        if (!m)
             continue;
-        int row = atomicAdd(pb.count, 1);
+        int b0 = 0;
+        if (lane == 0)
+            b0 = atomicAdd(pb.count, __popc(m));  // one atomic per warp
+        b0 = __shfl_sync(kFull, b0, 0);
+        if (!is)
+            continue;
+        int row = b0 + __popc(m & ((1u << lane) - 1u));
         if (row >= pb.cap) {
             row = -1;
         } else {
@@ -2040,6 +2049,9 @@ __global__ void __launch_bounds__(128) k_interp(const Inst *insts, const int *sl
     int cnt = 0, last_x = -1, last_z = -1;
     bool full = false;
     for (int s = 1; s < m && !full; s++) {
+        // each segment's samples are deduplicated on their own: the end cell
+        // of one segment and the start cell of the next are both kept
+        last_x = last_z = -1;
         const int p1x = (int)p[3 * (s - 1)], p1z = (int)p[3 * (s - 1) + 1];
         const int p2x = (int)p[3 * s], p2z = (int)p[3 * s + 1];
         const float p1h = p[3 * (s - 1) + 2], p2h = p[3 * s + 2];
@@ -2048,8 +2060,10 @@ __global__ void __launch_bounds__(128) k_interp(const Inst *insts, const int *sl
         const float dx = (float)(p2x - p1x), dz = (float)(p2z - p1z);
         const float d = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)));
         const float a1 = (float)(p1h - kPi / 2), a2 = (float)(p2h - kPi / 2);
-        const float t1x = __fmul_rn(d, cosf(a1)), t1y = __fmul_rn(d, sinf(a1));
-        const float t2x = __fmul_rn(d, cosf(a2)), t2y = __fmul_rn(d, sinf(a2));
+        // the host's float trigonometry, rounded from double (the correctly
+        // rounded float value but in rare halfway cases)
+        const float t1x = __fmul_rn(d, (float)cos((double)a1)), t1y = __fmul_rn(d, (float)sin((double)a1));
+        const float t2x = __fmul_rn(d, (float)cos((double)a2)), t2y = __fmul_rn(d, (float)sin((double)a2));
         const float fx1 = (float)p1x, fz1 = (float)p1z, fx2 = (float)p2x, fz2 = (float)p2z;
         // x = h00 p1 + h10 tan1 + h01 p2 + h11 tan2, summed left to right
         auto mix = [](float a, float b, float c, float d4, float u, float v, float w, float q) {
@@ -2086,7 +2100,7 @@ __global__ void __launch_bounds__(128) k_interp(const Inst *insts, const int *sl
                 const float t11 = __fsub_rn(__fmul_rn(3.0f, t2), __fmul_rn(2.0f, t));
                 const float ddx = mix(t00, t10, t01, t11, fx1, t1x, fx2, t2x);
                 const float ddz = mix(t00, t10, t01, t11, fz1, t1y, fz2, t2y);
-                const float heading = (float)(atan2f(ddz, ddx) + kPi / 2);
+                const float heading = (float)((double)(float)atan2((double)ddz, (double)ddx) + kPi / 2);
                 const int at = cnt + __popc(km & lower);
                 if (at < out_cap) {
                     o[3 * at] = (float)cx;
@@ -2239,6 +2253,53 @@ __global__ void __launch_bounds__(128) k_log_list(const Inst *insts, const State
         slot_of[row] = slot;
         labels[row] = proposal_bin(I.exp_steer[child], I.exp_len[child], (float)I.max_steer, I.max_path);
     }
+}
+
+// Training rows of every accepted expansion of the solved slots: each NODE
+// cell but the start, with its parent cell, its slot, and the bin of the draw
+// that made it.  blockIdx.y = list entry; the blocks of an entry stride over
+// its cells; rows appended warp by warp (their order is not deterministic).
+__global__ void __launch_bounds__(256) k_log_nodes(const Inst *insts, const State *states, const int *slots,
+                                                   const int *valid, int32_t *cells, int32_t *slot_of,
+                                                   int32_t *labels, int *count, int cap_rows)
+{
+    const int k = blockIdx.y;
+    const int slot = slots[k];
+    if (!valid[k] || !states[slot].goal_reached)
+        return;  // uniform across the block
+    const Inst &I = insts[slot];
+    const int lane = threadIdx.x & 31;
+    const int n_cells = I.W * I.H, start = I.start_z * I.W + I.start_x;
+    for (int base = blockIdx.x * blockDim.x; base < n_cells; base += gridDim.x * blockDim.x) {
+        const int c = base + threadIdx.x;
+        const bool is = c < n_cells && c != start && I.type[c] == T_NODE;
+        const unsigned m = __ballot_sync(kFull, is);
+        if (!m)
+            continue;
+        int b0 = 0;
+        if (lane == 0)
+            b0 = atomicAdd(count, __popc(m));
+        b0 = __shfl_sync(kFull, b0, 0);
+        if (!is)
+            continue;
+        const int row = b0 + __popc(m & ((1u << lane) - 1u));
+        if (row >= cap_rows)
+            continue;
+        const int32_t par = I.parent[c];
+        cells[row] = unpack_z(par) * I.W + unpack_x(par);
+        slot_of[row] = slot;
+        labels[row] = proposal_bin(I.exp_steer[c], I.exp_len[c], (float)I.max_steer, I.max_path);
+    }
+}
+
+void launch_log_nodes(const Inst *d_inst, const State *d_state, const int *d_slots, int n, const int *d_valid,
+                      int32_t *cells, int32_t *slot_of, int32_t *labels, int *count, int cap_rows,
+                      cudaStream_t st)
+{
+    if (n <= 0)
+        return;
+    k_log_nodes<<<dim3(16, n), 256, 0, st>>>(d_inst, d_state, d_slots, d_valid, cells, slot_of, labels, count,
+                                             cap_rows);
 }
 
 void launch_log_paths(const Inst *d_inst, const State *d_state, const int *d_slots, int n,

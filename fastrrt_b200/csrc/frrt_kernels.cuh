@@ -109,6 +109,11 @@ void launch_log_paths(const Inst *d_inst, const State *d_state, const int *d_slo
                       const float *d_paths, const int *d_path_n, const int *d_valid, int cap,
                       int32_t *cells, int32_t *slot_of, int32_t *labels, int *count, int cap_rows,
                       cudaStream_t st);
+// the same for every accepted expansion (NODE cell but the start) of the
+// solved slots of the list
+void launch_log_nodes(const Inst *d_inst, const State *d_state, const int *d_slots, int n, const int *d_valid,
+                      int32_t *cells, int32_t *slot_of, int32_t *labels, int *count, int cap_rows,
+                      cudaStream_t st);
 // count cells of `type` (type < 0: all non-NULL) for listed slots into d_out[k]
 void launch_count(const Inst *d_inst, const int *d_slots, int n, int max_cells, int type,
                   unsigned *d_out, cudaStream_t st);

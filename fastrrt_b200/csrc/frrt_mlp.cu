@@ -1,5 +1,5 @@
-// frrt_mlp.cu -- BF16 tensor-core GEMM, training kernels and planner-side
-// feature extraction of the learned expansion proposal.
+// frrt_mlp.cu -- training kernels, forward pass and planner-side feature
+// extraction of the learned expansion proposal (the GEMM is frrt_umma.cu).
 #include "frrt_mlp.cuh"
 #include "frrt_device.cuh"
 
@@ -9,131 +9,6 @@
 namespace frrt {
 
 namespace {
-
-constexpr int kBM = 64, kBN = 64, kBK = 32, kPad = 8;
-
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi)
-{
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// 64 x 64 output tile per block of 4 warps (2 x 2, 32 x 32 each), K in steps
-// of 32 through shared memory (both operands K-contiguous there), fragments
-// of mma.sync m16n8k16 (A row-major, B column-major).
-__global__ void __launch_bounds__(128) k_gemm(GemmArgs g)
-{
-    __shared__ __nv_bfloat16 As[kBM][kBK + kPad];
-    __shared__ __nv_bfloat16 Bs[kBN][kBK + kPad];
-    if (g.dM) {
-        const int cnt = *g.dM;
-        g.M = cnt < g.M ? cnt : g.M;
-    }
-    const int n0 = blockIdx.x * kBN;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int gq = lane >> 2, tq = lane & 3;
-    // row tiles grid-strided: the grid is sized for the machine, the rows (a
-    // device-side count in the planner) may be few (uniform across the block)
-    for (int m0 = blockIdx.y * kBM; m0 < g.M; m0 += gridDim.y * kBM) {
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-                acc[i][j][e] = 0.0f;
-    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-    for (int k0 = 0; k0 < g.K; k0 += kBK) {
-        for (int e = tid; e < kBM * kBK; e += blockDim.x) {
-            int r, c;
-            if (g.transA) {  // consecutive threads along m (contiguous in memory)
-                r = e % kBM;
-                c = e / kBM;
-            } else {
-                r = e / kBK;
-                c = e % kBK;
-            }
-            const int m = m0 + r, k = k0 + c;
-            __nv_bfloat16 v = zero;
-            if (m < g.M && k < g.K)
-                v = g.transA ? g.A[(long)k * g.lda + m] : g.A[(long)m * g.lda + k];
-            As[r][c] = v;
-        }
-        for (int e = tid; e < kBN * kBK; e += blockDim.x) {
-            int r, c;
-            if (g.transB) {  // contiguous along n
-                r = e % kBN;
-                c = e / kBN;
-            } else {
-                r = e / kBK;
-                c = e % kBK;
-            }
-            const int n = n0 + r, k = k0 + c;
-            __nv_bfloat16 v = zero;
-            if (n < g.N && k < g.K)
-                v = g.transB ? g.B[(long)k * g.ldb + n] : g.B[(long)n * g.ldb + k];
-            Bs[r][c] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kBK; kk += 16) {
-            uint32_t a[2][4], b[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm + i * 16 + gq, c = kk + 2 * tq;
-                a[i][0] = pack_bf16(As[r][c], As[r][c + 1]);
-                a[i][1] = pack_bf16(As[r + 8][c], As[r + 8][c + 1]);
-                a[i][2] = pack_bf16(As[r][c + 8], As[r][c + 9]);
-                a[i][3] = pack_bf16(As[r + 8][c + 8], As[r + 8][c + 9]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int n = wn + j * 8 + gq, c = kk + 2 * tq;
-                b[j][0] = pack_bf16(Bs[n][c], Bs[n][c + 1]);
-                b[j][1] = pack_bf16(Bs[n][c + 8], Bs[n][c + 9]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    mma_bf16(acc[i][j], a[i], b[j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const int m = m0 + wm + i * 16 + gq + (e >= 2 ? 8 : 0);
-                const int n = n0 + wn + j * 8 + 2 * tq + (e & 1);
-                if (m >= g.M || n >= g.N)
-                    continue;
-                float v = acc[i][j][e];
-                if (g.bias)
-                    v += g.bias[n];
-                if (g.relu)
-                    v = fmaxf(v, 0.0f);
-                if (g.mask && !(__bfloat162float(g.mask[(long)m * g.ldm + n]) > 0.0f))
-                    v = 0.0f;
-                if (g.cf)
-                    g.cf[(long)m * g.ldc + n] = v;
-                else
-                    g.cb[(long)m * g.ldc + n] = __float2bfloat16(v);
-            }
-    }
-}
 
 // one warp per row of 128 logits
 __global__ void k_softmax_xent(const float *logits, const int32_t *labels, int M, float scale,
@@ -239,16 +114,24 @@ __global__ void k_features(const Inst *insts, const int32_t *cells, const int32_
         // pixel offsets: forward (sin h, -cos h), right (cos h, sin h)
         __nv_bfloat16 *row = X + (long)k * kMlpInPad;
         const int half = kMlpPatch / 2;
-        for (int s = lane; s < kMlpPatch * kMlpPatch; s += 32) {
-            const int iu = s / kMlpPatch, iv = s % kMlpPatch;
+        // lane = patch column; the 32 rows' mask words are loaded before any
+        // is used, so their latencies overlap instead of adding up
+        const float v = (float)((lane - half) * kMlpPatchStride);  // right
+        uint32_t word[kMlpPatch];
+        int bit[kMlpPatch];
+#pragma unroll
+        for (int iu = 0; iu < kMlpPatch; iu++) {
             const float u = (float)((half - 1 - iu) * kMlpPatchStride);  // forward, row 0 ahead
-            const float v = (float)((iv - half) * kMlpPatchStride);      // right
             const int px = (int)floorf(x + u * sh + v * ch + 0.5f);
             const int pz = (int)floorf(z - u * ch + v * sh + 0.5f);
-            float val = 0.5f;  // outside the frame
-            if (px >= 0 && px < I.W && pz >= 0 && pz < I.H)
-                val = bit_xz(I.blocked, I.mask_rw, px, pz) ? 1.0f : 0.0f;
-            row[s] = __float2bfloat16(val);
+            const bool in = px >= 0 && px < I.W && pz >= 0 && pz < I.H;
+            word[iu] = in ? I.blocked[(long)pz * I.mask_rw + (px >> 5)] : 0u;
+            bit[iu] = in ? (px & 31) : -1;  // -1: outside the frame
+        }
+#pragma unroll
+        for (int iu = 0; iu < kMlpPatch; iu++) {
+            const float val = bit[iu] < 0 ? 0.5f : (((word[iu] >> bit[iu]) & 1u) ? 1.0f : 0.0f);
+            row[iu * kMlpPatch + lane] = __float2bfloat16(val);
         }
         if (lane < kMlpInPad - kMlpPatch * kMlpPatch) {
             const float dx = (float)(I.goal_x - x), dz = (float)(I.goal_z - z);
@@ -269,16 +152,6 @@ __global__ void k_features(const Inst *insts, const int32_t *cells, const int32_
 }
 
 }  // namespace
-
-void launch_gemm(const GemmArgs &g, cudaStream_t st)
-{
-    if (g.M <= 0 || g.N <= 0)
-        return;
-    // at most kMlpGridBlocks blocks (the row tiles loop beyond that)
-    const int nx = (g.N + kBN - 1) / kBN;
-    const int ny = std::min((g.M + kBM - 1) / kBM, std::max(1, kMlpGridBlocks / nx));
-    k_gemm<<<dim3(nx, ny), 128, 0, st>>>(g);
-}
 
 void launch_softmax_xent(const float *logits, const int32_t *labels, int M, float scale,
                          __nv_bfloat16 *dlogits, float *loss, cudaStream_t st)

@@ -1,7 +1,7 @@
 // frrt_mlp.cuh -- the learned expansion proposal: a BF16 MLP (1030 -> 256 ->
-// 256 -> 128, ReLU, FP32 accumulation) with hand-written tensor-core GEMMs
-// (mma.sync m16n8k16 bf16), its training kernels, and the planner-side
-// feature extraction and proposal sampling.
+// 256 -> 128, ReLU, FP32 accumulation) with a hand-written tcgen05 GEMM, its
+// training kernels, and the planner-side feature extraction and proposal
+// sampling.
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -53,7 +53,16 @@ struct GemmArgs {
     __nv_bfloat16 *cb;
     int ldc;
 };
+// on the 5th-generation tensor cores (frrt_umma.cu); a launch that cannot be
+// made, or a block whose pipeline wait ran out, leaves an error for
+// gemm_take_error()
 void launch_gemm(const GemmArgs &g, cudaStream_t st);
+// the GEMM's runtime (driver tensor-map entry point, kernel attributes,
+// error flag); false when it cannot run here
+bool umma_init();
+// the first GEMM error since the last call (launch or device), or nullptr;
+// read after the stream of the launches was synchronised
+const char *gemm_take_error();
 
 // softmax cross-entropy over rows of logits (M x 128, f32): per-row loss
 // (f32, summed into *loss), d logits = (softmax - onehot) * scale as bf16

@@ -30,6 +30,16 @@ bool cuda_ok(cudaError_t e, const char *what)
     return false;
 }
 
+// the GEMMs launched since the last check ran (after a stream sync)
+bool gemm_ok()
+{
+    if (const char *e = gemm_take_error()) {
+        set_error(std::string("mlp: ") + e);
+        return false;
+    }
+    return true;
+}
+
 }  // namespace
 
 const size_t Mlp::kSizes[6] = {(size_t)kMlpHidden * kMlpInPad, kMlpHidden,
@@ -38,6 +48,10 @@ const size_t Mlp::kSizes[6] = {(size_t)kMlpHidden * kMlpInPad, kMlpHidden,
 
 Mlp::Mlp(uint64_t seed, int max_batch) : max_batch_(max_batch)
 {
+    if (!umma_init()) {
+        gemm_ok();
+        return;
+    }
     if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) {
         set_error("mlp: stream");
         return;
@@ -225,7 +239,7 @@ bool Mlp::train(const __nv_bfloat16 *X, const int32_t *labels, int n_total, int 
         }
         if (!cuda_ok(cudaMemcpyAsync(&loss, loss_, sizeof(float), cudaMemcpyDeviceToHost, stream_),
                      "loss") ||
-            !cuda_ok(cudaStreamSynchronize(stream_), "epoch"))
+            !cuda_ok(cudaStreamSynchronize(stream_), "epoch") || !gemm_ok())
             return false;
     }
     if (last_loss)
@@ -290,7 +304,7 @@ int fastrrt_mlp_forward(void *mlp, int n, const float *X, float *logits)
     m->forward(m->x(), n, m->stream(), m->logits(), m->h1(), m->h2(), nullptr);
     return cuda_ok(cudaMemcpyAsync(logits, m->logits(), sizeof(float) * n * kMlpOut,
                                    cudaMemcpyDeviceToHost, m->stream()), "logits") &&
-                   cuda_ok(cudaStreamSynchronize(m->stream()), "forward")
+                   cuda_ok(cudaStreamSynchronize(m->stream()), "forward") && gemm_ok()
                ? 0
                : -1;
 }
@@ -310,11 +324,48 @@ int fastrrt_mlp_gradients(void *mlp, int n, const float *X, const int32_t *label
     float l = 0.0f;
     if (!cuda_ok(cudaMemcpyAsync(&l, m->loss(), sizeof(float), cudaMemcpyDeviceToHost, m->stream()),
                  "loss") ||
-        !cuda_ok(cudaStreamSynchronize(m->stream()), "gradients"))
+        !cuda_ok(cudaStreamSynchronize(m->stream()), "gradients") || !gemm_ok())
         return -1;
     if (loss)
         *loss = l / n;
     return 0;
+}
+
+int fastrrt_gemm_bf16(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb,
+                      int transB, const float *bias, int relu, const void *mask, int ldm, float *Cf, void *Cb,
+                      int ldc, const int *dM, void *stream)
+{
+    if (M < 0 || N < 0 || K <= 0 || !A || !B || (!Cf) == (!Cb) || ldc < N ||
+        lda < (transA ? M : K) || ldb < (transB ? N : K) || (mask && ldm < N)) {
+        set_error("gemm: bad arguments");
+        return -1;
+    }
+    if (!umma_init())
+        return gemm_ok() ? 0 : -1;
+    GemmArgs g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.dM = dM;
+    g.A = static_cast<const __nv_bfloat16 *>(A);
+    g.lda = lda;
+    g.transA = transA;
+    g.B = static_cast<const __nv_bfloat16 *>(B);
+    g.ldb = ldb;
+    g.transB = transB;
+    g.bias = bias;
+    g.relu = relu;
+    g.mask = static_cast<const __nv_bfloat16 *>(mask);
+    g.ldm = ldm;
+    g.cf = Cf;
+    g.cb = static_cast<__nv_bfloat16 *>(Cb);
+    g.ldc = ldc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    launch_gemm(g, st);
+    return cuda_ok(cudaGetLastError(), "gemm launch") && cuda_ok(cudaStreamSynchronize(st), "gemm") &&
+                   gemm_ok()
+               ? 0
+               : -1;
 }
 
 int fastrrt_mlp_train(void *mlp, const void *X_bf16, const int32_t *labels, int n, int epochs,

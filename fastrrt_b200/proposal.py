@@ -14,6 +14,10 @@ N_OUT = 128
 STEER_BINS = 16
 LEN_BINS = 8
 SHAPES = [(HIDDEN, N_IN_PAD), (HIDDEN,), (HIDDEN, HIDDEN), (HIDDEN,), (N_OUT, HIDDEN), (N_OUT,)]
+# GEMM FLOPs of one training row: forward (3 layers) + backward (the weight
+# gradients of all three layers, the input gradients of layers 2 and 3)
+FWD_FLOP_PER_ROW = 2 * (HIDDEN * N_IN_PAD + HIDDEN * HIDDEN + N_OUT * HIDDEN)
+TRAIN_FLOP_PER_ROW = FWD_FLOP_PER_ROW + 2 * (HIDDEN * N_IN_PAD + 2 * HIDDEN * HIDDEN + 2 * N_OUT * HIDDEN)
 
 
 class ProposalNet:
@@ -74,13 +78,16 @@ class ProposalNet:
 
 
 def collect_dataset(n_plans, seed0=500_000, max_rows=200_000, slots=256, max_iterations=100,
-                    sizes=(128, 256, 512), c0_share=0.0, net=None, mix=0.8):
+                    sizes=(128, 256, 512), c0_share=0.0, net=None, mix=0.8, source="paths"):
     """Training rows from the planner's own solves of seeded batched requests
     (mixed frame sizes, 5-30% obstacles; a share `c0_share` of them the
-    single-instance 256 x 256 layout, start at the centre, goal top centre):
-    one row per expansion on every validated path, with `net` attached at
-    `mix` when given.  Returns device tensors (X: rows x 1040 bf16, labels:
-    int32) and the number of plans solved."""
+    single-instance 256 x 256 layout, start at the centre, goal top centre),
+    with `net` attached at `mix` when given.  source "paths": one row per
+    expansion on every validated path; "nodes": one row per accepted
+    expansion (node of the final graph) of every solved request; "both":
+    the two sets (a path's expansions then appear twice).  Stops at max_rows.
+    Returns device tensors (X: rows x 1040 bf16, labels: int32) and the
+    number of plans solved."""
     import torch
 
     from . import synth
@@ -104,7 +111,10 @@ def collect_dataset(n_plans, seed0=500_000, max_rows=200_000, slots=256, max_ite
                                      seed=seed0 + k, max_iterations=max_iterations))
         valid, _, _, _ = planner.plan(reqs, max_launches=max_iterations + 8, check_every=4)
         solved += int(valid.sum())
-        rows += planner.log_paths(X, labels, rows, max_rows)
+        if source in ("paths", "both"):
+            rows += planner.log_paths(X, labels, rows, max_rows)
+        if source in ("nodes", "both") and rows < max_rows:
+            rows += planner.log_nodes(X, labels, rows, max_rows)
         if rows >= max_rows:
             break
     return X[:rows], labels[:rows], solved
@@ -133,4 +143,28 @@ def evaluate(net, n_plans, seed0, mix=0.5, slots=256, max_iterations=60, sizes=(
             valid.extend(v.tolist())
             loops.extend(lp[:len(reqs)].tolist())
         out[name] = {"valid": np.array(valid), "loops": np.array(loops)}
+    return out
+
+
+def gemm(A, B, trans_a=False, trans_b=False, bias=None, relu=False, mask=None, out=None, M=None,
+         d_count=None):
+    """The network's tcgen05 GEMM on torch CUDA tensors (bf16 A, B; see
+    fastrrt_gemm_bf16): out (M x N, f32 or bf16) = epilogue(A(m, k) B(k, n))
+    with A (M x K), or (K x M) when trans_a; B (N x K) -- a weight matrix --,
+    or (K x N) when trans_b.  Row strides are the tensors' own."""
+    import torch
+    assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16 and A.is_cuda and B.is_cuda
+    K = A.shape[0] if trans_a else A.shape[1]
+    Mx = A.shape[1] if trans_a else A.shape[0]
+    N = B.shape[1] if trans_b else B.shape[0]
+    M = Mx if M is None else M
+    if out is None:
+        out = torch.empty((M, N), dtype=torch.float32, device=A.device)
+    cf = out.data_ptr() if out.dtype == torch.float32 else None
+    cb = out.data_ptr() if out.dtype == torch.bfloat16 else None
+    _lib.check(_lib.lib().fastrrt_gemm_bf16(
+        M, N, K, A.data_ptr(), A.stride(0), int(trans_a), B.data_ptr(), B.stride(0), int(trans_b),
+        None if bias is None else bias.data_ptr(), int(relu), None if mask is None else mask.data_ptr(),
+        0 if mask is None else mask.stride(0), cf, cb, out.stride(0),
+        None if d_count is None else d_count.data_ptr(), torch.cuda.current_stream().cuda_stream), "gemm")
     return out

@@ -1,7 +1,8 @@
 """Trains the learned expansion proposal on the planner's own solves and
 saves its weights (npz of w1, b1, w2, b2, w3, b3).
 
-    python -m fastrrt_b200.train_proposal [--plans N] [--epochs E] [--out PATH]
+    python -m fastrrt_b200.train_proposal [--plans N] [--epochs E] [--source S] [--rows R]
+                                          [--batch B] [--out PATH]
 
 Training rows come from seeded batched requests (mixed 128 / 256 / 512
 frames, 5-30% obstacles, seeds from 500000 on, disjoint from the evaluation
@@ -29,29 +30,50 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--c0-share", type=float, default=0.5)
     ap.add_argument("--rounds", type=int, default=2)
+    ap.add_argument("--source", default="paths", choices=("paths", "nodes", "both"),
+                    help="rows: expansions on validated paths, every accepted expansion, or both")
+    ap.add_argument("--rows", type=int, default=2_000_000, help="rows collected per round at most")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     a = ap.parse_args()
     import torch
 
     from . import proposal as P
     t0 = time.time()
-    X, L, solved = P.collect_dataset(a.plans, seed0=500_000, max_rows=2_000_000, c0_share=a.c0_share)
+    X, L, solved = P.collect_dataset(a.plans, seed0=500_000, max_rows=a.rows, c0_share=a.c0_share,
+                                     source=a.source)
     t1 = time.time()
-    net = P.ProposalNet(seed=a.seed, max_batch=a.batch)
-    loss = net.train(X, L, len(L), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
+    train_s, trained_rows = 0.0, 0
+
+    def train(seed):
+        nonlocal train_s, trained_rows
+        net = P.ProposalNet(seed=seed, max_batch=a.batch)
+        torch.cuda.synchronize()
+        ts = time.time()
+        loss = net.train(X, L, len(L), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=seed)
+        torch.cuda.synchronize()
+        train_s += time.time() - ts
+        trained_rows += (len(L) // a.batch) * a.batch * a.epochs
+        return net, loss
+
+    net, loss = train(a.seed)
     for r in range(1, a.rounds):
-        X2, L2, s2 = P.collect_dataset(a.plans, seed0=500_000 + r * 10_000_000, max_rows=2_000_000,
-                                       c0_share=a.c0_share, net=net)
+        X2, L2, s2 = P.collect_dataset(a.plans, seed0=500_000 + r * 10_000_000, max_rows=a.rows,
+                                       c0_share=a.c0_share, net=net, source=a.source)
         X, L = torch.cat([X, X2]), torch.cat([L, L2])
         solved += s2
-        net = P.ProposalNet(seed=a.seed + r, max_batch=a.batch)
-        loss = net.train(X, L, len(L), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed + r)
+        net, loss = train(a.seed + r)
     t2 = time.time()
+    rows_per_s = trained_rows / max(train_s, 1e-9)
+    tflops = rows_per_s * P.TRAIN_FLOP_PER_ROW / 1e12
     ws = net.get_weights()
     np.savez_compressed(a.out, **{k: w for k, w in zip(["w1", "b1", "w2", "b2", "w3", "b3"], ws)},
-                        rows=len(L), plans=a.plans * a.rounds, solved=solved, loss=loss)
-    print(f"rows {len(L)} from {solved} solved of {a.plans * a.rounds} plans ({t1 - t0:.1f} s), "
-          f"trained {a.epochs} epochs in {t2 - t1:.1f} s, last-batch loss {loss:.3f} -> {a.out}")
+                        rows=len(L), plans=a.plans * a.rounds, solved=solved, loss=loss, source=a.source,
+                        batch=a.batch, epochs=a.epochs, train_s=train_s, train_rows_per_s=rows_per_s,
+                        train_tflops=tflops)
+    print(f"rows {len(L)} ({a.source}) from {solved} solved of {a.plans * a.rounds} plans "
+          f"({t1 - t0:.1f} s to collect the first round), trained {a.epochs} epochs per round in "
+          f"{train_s:.1f} s ({rows_per_s:.3g} rows/s, {tflops:.1f} TFLOP/s), last-batch loss {loss:.3f} "
+          f"-> {a.out}; {t2 - t0:.1f} s in all")
 
 
 def load(net, path=DEFAULT_WEIGHTS):

@@ -363,7 +363,7 @@ int fastrrt_batch_direct_connections(void *batch, int slot, uint8_t *flag, float
 
 /* ---- part 5: the learned expansion proposal ------------------------------
  * No counterpart in the reference.  A BF16 MLP (1030 -> 256 -> 256 -> 128,
- * ReLU, FP32 accumulation, mma.sync tensor-core GEMMs) that proposes the
+ * ReLU, FP32 accumulation, tcgen05 tensor-core GEMMs) that proposes the
  * (steering, length) bin of an expansion from a 32 x 32 obstacle patch around
  * the parent (its heading frame, 2 px stride), the goal in that frame, the
  * distance to the goal, sin / cos of the heading and the steering limit.
@@ -394,10 +394,26 @@ int fastrrt_batch_set_proposal(void *batch, void *mlp, float mix, int cap);
  * offset.. of the device arrays X_bf16 (rows of 1040 bf16) and labels (int32),
  * at most cap rows in all.  Returns the rows written. */
 int fastrrt_batch_log_paths(void *batch, void *X_bf16, int32_t *labels, int offset, int cap);
+/* The same for every accepted expansion of the solved requests of that list:
+ * one row per node of the final graph but the start (features of its parent,
+ * label = the bin of the draw that made it), in no particular order. */
+int fastrrt_batch_log_nodes(void *batch, void *X_bf16, int32_t *labels, int offset, int cap);
 /* Adam training on a device dataset: X_bf16 n x 1040 bf16 rows, labels n
  * int32 (device pointers); *last_loss = mean loss of the last batch */
 int fastrrt_mlp_train(void *mlp, const void *X_bf16, const int32_t *labels, int n, int epochs,
                       int batch, float lr, uint64_t seed, float *last_loss);
+/* The network's GEMM on device buffers (synchronous on `stream`, NULL = the
+ * default stream): C (M x N) = epilogue(sum_k A(m, k) B(k, n)), bf16 operands,
+ * f32 accumulation in TMEM.  A(m, k) = A[m * lda + k], or A[k * lda + m] with
+ * transA; B(k, n) = B[n * ldb + k] (out x in weights), or B[k * ldb + n] with
+ * transB.  Epilogue: + bias[n] (f32, optional), ReLU when relu, times
+ * (mask[m * ldm + n] > 0) when mask (bf16, optional); the result goes to Cf
+ * (f32) or Cb (bf16), exactly one of them, rows ldc apart.  M is capped by
+ * *dM when dM (device int) is given.  A and B start on 16 bytes with lda,
+ * ldb multiples of 8. */
+int fastrrt_gemm_bf16(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb,
+                      int transB, const float *bias, int relu, const void *mask, int ldm, float *Cf, void *Cb,
+                      int ldc, const int *dM, void *stream);
 
 #ifdef __cplusplus
 }

@@ -54,6 +54,15 @@ def test_logged_rows(gpu, torch_gpu):
     assert set(np.unique(patch)).issubset({0.0, 0.5, 1.0})
     assert np.all(x[:, 1030:] == 0)
     assert np.all(np.abs(x[:, 1027] ** 2 + x[:, 1028] ** 2 - 1) < 2e-2)  # sin, cos of the heading
+    # every accepted expansion of the same (deterministic) solves: more rows,
+    # the same form
+    Xn, Ln, solved_n = P.collect_dataset(256, seed0=700_000, max_rows=200_000, max_iterations=60,
+                                         source="nodes")
+    assert solved_n == solved and len(Ln) > len(L)
+    lab = Ln.cpu().numpy()
+    assert lab.min() >= 0 and lab.max() < 128
+    xn = Xn.float().cpu().numpy()
+    assert set(np.unique(xn[:, :1024])).issubset({0.0, 0.5, 1.0}) and np.all(xn[:, 1030:] == 0)
 
 
 def test_trained_proposal_raises_success(gpu, torch_gpu):
