@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--candidates", type=int, default=1 << 20, help="per-candidate microbench size")
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-size legs (C2 batched, C3 served) for short runs")
     ap.add_argument("--plain", type=int, default=256, help="plans of the plain single-instance loop")
     ap.add_argument("--ref-plans", type=int, default=None,
                     help="plans per step of the reference arm (default: one per host core)")
@@ -506,17 +508,31 @@ def c3_serving(args, rank, world, tuned, attach_net):
                        f"{C3_BUDGET >> 30} GB node-grid budget, at most {slots} requests at once",
            "requests_per_rate": n, "size_counts": {str(c[0]): int((sizes == c[0]).sum()) for c in C3_SIZES},
            "slot_bytes": {str(c[0]): F.batch.slot_bytes(c[0], c[0]) for c in C3_SIZES}}
-    for rate in [float(x) for x in args.rates.split(",") if x]:
-        arrival = np.cumsum(rng.exponential(1e3 / rate, n))
-        out = planner.serve(reqs, arrival_ms=arrival, timeout_ms=TIMEOUT_MS, check_every=args.check_every)
-        v = out["valid"] > 0
-        lat = out["latency_ms"][v]
-        res[f"{rate:g}_req_s"] = {
-            "offered": rate, "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
-            "success_rate": float(v.mean()), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
-            "p99_ms": pct(lat, 99),
-            "success_by_size": {str(c[0]): float(v[sizes == c[0]].mean()) for c in C3_SIZES
-                                if (sizes == c[0]).any()}}
+    rates = [float(x) for x in args.rates.split(",") if x]
+    arrivals = {rate: np.cumsum(rng.exponential(1e3 / rate, n)) for rate in rates}
+
+    def rates_block():
+        out_rates = {}
+        for rate in rates:
+            out = planner.serve(reqs, arrival_ms=arrivals[rate], timeout_ms=TIMEOUT_MS,
+                                check_every=args.check_every)
+            v = out["valid"] > 0
+            lat = out["latency_ms"][v]
+            out_rates[f"{rate:g}_req_s"] = {
+                "offered": rate, "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
+                "success_rate": float(v.mean()), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
+                "p99_ms": pct(lat, 99), "mean_loops": float(out["loops"].mean()),
+                "success_by_size": {str(c[0]): float(v[sizes == c[0]].mean()) for c in C3_SIZES
+                                    if (sizes == c[0]).any()}}
+        return out_rates
+
+    # the headline's proposal, then uniform draws on the same arrivals
+    res.update(rates_block())
+    res["proposal"] = "learned" if planner.proposal_attached() else "uniform"
+    if planner.proposal_attached():
+        planner.set_proposal(None)
+        planner.serve(reqs[:min(n, 64)], timeout_ms=TIMEOUT_MS, check_every=args.check_every)
+        res["uniform"] = rates_block()
     budget, used, peak = planner.memory()
     res["memory"] = {"budget_bytes": budget, "peak_bytes_held": peak, "bytes_held_after": used}
     planner.set_proposal(None)
@@ -672,8 +688,8 @@ def run_mine(args, rank, world, local):
     def attach_to(pl):
         pl.set_proposal(net if learned else None, mix=args.mix if learned else 0.0)
 
-    c3 = c3_serving(args, rank, world, tuned, attach_to)
-    c2 = c2_batched(args, rank, world, tuned)
+    c3 = None if args.no_mixed else c3_serving(args, rank, world, tuned, attach_to)
+    c2 = None if args.no_mixed else c2_batched(args, rank, world, tuned)
 
     # kernel timing replay of one step (same inputs, kernels launched one by one)
     planner.profile(True)

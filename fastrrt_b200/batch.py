@@ -207,6 +207,10 @@ class BatchPlanner:
         _lib.check(_lib.lib().fastrrt_batch_set_proposal(self._h, net.handle if net else None,
                                                          float(mix), int(cap)), "batch_set_proposal")
 
+    def proposal_attached(self):
+        """whether a network is attached (set_proposal with a net)"""
+        return getattr(self, "_net", None) is not None
+
     def log_paths(self, X_dev, labels_dev, offset, cap):
         """training rows of the last collected list's valid paths into device
         tensors (X: rows of 1040 bf16, labels: int32); returns rows written"""
