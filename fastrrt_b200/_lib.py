@@ -182,7 +182,8 @@ def lib():
                                         P(C.c_float)]),
         "fastrrt_batch_set_proposal": (C.c_int, [vp, vp, C.c_float, C.c_int]),
         "fastrrt_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int,
-                                        C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp, vp]),
+                                        C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp, vp,
+                                        C.c_uint64, vp]),
         "fastrrt_batch_set_launch": (C.c_int, [vp, C.c_int, C.c_int]),
         "fastrrt_batch_log_paths": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
         "fastrrt_batch_log_nodes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),

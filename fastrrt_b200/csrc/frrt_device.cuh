@@ -65,6 +65,17 @@ __device__ inline void draw_expansion(unsigned long long seed, uint32_t pos, uin
 // ---------------------------------------------------------------------------
 // frame access
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch: a kernel of the iteration graph waits for
+// the kernel before it (completion and memory visibility) before it reads
+// anything, then lets the kernel after it be scheduled, so that kernel's
+// launch overlaps this one's run instead of following its end.  Without a
+// programmatic predecessor the wait returns at once.
+__device__ __forceinline__ void griddep_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ bool bit_xz(const uint32_t *m, int rw, int x, int z)
 {
     return (m[(long)z * rw + (x >> 5)] >> (x & 31)) & 1u;

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace frrt {
@@ -444,6 +445,10 @@ Engine::Engine(int n_slots, int max_w, int max_h, int device, size_t budget_byte
     }
     L_.work_blocks = sms * work_per_sm_;
     L_.sweep_blocks = sms * sweep_per_sm_;
+    // FRRT_NO_PDL=1: every iteration kernel waits for the end of the one
+    // before it (no programmatic dependent launch), for measurement
+    const char *no_pdl = getenv("FRRT_NO_PDL");
+    L_.pdl = (no_pdl && atoi(no_pdl)) ? 0 : 1;
     ok_ = true;
     ok_ = commit();
 }

@@ -492,6 +492,7 @@ void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, 
 // graph_expansion_search_zones.cu:358-368, 461-473)
 __global__ void __launch_bounds__(256) k_scan(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->sweep_total;
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -621,6 +622,7 @@ __device__ void plan_prefix(const Inst *insts, State *states, int n, int which, 
 __global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states, Sched *sc,
                                               int which)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     int *out = which == 0   ? sc->cand_start
                : which == 1 ? sc->node_start
@@ -637,6 +639,7 @@ __global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states,
 // the winner of each claimed cell applies expand_node's transitions
 __global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->cand_start[n];
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -676,6 +679,7 @@ __global__ void __launch_bounds__(256) k_apply(const Inst *insts, State *states,
 // NODE count (erase bound) and region density after the expansion
 __global__ void __launch_bounds__(256) k_post(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->sweep_total;
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -745,6 +749,7 @@ __global__ void __launch_bounds__(256) k_post(const Inst *insts, State *states, 
 // numNodes + 4 hops (graph_collision.cu:32-83; an exhausted walk keeps the node)
 __global__ void __launch_bounds__(256) k_erase(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     // the chunk's non-NULL cells (offsets in the chunk), walked one per thread
     __shared__ uint16_t list[kSweepCells];
     __shared__ int count;
@@ -818,6 +823,7 @@ __global__ void __launch_bounds__(256) k_erase(const Inst *insts, State *states,
 // (graph_collision.cu:84-104)
 __global__ void __launch_bounds__(256) k_setnodes(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->sweep_total;
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -864,6 +870,7 @@ __device__ __forceinline__ void goal_check_node(const Inst &I, State &S, int pos
 
 __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->sweep_total;
     for (int c = blockIdx.x; c < total; c += gridDim.x) {
@@ -952,6 +959,7 @@ __device__ __forceinline__ int window_count(int c, float r, int &lo)
 // over many warps, so the pass costs a few memory round trips at any load.
 __global__ void __launch_bounds__(256) k_gd_demand(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->goal_start[n];
     const int lane = threadIdx.x & 31;
@@ -1034,6 +1042,7 @@ __device__ inline bool coop_probe(const Foot &mine, int leader, int lane, int x,
 // read through L1.
 __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts, State *states, Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->gd_start[n];
     const int lane = threadIdx.x & 31;
@@ -1080,6 +1089,7 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
 // each over 32 lanes.  Masks are read through L1.
 __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states, Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->cand_exact[n];
     const int lane = threadIdx.x & 31;
@@ -1155,6 +1165,7 @@ __device__ __forceinline__ unsigned long long connection_key(long long lc, int c
 // no unit skipped a cell by the bound.  Masks are read through L1.
 __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, State *states, Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->goal_start[n];
     const int lane = threadIdx.x & 31;
@@ -1293,6 +1304,7 @@ __global__ void __launch_bounds__(256, kGoalBlocks) k_goal(const Inst *insts, St
 // among listed nodes with the minimum, the highest node cell index wins
 __global__ void __launch_bounds__(256) k_select(const Inst *insts, State *states, const Sched *sc)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const long entries = (long)sc->node_start[n] * kNodeChunk;
     for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < entries;
@@ -1332,6 +1344,7 @@ __device__ float connection_segment_cost(const Inst &I, int ppos, int cell, int 
 // lane 0 re-run the winning connection's curve)
 __global__ void k_finish(const Inst *insts, State *states, int n)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int slot = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (slot >= n)
@@ -1414,6 +1427,7 @@ const char *const kIterKernelNames[kIterKernels] = {
 __global__ void __launch_bounds__(256) k_prop_list(const Inst *insts, const State *states,
                                                    const Sched *sc, ProposalBufs pb)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
     const int total = sc->cand_start[n];
     const int lane = threadIdx.x & 31;
@@ -1521,6 +1535,7 @@ __device__ void prop_sample_row(const Inst *insts, const State *states, const Pr
 __global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const State *states,
                                                      ProposalBufs pb)
 {
+    griddep_wait();  // the previous kernel of the iteration has finished
     const int lane = threadIdx.x & 31;
     const int rows = min(*pb.count, pb.cap);
     const int warps = (int)((gridDim.x * (long)blockDim.x) >> 5);
@@ -1529,19 +1544,22 @@ __global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const St
 }
 
 void launch_proposal(const Inst *d_inst, State *d_state, const Sched *d_sched, const ProposalBufs &pb,
-                     const Launch &L, cudaStream_t st)
+                     const Launch &L, cudaStream_t st, bool dep)
 {
     cudaMemsetAsync(pb.count, 0, sizeof(int), st);
-    k_prop_list<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched, pb);
-    launch_features(d_inst, pb.cells, pb.slot_of, pb.cap, pb.X, st, pb.count);
-    launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, pb.h1, pb.h2, pb.logits, st);
-    k_prop_sample<<<std::min((pb.cap * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st>>>(d_inst, d_state, pb);
+    launch_dep(dep, k_prop_list, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched, pb);
+    launch_features(d_inst, pb.cells, pb.slot_of, pb.cap, pb.X, st, pb.count, dep);
+    launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, pb.h1, pb.h2, pb.logits, st, dep);
+    launch_dep(dep, k_prop_sample, std::min((pb.cap * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st, d_inst,
+               d_state, pb);
 }
 
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,
                       const Launch &L, cudaStream_t st, cudaEvent_t *ev, const ProposalBufs *pb)
 {
-    const size_t smem = (size_t)L.smem_words * 2 * 4;
+    // programmatic dependent launches, except in the kernel-timing mode
+    // (events between the kernels)
+    const bool dep = L.pdl && !ev;
     int k = 0;
     auto mark = [&]() {
         if (ev)
@@ -1549,42 +1567,42 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
         k++;
     };
     mark();
-    k_scan<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_scan, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 0);
+    launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 0);
     mark();
     if (pb)
-        launch_proposal(d_inst, d_state, d_sched, *pb, L, st);
+        launch_proposal(d_inst, d_state, d_sched, *pb, L, st, dep);
     mark();
-    k_expand<<<L.work_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_expand, L.work_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_apply<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_apply, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_post<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_post, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_erase<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_erase, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_setnodes<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_setnodes, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_accept<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_accept, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 1);
+    launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 1);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 3);
+    launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 3);
     mark();
     // one warp per (node, window chunk): its grid follows the machine, not
     // the frame's sweep chunks (16 for one 256 x 256 slot)
-    k_gd_demand<<<L.sms * 8, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_gd_demand, L.sms * 8, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_plan<<<1, 1024, 0, st>>>(d_inst, d_state, d_sched, 2);
+    launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 2);
     mark();
-    k_gd_eval<<<L.sms * kEvalBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_gd_eval, L.sms * kEvalBlocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_goal<<<L.sms * kGoalBlocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_goal, L.sms * kGoalBlocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_select<<<L.sweep_blocks, 256, 0, st>>>(d_inst, d_state, d_sched);
+    launch_dep(dep, k_select, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    k_finish<<<(n_slots * 32 + 127) / 128, 128, 0, st>>>(d_inst, d_state, n_slots);
+    launch_dep(dep, k_finish, (n_slots * 32 + 127) / 128, 128, 0, st, d_inst, d_state, n_slots);
     mark();
 }
 

@@ -40,7 +40,27 @@ struct Launch {
     int sweep_blocks;         // grid of the sweep kernels
     int work_blocks;          // grid of the persistent expansion / goal kernels
     int smem_words;           // words per mask staged in shared memory (0 = global masks)
+    int pdl = 1;              // iteration kernels launched as programmatic dependents
 };
+
+// a kernel launch, as a programmatic dependent of the previous kernel on the
+// stream when `pdl` (the kernel starts with griddep_wait())
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dep(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
 
 // writes the device clock of the state timestamps (ns) to *d_out
 void launch_clock(long long *d_out, cudaStream_t st);

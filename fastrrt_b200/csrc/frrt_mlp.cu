@@ -2,6 +2,7 @@
 // extraction of the learned expansion proposal (the GEMM is frrt_umma.cu).
 #include "frrt_mlp.cuh"
 #include "frrt_device.cuh"
+#include "frrt_kernels.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -47,20 +48,36 @@ __global__ void k_softmax_xent(const float *logits, const int32_t *labels, int M
     }
 }
 
-__global__ void k_bias_grad(const __nv_bfloat16 *dY, int M, int N, int ld, float *db)
+// db[n] = sum_m dY[m * ld + n]: one block per 32 columns; warp w sums rows
+// w, w + 8, ... (lane = column, coalesced), the warps' partial sums are
+// added in warp order (deterministic)
+__global__ void __launch_bounds__(256) k_bias_grad(const __nv_bfloat16 *dY, int M, int N, int ld, float *db)
 {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N)
-        return;
+    __shared__ float part[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = blockIdx.x * 32 + lane;
     float s = 0.0f;
-    for (int m = 0; m < M; m++)
-        s += __bfloat162float(dY[(long)m * ld + n]);
-    db[n] = s;
+    if (n < N)
+        for (int m = warp; m < M; m += 8)
+            s += __bfloat162float(dY[(long)m * ld + n]);
+    part[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && n < N) {
+        float t = 0.0f;
+        for (int w = 0; w < 8; w++)
+            t += part[w][lane];
+        db[n] = t;
+    }
 }
 
 __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *w16, int n,
-                       float lr, float b1, float b2, float eps, float c1, float c2)
+                       float lr, float b1, float b2, float eps, float c1, float c2, const int *d_step)
 {
+    if (d_step) {  // bias corrections of the device's step number
+        const float t = (float)*d_step;
+        c1 = 1.0f - powf(b1, t);
+        c2 = 1.0f - powf(b2, t);
+    }
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -75,6 +92,12 @@ __global__ void k_adam(float *w, float *m, float *v, const float *g, __nv_bfloat
         w16[i] = __float2bfloat16(wi);
 }
 
+__global__ void k_train_advance(int *d_base, int *d_step, int batch)
+{
+    *d_base += batch;
+    *d_step += 1;
+}
+
 __global__ void k_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -82,15 +105,21 @@ __global__ void k_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n)
         dst[i] = __float2bfloat16(src[i]);
 }
 
+// rows of X (kMlpInPad bf16 = 130 x 16 B) and their labels gathered by index
 __global__ void k_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int32_t *idx,
-                              int n, __nv_bfloat16 *Xb, int32_t *lb)
+                              int n, __nv_bfloat16 *Xb, int32_t *lb, const int *d_base)
 {
     const int r = blockIdx.x;
     if (r >= n)
         return;
-    const long src = (long)idx[r] * kMlpInPad, dst = (long)r * kMlpInPad;
-    for (int c = threadIdx.x; c < kMlpInPad; c += blockDim.x)
-        Xb[dst + c] = X[src + c];
+    if (d_base)
+        idx += *d_base;
+    static_assert(kMlpInPad * 2 % 16 == 0, "feature rows are whole 16-byte vectors");
+    constexpr int kVec = kMlpInPad * 2 / 16;
+    const uint4 *src = reinterpret_cast<const uint4 *>(X + (long)idx[r] * kMlpInPad);
+    uint4 *dst = reinterpret_cast<uint4 *>(Xb + (long)r * kMlpInPad);
+    for (int c = threadIdx.x; c < kVec; c += blockDim.x)
+        dst[c] = src[c];
     if (threadIdx.x == 0)
         lb[r] = labels[idx[r]];
 }
@@ -99,6 +128,7 @@ __global__ void k_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, con
 __global__ void k_features(const Inst *insts, const int32_t *cells, const int32_t *slot_of, int n,
                            __nv_bfloat16 *X, const int *d_count)
 {
+    griddep_wait();  // the candidate list is complete
     const int lane = threadIdx.x & 31;
     if (d_count && *d_count < n)
         n = *d_count;
@@ -163,14 +193,19 @@ void launch_softmax_xent(const float *logits, const int32_t *labels, int M, floa
 
 void launch_bias_grad(const __nv_bfloat16 *dY, int M, int N, int ld, float *db, cudaStream_t st)
 {
-    k_bias_grad<<<(N + 127) / 128, 128, 0, st>>>(dY, M, N, ld, db);
+    k_bias_grad<<<(N + 31) / 32, 256, 0, st>>>(dY, M, N, ld, db);
 }
 
 void launch_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *w16, int n, float lr,
-                 float b1, float b2, float eps, int step, cudaStream_t st)
+                 float b1, float b2, float eps, int step, cudaStream_t st, const int *d_step)
 {
     const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
-    k_adam<<<(n + 255) / 256, 256, 0, st>>>(w, m, v, g, w16, n, lr, b1, b2, eps, c1, c2);
+    k_adam<<<(n + 255) / 256, 256, 0, st>>>(w, m, v, g, w16, n, lr, b1, b2, eps, c1, c2, d_step);
+}
+
+void launch_train_advance(int *d_base, int *d_step, int batch, cudaStream_t st)
+{
+    k_train_advance<<<1, 1, 0, st>>>(d_base, d_step, batch);
 }
 
 void launch_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n, cudaStream_t st)
@@ -179,23 +214,23 @@ void launch_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n, cudaStream_
 }
 
 void launch_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int32_t *idx, int n,
-                        __nv_bfloat16 *Xb, int32_t *lb, cudaStream_t st)
+                        __nv_bfloat16 *Xb, int32_t *lb, cudaStream_t st, const int *d_base)
 {
     if (n > 0)
-        k_gather_rows<<<n, 128, 0, st>>>(X, labels, idx, n, Xb, lb);
+        k_gather_rows<<<n, 128, 0, st>>>(X, labels, idx, n, Xb, lb, d_base);
 }
 
 void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *slot_of, int n,
-                     __nv_bfloat16 *X, cudaStream_t st, const int *d_count)
+                     __nv_bfloat16 *X, cudaStream_t st, const int *d_count, bool dep)
 {
     if (n <= 0)
         return;
-    k_features<<<std::min((n * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st>>>(d_inst, cells, slot_of, n, X,
-                                                                                 d_count);
+    launch_dep(dep, k_features, std::min((n * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st, d_inst, cells,
+               slot_of, n, X, d_count);
 }
 
 void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
-                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st)
+                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st, bool dep)
 {
     GemmArgs g{};
     g.M = n;
@@ -210,7 +245,7 @@ void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, cons
     g.relu = 1;
     g.cb = h1;
     g.ldc = kMlpHidden;
-    launch_gemm(g, st);
+    launch_gemm(g, st, dep);
     g.K = kMlpHidden;
     g.A = h1;
     g.lda = kMlpHidden;
@@ -218,7 +253,7 @@ void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, cons
     g.ldb = kMlpHidden;
     g.bias = w.b2;
     g.cb = h2;
-    launch_gemm(g, st);
+    launch_gemm(g, st, dep);
     g.N = kMlpOut;
     g.A = h2;
     g.B = w.w3;
@@ -227,7 +262,7 @@ void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, cons
     g.cb = nullptr;
     g.cf = logits;
     g.ldc = kMlpOut;
-    launch_gemm(g, st);
+    launch_gemm(g, st, dep);
 }
 
 }  // namespace frrt

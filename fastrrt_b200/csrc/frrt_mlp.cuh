@@ -52,11 +52,18 @@ struct GemmArgs {
     float *cf;
     __nv_bfloat16 *cb;
     int ldc;
+    // optional f32 workspace (split_floats floats) for a split over K: a raw
+    // f32 GEMM (no bias, ReLU or mask) of few output tiles and a long K is
+    // computed as partial sums of K ranges by more CTAs, then reduced in a
+    // fixed order (deterministic)
+    float *split_ws;
+    size_t split_floats;
 };
 // on the 5th-generation tensor cores (frrt_umma.cu); a launch that cannot be
 // made, or a block whose pipeline wait ran out, leaves an error for
-// gemm_take_error()
-void launch_gemm(const GemmArgs &g, cudaStream_t st);
+// gemm_take_error().  dep: launched as a programmatic dependent of the
+// previous kernel on the stream
+void launch_gemm(const GemmArgs &g, cudaStream_t st, bool dep = false);
 // the GEMM's runtime (driver tensor-map entry point, kernel attributes,
 // error flag); false when it cannot run here
 bool umma_init();
@@ -70,18 +77,24 @@ void launch_softmax_xent(const float *logits, const int32_t *labels, int M, floa
                          __nv_bfloat16 *dlogits, float *loss, cudaStream_t st);
 // db[n] = sum_m dY[m * ld + n] (bf16 in, f32 out)
 void launch_bias_grad(const __nv_bfloat16 *dY, int M, int N, int ld, float *db, cudaStream_t st);
-// Adam on f32 master weights; refreshes the bf16 copy
+// Adam on f32 master weights; refreshes the bf16 copy.  The step number
+// (for the bias corrections) is `step`, or *d_step when d_step is given (a
+// captured training step reads it on the device)
 void launch_adam(float *w, float *m, float *v, const float *g, __nv_bfloat16 *w16, int n, float lr,
-                 float b1, float b2, float eps, int step, cudaStream_t st);
+                 float b1, float b2, float eps, int step, cudaStream_t st, const int *d_step = nullptr);
 void launch_f32_to_bf16(const float *src, __nv_bfloat16 *dst, int n, cudaStream_t st);
-// X rows and labels of a minibatch gathered by index
+// X rows and labels of a minibatch gathered by index: idx[*d_base + r] when
+// d_base is given (a captured training step reads its batch offset on the
+// device), else idx[r]
 void launch_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int32_t *idx, int n,
-                        __nv_bfloat16 *Xb, int32_t *lb, cudaStream_t st);
+                        __nv_bfloat16 *Xb, int32_t *lb, cudaStream_t st, const int *d_base = nullptr);
+// the end of a captured training step: *d_base += batch, *d_step += 1
+void launch_train_advance(int *d_base, int *d_step, int batch, cudaStream_t st);
 
 // the network's forward pass: logits (n x 128, f32) of X (n x kMlpInPad);
 // d_count, when given, caps n on the device
 void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
-                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st);
+                        __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st, bool dep = false);
 
 // Buffers of the proposal step inside a planning iteration (cap rows).
 struct ProposalBufs {
@@ -100,7 +113,7 @@ struct ProposalBufs {
 // the goal, sin / cos of the heading and the steering limit; bf16, rows of
 // kMlpInPad (zero padded).  cells[k] / slots[k] name the parent.
 void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *slot_of, int n,
-                     __nv_bfloat16 *X, cudaStream_t st, const int *d_count = nullptr);
+                     __nv_bfloat16 *X, cudaStream_t st, const int *d_count = nullptr, bool dep = false);
 
 // The (steering, length) bin of a draw, the training label
 __host__ __device__ inline int proposal_bin(float steer, float len, float max_steer, float max_path)

@@ -49,7 +49,11 @@ private:
     __nv_bfloat16 *x_ = nullptr, *h1_ = nullptr, *h2_ = nullptr, *dl_ = nullptr, *dh2_ = nullptr,
                   *dh1_ = nullptr;
     float *logits_ = nullptr, *loss_ = nullptr, *xf_ = nullptr;
-    int32_t *labels_ = nullptr, *idx_ = nullptr;
+    int32_t *labels_ = nullptr;
+    float *split_ws_ = nullptr;  // the weight gradients' split-over-K partial sums
+    int32_t *perm_ = nullptr;    // an epoch's row order on the device
+    int perm_cap_ = 0;
+    int *ctl_ = nullptr;         // captured training step: batch offset, step number
 };
 
 }  // namespace frrt

@@ -42,6 +42,10 @@ bool gemm_ok()
 
 }  // namespace
 
+// workspace of the weight gradients' split over K: at most 16 splits of the
+// largest gradient (256 x 1040)
+constexpr size_t kSplitFloats = 16 * (size_t)kMlpHidden * kMlpInPad;
+
 const size_t Mlp::kSizes[6] = {(size_t)kMlpHidden * kMlpInPad, kMlpHidden,
                                (size_t)kMlpHidden * kMlpHidden, kMlpHidden,
                                (size_t)kMlpOut * kMlpHidden,    kMlpOut};
@@ -68,8 +72,8 @@ Mlp::Mlp(uint64_t seed, int max_batch) : max_batch_(max_batch)
     const size_t B = (size_t)max_batch;
     ok = ok && dalloc(x_, B * kMlpInPad) && dalloc(h1_, B * kMlpHidden) && dalloc(h2_, B * kMlpHidden) &&
          dalloc(logits_, B * kMlpOut) && dalloc(dl_, B * kMlpOut) && dalloc(dh2_, B * kMlpHidden) &&
-         dalloc(dh1_, B * kMlpHidden) && dalloc(labels_, B) && dalloc(loss_, 1) && dalloc(idx_, B) &&
-         dalloc(xf_, B * kMlpInPad);
+         dalloc(dh1_, B * kMlpHidden) && dalloc(labels_, B) && dalloc(loss_, 1) &&
+         dalloc(xf_, B * kMlpInPad) && dalloc(split_ws_, kSplitFloats);
     if (!ok) {
         set_error("mlp: device allocation failed");
         return;
@@ -114,8 +118,10 @@ Mlp::~Mlp()
     cudaFree(dh1_);
     cudaFree(labels_);
     cudaFree(loss_);
-    cudaFree(idx_);
     cudaFree(xf_);
+    cudaFree(split_ws_);
+    cudaFree(perm_);
+    cudaFree(ctl_);
     if (stream_)
         cudaStreamDestroy(stream_);
 }
@@ -150,6 +156,7 @@ void Mlp::backward(int n)
     g.A = dl_; g.lda = kMlpOut; g.transA = 1;
     g.B = h2_; g.ldb = kMlpHidden; g.transB = 1;
     g.cf = g_[4]; g.ldc = kMlpHidden;
+    g.split_ws = split_ws_; g.split_floats = kSplitFloats;
     launch_gemm(g, stream_);
     launch_bias_grad(dl_, n, kMlpOut, kMlpOut, g_[5], stream_);
     // dH2 = dL W3 * (H2 > 0)
@@ -166,6 +173,7 @@ void Mlp::backward(int n)
     g.A = dh2_; g.lda = kMlpHidden; g.transA = 1;
     g.B = h1_; g.ldb = kMlpHidden; g.transB = 1;
     g.cf = g_[2]; g.ldc = kMlpHidden;
+    g.split_ws = split_ws_; g.split_floats = kSplitFloats;
     launch_gemm(g, stream_);
     launch_bias_grad(dh2_, n, kMlpHidden, kMlpHidden, g_[3], stream_);
     // dH1 = dH2 W2 * (H1 > 0)
@@ -182,6 +190,7 @@ void Mlp::backward(int n)
     g.A = dh1_; g.lda = kMlpHidden; g.transA = 1;
     g.B = x_; g.ldb = kMlpInPad; g.transB = 1;
     g.cf = g_[0]; g.ldc = kMlpInPad;
+    g.split_ws = split_ws_; g.split_floats = kSplitFloats;
     launch_gemm(g, stream_);
     launch_bias_grad(dh1_, n, kMlpHidden, kMlpHidden, g_[1], stream_);
 }
@@ -224,27 +233,59 @@ bool Mlp::train(const __nv_bfloat16 *X, const int32_t *labels, int n_total, int 
     }
     std::mt19937_64 rng(seed);
     std::vector<int32_t> perm(n_total);
+    if (n_total > perm_cap_) {
+        cudaFree(perm_);
+        perm_ = nullptr;
+        perm_cap_ = 0;
+        if (!cuda_ok(cudaMalloc(&perm_, sizeof(int32_t) * (size_t)n_total), "permutation"))
+            return false;
+        perm_cap_ = n_total;
+    }
+    if (!ctl_ && !cuda_ok(cudaMalloc(&ctl_, 2 * sizeof(int)), "training control"))
+        return false;
+    // One training step as a CUDA graph: the gather of the batch (its offset
+    // in the epoch's order, ctl_[0], read on the device), forward, backward,
+    // Adam (the step number ctl_[1] read on the device) and the advance of
+    // both; one graph launch per batch.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (!cuda_ok(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "step capture"))
+        return false;
+    launch_gather_rows(X, labels, perm_, batch, x_, labels_, stream_, ctl_);
+    backward(batch);
+    for (int t = 0; t < 6; t++)
+        launch_adam(w_[t], m_[t], v_[t], g_[t], (t % 2 == 0) ? w16_[t / 2] : nullptr, (int)kSizes[t], lr,
+                    0.9f, 0.999f, 1e-8f, 1, stream_, ctl_ + 1);
+    launch_train_advance(ctl_, ctl_ + 1, batch, stream_);
+    const cudaError_t cap = cudaStreamEndCapture(stream_, &graph);
+    if (!cuda_ok(cap, "step capture") || !cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "step graph")) {
+        if (graph)
+            cudaGraphDestroy(graph);
+        return false;
+    }
+    cudaGraphDestroy(graph);
     float loss = 0.0f;
-    for (int e = 0; e < epochs; e++) {
+    bool ok = true;
+    for (int e = 0; e < epochs && ok; e++) {
         for (int i = 0; i < n_total; i++)
             perm[i] = i;
         std::shuffle(perm.begin(), perm.end(), rng);
-        for (int b0 = 0; b0 + batch <= n_total; b0 += batch) {
-            if (!cuda_ok(cudaMemcpyAsync(idx_, perm.data() + b0, sizeof(int32_t) * batch,
-                                         cudaMemcpyHostToDevice, stream_), "index upload"))
-                return false;
-            launch_gather_rows(X, labels, idx_, batch, x_, labels_, stream_);
-            if (!step(batch, lr))
-                return false;
+        // the epoch's order goes to the device once; each batch gathers its rows
+        const int ctl[2] = {0, step_ + 1};
+        ok = cuda_ok(cudaMemcpyAsync(perm_, perm.data(), sizeof(int32_t) * (size_t)n_total,
+                                     cudaMemcpyHostToDevice, stream_), "permutation upload") &&
+             cuda_ok(cudaMemcpyAsync(ctl_, ctl, sizeof(ctl), cudaMemcpyHostToDevice, stream_), "step control");
+        for (int b0 = 0; ok && b0 + batch <= n_total; b0 += batch) {
+            ok = cuda_ok(cudaGraphLaunch(exec, stream_), "train step");
+            step_++;
         }
-        if (!cuda_ok(cudaMemcpyAsync(&loss, loss_, sizeof(float), cudaMemcpyDeviceToHost, stream_),
-                     "loss") ||
-            !cuda_ok(cudaStreamSynchronize(stream_), "epoch") || !gemm_ok())
-            return false;
+        ok = ok && cuda_ok(cudaMemcpyAsync(&loss, loss_, sizeof(float), cudaMemcpyDeviceToHost, stream_), "loss") &&
+             cuda_ok(cudaStreamSynchronize(stream_), "epoch") && gemm_ok();
     }
-    if (last_loss)
+    cudaGraphExecDestroy(exec);
+    if (ok && last_loss)
         *last_loss = loss / batch;
-    return true;
+    return ok;
 }
 
 }  // namespace frrt
@@ -333,7 +374,7 @@ int fastrrt_mlp_gradients(void *mlp, int n, const float *X, const int32_t *label
 
 int fastrrt_gemm_bf16(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb,
                       int transB, const float *bias, int relu, const void *mask, int ldm, float *Cf, void *Cb,
-                      int ldc, const int *dM, void *stream)
+                      int ldc, const int *dM, float *split_ws, uint64_t split_floats, void *stream)
 {
     if (M < 0 || N < 0 || K <= 0 || !A || !B || (!Cf) == (!Cb) || ldc < N ||
         lda < (transA ? M : K) || ldb < (transB ? N : K) || (mask && ldm < N)) {
@@ -360,6 +401,8 @@ int fastrrt_gemm_bf16(int M, int N, int K, const void *A, int lda, int transA, c
     g.cf = Cf;
     g.cb = static_cast<__nv_bfloat16 *>(Cb);
     g.ldc = ldc;
+    g.split_ws = split_ws;
+    g.split_floats = split_ws ? (size_t)split_floats : 0;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     launch_gemm(g, st);
     return cuda_ok(cudaGetLastError(), "gemm launch") && cuda_ok(cudaStreamSynchronize(st), "gemm") &&

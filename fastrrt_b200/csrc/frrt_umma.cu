@@ -25,13 +25,18 @@
 #include <mutex>
 
 #include "frrt_device.cuh"
+#include "frrt_kernels.cuh"
 #include "frrt_mlp.cuh"
 
 namespace frrt {
 
 namespace {
 
-constexpr int kUM = 128, kUN = 128, kUK = 64, kUStages = 4;
+// stages of the operand ring (32 KB each; a build-time knob for measurement)
+#ifndef FRRT_UMMA_STAGES
+#define FRRT_UMMA_STAGES 4
+#endif
+constexpr int kUM = 128, kUN = 128, kUK = 64, kUStages = FRRT_UMMA_STAGES;
 constexpr int kUOpBytes = kUM * kUK * 2;  // one operand tile of one stage: 16 KB
 constexpr int kUThreads = 192;
 constexpr int kUTmemCols = 2 * kUN;       // two accumulators of 128 f32 columns
@@ -49,6 +54,7 @@ struct UmmaParams {
     __nv_bfloat16 *cb;
     int ldc;
     int vec;  // rows of C and of the mask start on 16-byte boundaries
+    int splits, kb_per;  // K split: partial sums of kb_per k-blocks each, into cf + split * M * ldc
     int *err;
 };
 
@@ -234,6 +240,7 @@ __device__ __forceinline__ void store_chunk(const UmmaParams &p, int row, int n,
 __global__ void __launch_bounds__(kUThreads, 1)
     k_umma(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, UmmaParams p)
 {
+    griddep_wait();  // the producer of A (and of the row count) has finished
     extern __shared__ uint8_t smem_raw[];
     const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
     UmmaSmem &S = *reinterpret_cast<UmmaSmem *>(smem_raw + pad);
@@ -244,7 +251,13 @@ __global__ void __launch_bounds__(kUThreads, 1)
         M = c < M ? c : M;
     }
     const int ntn = (p.N + kUN - 1) / kUN, ntm = (M + kUM - 1) / kUM;
-    const int ntiles = ntm * ntn, nk = (p.K + kUK - 1) / kUK;
+    const int nk = (p.K + kUK - 1) / kUK;
+    const int ntiles_mn = ntm * ntn, ntiles = ntiles_mn * p.splits;
+    // work unit t: K split t / ntiles_mn, output tile t % ntiles_mn (N fastest)
+    auto k_range = [&](int t, int &kb0, int &kb1) {
+        kb0 = (t / ntiles_mn) * p.kb_per;
+        kb1 = min(nk, kb0 + p.kb_per);
+    };
     if (threadIdx.x == 0) {
         for (int s = 0; s < kUStages; s++) {
             mbar_init(&S.full[s], 1);
@@ -275,8 +288,11 @@ __global__ void __launch_bounds__(kUThreads, 1)
         // TMA producer
         long it = 0;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            const int m0 = (t / ntn) * kUM, n0 = (t % ntn) * kUN;
-            for (int kb = 0; kb < nk; kb++) {
+            const int tm = t % ntiles_mn;
+            const int m0 = (tm / ntn) * kUM, n0 = (tm % ntn) * kUN;
+            int kb0, kb1;
+            k_range(t, kb0, kb1);
+            for (int kb = kb0; kb < kb1; kb++) {
                 const int s = (int)(it % kUStages);
                 const long round = it / kUStages;
                 if (round > 0 && !wait_bounded(&S.empty[s], (unsigned)((round - 1) & 1), abort)) {
@@ -318,7 +334,9 @@ __global__ void __launch_bounds__(kUThreads, 1)
             }
             tc_fence_after();
             const uint32_t d = tbase + (uint32_t)(b * kUN);
-            for (int kb = 0; kb < nk; kb++, it++) {
+            int kb0, kb1;
+            k_range(t, kb0, kb1);
+            for (int kb = kb0; kb < kb1; kb++, it++) {
                 const int s = (int)(it % kUStages);
                 if (!wait_bounded(&S.full[s], (unsigned)((it / kUStages) & 1), abort)) {
                     ok = false;
@@ -330,7 +348,7 @@ __global__ void __launch_bounds__(kUThreads, 1)
                 for (int kk = 0; kk < kUK / 16; kk++) {
                     const uint64_t ad = p.a_mn ? smem_desc(sa + kk * 2048, 8192, 1024) : smem_desc(sa + kk * 32, 16, 1024);
                     const uint64_t bd = p.b_mn ? smem_desc(sb + kk * 2048, 8192, 1024) : smem_desc(sb + kk * 32, 16, 1024);
-                    umma_bf16(d, ad, bd, idesc, (uint32_t)(kb | kk));
+                    umma_bf16(d, ad, bd, idesc, (uint32_t)((kb - kb0) | kk));
                 }
                 issued = true;
                 umma_commit(&S.empty[s]);
@@ -353,14 +371,18 @@ __global__ void __launch_bounds__(kUThreads, 1)
                 break;
             }
             tc_fence_after();
-            const int m0 = (t / ntn) * kUM, n0 = (t % ntn) * kUN;
+            const int tm = t % ntiles_mn;
+            const int m0 = (tm / ntn) * kUM, n0 = (tm % ntn) * kUN;
             const int row = m0 + warp * 32 + lane;
             const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * kUN);
+            UmmaParams q = p;
+            if (p.splits > 1)  // this split's partial sums
+                q.cf = p.cf + (long)(t / ntiles_mn) * p.M * p.ldc;
             for (int c0 = 0; c0 < kUN && n0 + c0 < p.N; c0 += 32) {
                 uint32_t r[32];
                 tmem_ld32(taddr + (uint32_t)c0, r);
                 if (row < M)
-                    store_chunk(p, row, n0 + c0, r);
+                    store_chunk(q, row, n0 + c0, r);
             }
             tc_fence_before();
             mbar_arrive(&S.tempty[b]);
@@ -376,6 +398,20 @@ __global__ void __launch_bounds__(kUThreads, 1)
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kUTmemCols)
                      : "memory");
+    }
+}
+
+// C[m][n] = sum over splits s (in order) of ws[s][m][n] (rows of N floats)
+__global__ void __launch_bounds__(256) k_split_reduce(const float *ws, int splits, int M, int N, float *C,
+                                                      int ldc)
+{
+    const long total = (long)M * N;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int k = 0; k < splits; k++)
+            s += ws[(long)k * total + i];
+        const long m = i / N;
+        C[m * ldc + (i - m * N)] = s;
     }
 }
 
@@ -466,7 +502,7 @@ void fail(const char *msg)
 }
 }  // namespace
 
-void launch_gemm(const GemmArgs &g, cudaStream_t st)
+void launch_gemm(const GemmArgs &g, cudaStream_t st, bool dep)
 {
     if (g.M <= 0 || g.N <= 0)
         return;
@@ -502,9 +538,31 @@ void launch_gemm(const GemmArgs &g, cudaStream_t st)
     p.vec = aligned16(g.cf ? (const void *)g.cf : (const void *)g.cb) && g.ldc % 8 == 0 &&
             (!g.mask || (aligned16(g.mask) && g.ldm % 8 == 0));
     p.err = rt.d_err;
+    p.splits = 1;
     const long tiles = (long)((g.M + kUM - 1) / kUM) * ((g.N + kUN - 1) / kUN);
-    const int grid = (int)std::min<long>(tiles, rt.sms);
-    k_umma<<<grid, kUThreads, kUSmemBytes, st>>>(ta, tb, p);
+    const int nk = (g.K + kUK - 1) / kUK;
+    p.kb_per = nk;
+    // split over K: a raw f32 result with fewer tiles than half the SMs and
+    // at least 8 k-blocks, into the caller's workspace
+    if (g.split_ws && g.cf && !g.bias && !g.relu && !g.mask && !g.dM && 2 * tiles < rt.sms && nk >= 8) {
+        int s = (int)std::min<long>(std::min<long>(nk / 4, rt.sms / tiles), 16);
+        const int per = (nk + s - 1) / s;
+        s = (nk + per - 1) / per;  // no empty split
+        if (s > 1 && (size_t)s * g.M * g.N <= g.split_floats) {
+            p.splits = s;
+            p.kb_per = per;
+            p.cf = g.split_ws;
+            p.ldc = g.N;
+            p.vec = g.N % 8 == 0 && aligned16(g.split_ws);
+        }
+    }
+    const int grid = (int)std::min<long>(tiles * p.splits, rt.sms);
+    launch_dep(dep, k_umma, grid, kUThreads, kUSmemBytes, st, ta, tb, p);
+    if (p.splits > 1) {
+        const long total = (long)g.M * g.N;
+        k_split_reduce<<<(int)std::min<long>((total + 255) / 256, (long)rt.sms * 8), 256, 0, st>>>(
+            g.split_ws, p.splits, g.M, g.N, g.cf, g.ldc);
+    }
 }
 
 }  // namespace frrt

@@ -147,11 +147,12 @@ def evaluate(net, n_plans, seed0, mix=0.5, slots=256, max_iterations=60, sizes=(
 
 
 def gemm(A, B, trans_a=False, trans_b=False, bias=None, relu=False, mask=None, out=None, M=None,
-         d_count=None):
+         d_count=None, split_ws=None):
     """The network's tcgen05 GEMM on torch CUDA tensors (bf16 A, B; see
     fastrrt_gemm_bf16): out (M x N, f32 or bf16) = epilogue(A(m, k) B(k, n))
     with A (M x K), or (K x M) when trans_a; B (N x K) -- a weight matrix --,
-    or (K x N) when trans_b.  Row strides are the tensors' own."""
+    or (K x N) when trans_b.  Row strides are the tensors' own.  split_ws: an
+    f32 CUDA tensor for the split over K of a raw f32 product."""
     import torch
     assert A.dtype == torch.bfloat16 and B.dtype == torch.bfloat16 and A.is_cuda and B.is_cuda
     K = A.shape[0] if trans_a else A.shape[1]
@@ -166,5 +167,6 @@ def gemm(A, B, trans_a=False, trans_b=False, bias=None, relu=False, mask=None, o
         M, N, K, A.data_ptr(), A.stride(0), int(trans_a), B.data_ptr(), B.stride(0), int(trans_b),
         None if bias is None else bias.data_ptr(), int(relu), None if mask is None else mask.data_ptr(),
         0 if mask is None else mask.stride(0), cf, cb, out.stride(0),
-        None if d_count is None else d_count.data_ptr(), torch.cuda.current_stream().cuda_stream), "gemm")
+        None if d_count is None else d_count.data_ptr(), None if split_ws is None else split_ws.data_ptr(),
+        0 if split_ws is None else split_ws.numel(), torch.cuda.current_stream().cuda_stream), "gemm")
     return out

@@ -410,10 +410,12 @@ int fastrrt_mlp_train(void *mlp, const void *X_bf16, const int32_t *labels, int 
  * (mask[m * ldm + n] > 0) when mask (bf16, optional); the result goes to Cf
  * (f32) or Cb (bf16), exactly one of them, rows ldc apart.  M is capped by
  * *dM when dM (device int) is given.  A and B start on 16 bytes with lda,
- * ldb multiples of 8. */
+ * ldb multiples of 8.  split_ws (device, split_floats floats, optional): a
+ * raw f32 product of few output tiles and a long K is split over K into
+ * partial sums there and reduced in a fixed order. */
 int fastrrt_gemm_bf16(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb,
                       int transB, const float *bias, int relu, const void *mask, int ldm, float *Cf, void *Cb,
-                      int ldc, const int *dM, void *stream);
+                      int ldc, const int *dM, float *split_ws, uint64_t split_floats, void *stream);
 
 #ifdef __cplusplus
 }

@@ -113,3 +113,21 @@ def test_gemm_rejects_unaligned_strides(T, gpu):
     B = T.zeros((32, 99), dtype=T.bfloat16, device="cuda")             # 198-byte rows: not a TMA stride
     with pytest.raises(gpu.FastRRTError):
         gemm(A, B)
+
+
+@pytest.mark.parametrize("M,N,K", [(256, 1040, 4096), (128, 256, 4096), (256, 256, 1000)])
+def test_gemm_split_over_k(T, M, N, K):
+    """weight-gradient shapes (both operands MN-major, few output tiles, long
+    K) split over K into the workspace and reduced in a fixed order: the
+    float64 bound holds and two runs are bit-identical"""
+    from fastrrt_b200.proposal import gemm
+    rng = np.random.default_rng(M + N + K)
+    A, B, Am, Bm = operands(T, rng, M, N, K, 1, 1)
+    ws = T.empty(16 * M * N, dtype=T.float32, device="cuda")
+    got = gemm(A, B, trans_a=True, trans_b=True, split_ws=ws)
+    check(got, Am @ Bm, Am.abs() @ Bm.abs(), False)
+    again = gemm(A, B, trans_a=True, trans_b=True, split_ws=ws)
+    assert T.equal(got, again)
+    # too small a workspace: the unsplit product, within the same bound
+    small = gemm(A, B, trans_a=True, trans_b=True, split_ws=ws[:M * N])
+    check(small, Am @ Bm, Am.abs() @ Bm.abs(), False)
