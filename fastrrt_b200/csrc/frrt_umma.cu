@@ -430,6 +430,8 @@ struct UmmaRuntime {
     const char *host_err = nullptr;  // the first launch error since the last check
 };
 
+// set up once per process, for the device current at the first call (one
+// device per process, as the library's planners are used)
 UmmaRuntime &runtime()
 {
     static UmmaRuntime rt;
