@@ -478,8 +478,6 @@ Engine::~Engine()
     cudaFree(pb_.idx);
     cudaFree(pb_.count);
     cudaFree(pb_.X);
-    cudaFree(pb_.h1);
-    cudaFree(pb_.h2);
     cudaFree(pb_.logits);
     cudaFree(d_log_cells_);
     cudaFree(d_log_slots_);
@@ -1226,8 +1224,6 @@ bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
         cudaFree(pb_.idx);
         cudaFree(pb_.count);
         cudaFree(pb_.X);
-        cudaFree(pb_.h1);
-        cudaFree(pb_.h2);
         cudaFree(pb_.logits);
         pb_ = ProposalBufs{};
         const size_t c = (size_t)cap;
@@ -1236,8 +1232,6 @@ bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
             !check(cudaMalloc(&pb_.idx, 4 * c), "proposal buffers") ||
             !check(cudaMalloc(&pb_.count, sizeof(int)), "proposal buffers") ||
             !check(cudaMalloc(&pb_.X, 2 * c * kMlpInPad), "proposal buffers") ||
-            !check(cudaMalloc(&pb_.h1, 2 * c * kMlpHidden), "proposal buffers") ||
-            !check(cudaMalloc(&pb_.h2, 2 * c * kMlpHidden), "proposal buffers") ||
             !check(cudaMalloc(&pb_.logits, 4 * c * kMlpOut), "proposal buffers"))
             return false;
         pb_.cap = cap;

@@ -1549,7 +1549,7 @@ void launch_proposal(const Inst *d_inst, State *d_state, const Sched *d_sched, c
     cudaMemsetAsync(pb.count, 0, sizeof(int), st);
     launch_dep(dep, k_prop_list, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched, pb);
     launch_features(d_inst, pb.cells, pb.slot_of, pb.cap, pb.X, st, pb.count, dep);
-    launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, pb.h1, pb.h2, pb.logits, st, dep);
+    launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, nullptr, nullptr, pb.logits, st, dep);
     launch_dep(dep, k_prop_sample, std::min((pb.cap * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st, d_inst,
                d_state, pb);
 }

@@ -232,37 +232,7 @@ void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *sl
 void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
                         __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st, bool dep)
 {
-    GemmArgs g{};
-    g.M = n;
-    g.dM = d_count;
-    g.N = kMlpHidden;
-    g.K = kMlpInPad;
-    g.A = X;
-    g.lda = kMlpInPad;
-    g.B = w.w1;
-    g.ldb = kMlpInPad;
-    g.bias = w.b1;
-    g.relu = 1;
-    g.cb = h1;
-    g.ldc = kMlpHidden;
-    launch_gemm(g, st, dep);
-    g.K = kMlpHidden;
-    g.A = h1;
-    g.lda = kMlpHidden;
-    g.B = w.w2;
-    g.ldb = kMlpHidden;
-    g.bias = w.b2;
-    g.cb = h2;
-    launch_gemm(g, st, dep);
-    g.N = kMlpOut;
-    g.A = h2;
-    g.B = w.w3;
-    g.bias = w.b3;
-    g.relu = 0;
-    g.cb = nullptr;
-    g.cf = logits;
-    g.ldc = kMlpOut;
-    launch_gemm(g, st, dep);
+    launch_mlp_fused(w, X, n, d_count, h1, h2, logits, st, dep);
 }
 
 }  // namespace frrt

@@ -92,9 +92,14 @@ void launch_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, const int
 void launch_train_advance(int *d_base, int *d_step, int batch, cudaStream_t st);
 
 // the network's forward pass: logits (n x 128, f32) of X (n x kMlpInPad);
-// d_count, when given, caps n on the device
+// d_count, when given, caps n on the device; the hidden activations go to h1
+// / h2 when they are not null (training's backward pass reads them).  One
+// kernel (frrt_umma.cu): the activations stay in shared memory between the
+// layers.
 void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
                         __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st, bool dep = false);
+void launch_mlp_fused(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
+                      __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st, bool dep);
 
 // Buffers of the proposal step inside a planning iteration (cap rows).
 struct ProposalBufs {
@@ -102,7 +107,7 @@ struct ProposalBufs {
     float mix;                 // probability of sampling from the network (else uniform)
     int32_t *cells, *slot_of, *idx;
     int *count;                // candidates listed this iteration (may exceed cap)
-    __nv_bfloat16 *X, *h1, *h2;
+    __nv_bfloat16 *X;
     float *logits;
     MlpWeights w;
 };

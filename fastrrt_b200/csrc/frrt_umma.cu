@@ -415,6 +415,256 @@ __global__ void __launch_bounds__(256) k_split_reduce(const float *ws, int split
     }
 }
 
+// ---------------------------------------------------------------------------
+// The network's forward pass in one kernel (the planner's proposal step):
+// per 128-row tile, layer 1 streams X and W1 through a 3-stage TMA ring into
+// one N = 256 accumulator; the epilogue writes bias + ReLU as bf16 into a
+// shared-memory activation tile in the 128-byte-swizzled K-major layout the
+// tensor core reads (the layout TMA writes), layer 2 takes its A operand from
+// there and W2 from the ring, layer 3 likewise with W3, and the epilogue
+// writes the logits.  The hidden activations go to global memory only when
+// asked (training needs them).  Same instruction sequence per output element
+// as three launches of k_umma, so the same results.
+// ---------------------------------------------------------------------------
+
+constexpr int kFStages = 3;
+constexpr int kFK1 = (kMlpInPad + kUK - 1) / kUK;  // 17 k-blocks of layer 1
+constexpr int kFK2 = kMlpHidden / kUK;             // 4 of layers 2 and 3
+constexpr int kFUnits = kFK1 + 2 * kFK2;           // ring stages per tile
+constexpr int kFTmemCols = kMlpHidden;             // one 128 x 256 f32 accumulator
+
+struct FusedParams {
+    int M;
+    const int *dM;
+    const float *b1, *b2, *b3;
+    __nv_bfloat16 *h1, *h2;  // optional copies of the activations
+    float *logits;
+    int *err;
+};
+
+struct FusedSmem {
+    __nv_bfloat16 a[kFStages][kUM * kUK];          // X tiles (layer 1)
+    __nv_bfloat16 b[kFStages][kMlpHidden * kUK];   // weight tiles
+    __nv_bfloat16 act[kMlpHidden / kUK][kUM * kUK]; // h1, then h2: 4 swizzled K-blocks
+    uint64_t full[kFStages], empty[kFStages], acc_full, acc_free, act_ready, drain;
+    uint32_t tmem_base;
+    int abort;
+};
+constexpr size_t kFSmemBytes = sizeof(FusedSmem) + 1024;
+
+__host__ __device__ constexpr uint32_t instr_desc_n(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kUM >> 4) << 24);
+}
+
+// bytes a ring stage of unit j (0 .. kFUnits - 1) receives
+__device__ __forceinline__ unsigned fused_unit_bytes(int j)
+{
+    if (j < kFK1)
+        return (unsigned)(kUM * kUK * 2 + kMlpHidden * kUK * 2);
+    if (j < kFK1 + kFK2)
+        return (unsigned)(kMlpHidden * kUK * 2);
+    return (unsigned)(kMlpOut * kUK * 2);
+}
+
+// the epilogue's 32 columns c0 .. c0 + 31 of its row as bias + ReLU bf16:
+// into the activation tile (128-byte swizzle: 16-byte chunk q of row r at
+// chunk q ^ (r & 7)) and, when asked, to global memory
+__device__ __forceinline__ void fused_store_act(FusedSmem &S, int r, int c0, const uint32_t (&v)[32],
+                                                const float *bias, __nv_bfloat16 *gout, int row, int M)
+{
+    uint32_t w[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+        const float lo = fmaxf(__uint_as_float(v[2 * e]) + bias[c0 + 2 * e], 0.0f);
+        const float hi = fmaxf(__uint_as_float(v[2 * e + 1]) + bias[c0 + 2 * e + 1], 0.0f);
+        w[e] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16(lo)) |
+               ((uint32_t)__bfloat16_as_ushort(__float2bfloat16(hi)) << 16);
+    }
+    const int kb = c0 / kUK, q0 = (c0 % kUK) / 8;
+    uint8_t *rowp = reinterpret_cast<uint8_t *>(S.act[kb]) + r * 128;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        *reinterpret_cast<uint4 *>(rowp + (((q0 + q) ^ (r & 7)) * 16)) =
+            make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    if (gout && row < M) {
+        uint4 *g = reinterpret_cast<uint4 *>(gout + (long)row * kMlpHidden + c0);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            g[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    }
+}
+
+__global__ void __launch_bounds__(kUThreads, 1)
+    k_mlp_fused(const __grid_constant__ CUtensorMap tx, const __grid_constant__ CUtensorMap tw1,
+                const __grid_constant__ CUtensorMap tw2, const __grid_constant__ CUtensorMap tw3, FusedParams p)
+{
+    griddep_wait();  // the features (and the row count) are written
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+    FusedSmem &S = *reinterpret_cast<FusedSmem *>(smem_raw + pad);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int M = p.M;
+    if (p.dM) {
+        const int c = *p.dM;
+        M = c < M ? c : M;
+    }
+    const int ntiles = (M + kUM - 1) / kUM;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kFStages; s++) {
+            mbar_init(&S.full[s], 1);
+            mbar_init(&S.empty[s], 1);
+        }
+        mbar_init(&S.acc_full, 1);
+        mbar_init(&S.acc_free, 4 * 32);
+        mbar_init(&S.act_ready, 4 * 32);
+        mbar_init(&S.drain, 1);
+        S.abort = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&S.tmem_base)),
+                     "r"(kFTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = S.tmem_base;
+    volatile int *abort = &S.abort;
+    bool ok = true;
+
+    if (warp == 4 && lane == 0) {
+        // TMA producer: per tile 17 units of (X, W1), 4 of W2, 4 of W3
+        long it = 0;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            const int m0 = t * kUM;
+            for (int j = 0; j < kFUnits; j++) {
+                const int s = (int)(it % kFStages);
+                const long round = it / kFStages;
+                if (round > 0 && !wait_bounded(&S.empty[s], (unsigned)((round - 1) & 1), abort)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&S.full[s], fused_unit_bytes(j));
+                if (j < kFK1) {
+                    tma_load_2d(S.a[s], &tx, j * kUK, m0, &S.full[s]);
+                    tma_load_2d(S.b[s], &tw1, j * kUK, 0, &S.full[s]);
+                } else if (j < kFK1 + kFK2) {
+                    tma_load_2d(S.b[s], &tw2, (j - kFK1) * kUK, 0, &S.full[s]);
+                } else {
+                    tma_load_2d(S.b[s], &tw3, (j - kFK1 - kFK2) * kUK, 0, &S.full[s]);
+                }
+                it++;
+            }
+        }
+        for (long j = it > kFStages ? it - kFStages : 0; j < it; j++)
+            wait_drain(&S.full[j % kFStages], (unsigned)((j / kFStages) & 1));
+    } else if (warp == 5 && lane == 0) {
+        // MMA issuer
+        long it = 0;
+        int tl = 0;
+        bool issued = false;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, tl++) {
+            if (tl > 0 && !wait_bounded(&S.acc_free, (unsigned)((tl - 1) & 1), abort)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            for (int layer = 0; layer < 3 && ok; layer++) {
+                const int nkb = layer == 0 ? kFK1 : kFK2;
+                const uint32_t idesc = instr_desc_n(layer == 2 ? kMlpOut : kMlpHidden);
+                if (layer > 0) {  // the activation tile of the layer before is written
+                    if (!wait_bounded(&S.act_ready, (unsigned)(layer - 1), abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                }
+                for (int kb = 0; kb < nkb; kb++, it++) {
+                    const int s = (int)(it % kFStages);
+                    if (!wait_bounded(&S.full[s], (unsigned)((it / kFStages) & 1), abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = layer == 0 ? smem_u32(S.a[s]) : smem_u32(S.act[kb]);
+                    const uint32_t sb = smem_u32(S.b[s]);
+#pragma unroll
+                    for (int kk = 0; kk < kUK / 16; kk++)
+                        umma_bf16(tbase, smem_desc(sa + kk * 32, 16, 1024), smem_desc(sb + kk * 32, 16, 1024),
+                                  idesc, (uint32_t)(kb | kk));
+                    issued = true;
+                    umma_commit(&S.empty[s]);
+                }
+                if (ok)
+                    umma_commit(&S.acc_full);
+            }
+        }
+        if (issued) {
+            umma_commit(&S.drain);
+            wait_drain(&S.drain, 0);
+        }
+    } else if (warp < 4) {
+        // epilogue: TMEM lane = tile row
+        int tl = 0;
+        const int r = warp * 32 + lane;
+        const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16);
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, tl++) {
+            const int row = t * kUM + r;
+            for (int layer = 0; layer < 3; layer++) {
+                const unsigned parity = (unsigned)((3 * tl + layer) & 1);
+                if (!__all_sync(kFull, wait_bounded(&S.acc_full, parity, abort))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                if (layer < 2) {
+                    const float *bias = layer == 0 ? p.b1 : p.b2;
+                    __nv_bfloat16 *gout = layer == 0 ? p.h1 : p.h2;
+                    for (int c0 = 0; c0 < kMlpHidden; c0 += 32) {
+                        uint32_t v[32];
+                        tmem_ld32(taddr + (uint32_t)c0, v);
+                        fused_store_act(S, r, c0, v, bias, gout, row, M);
+                    }
+                    // the generic-proxy writes become visible to the tensor core
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    tc_fence_before();
+                    mbar_arrive(&S.act_ready);
+                } else {
+                    for (int c0 = 0; c0 < kMlpOut; c0 += 32) {
+                        uint32_t v[32];
+                        tmem_ld32(taddr + (uint32_t)c0, v);
+                        if (row < M) {
+                            float4 *o = reinterpret_cast<float4 *>(p.logits + (long)row * kMlpOut + c0);
+#pragma unroll
+                            for (int q = 0; q < 8; q++)
+                                o[q] = make_float4(__uint_as_float(v[4 * q]) + p.b3[c0 + 4 * q],
+                                                   __uint_as_float(v[4 * q + 1]) + p.b3[c0 + 4 * q + 1],
+                                                   __uint_as_float(v[4 * q + 2]) + p.b3[c0 + 4 * q + 2],
+                                                   __uint_as_float(v[4 * q + 3]) + p.b3[c0 + 4 * q + 3]);
+                        }
+                    }
+                    tc_fence_before();
+                    mbar_arrive(&S.acc_free);
+                }
+            }
+        }
+    }
+    if (!ok) {
+        *abort = 1;
+        *reinterpret_cast<volatile int *>(p.err) = 1;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kFTmemCols)
+                     : "memory");
+    }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
@@ -448,7 +698,9 @@ UmmaRuntime &runtime()
             cudaDeviceGetAttribute(&rt.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return;
         if (cudaFuncSetAttribute(k_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmemBytes) !=
-            cudaSuccess)
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFSmemBytes) !=
+                cudaSuccess)
             return;
         if (cudaHostAlloc(reinterpret_cast<void **>(&rt.h_err), sizeof(int), cudaHostAllocMapped) != cudaSuccess)
             return;
@@ -565,6 +817,37 @@ void launch_gemm(const GemmArgs &g, cudaStream_t st, bool dep)
         k_split_reduce<<<(int)std::min<long>((total + 255) / 256, (long)rt.sms * 8), 256, 0, st>>>(
             g.split_ws, p.splits, g.M, g.N, g.cf, g.ldc);
     }
+}
+
+void launch_mlp_fused(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,
+                      __nv_bfloat16 *h1, __nv_bfloat16 *h2, float *logits, cudaStream_t st, bool dep)
+{
+    if (n <= 0)
+        return;
+    UmmaRuntime &rt = runtime();
+    if (!rt.ok)
+        return fail("tensor-core GEMM: the driver's tensor-map entry point or the kernel attributes are unavailable");
+    if (!aligned16(X) || !aligned16(w.w1) || !aligned16(w.w2) || !aligned16(w.w3) || !aligned16(logits) ||
+        (h1 && !aligned16(h1)) || (h2 && !aligned16(h2)))
+        return fail("fused forward: buffers must start on 16 bytes");
+    CUtensorMap tx, t1, t2, t3;
+    if (!make_map(&tx, X, kMlpInPad, n, kMlpInPad, kUK, kUM) ||
+        !make_map(&t1, w.w1, kMlpInPad, kMlpHidden, kMlpInPad, kUK, kMlpHidden) ||
+        !make_map(&t2, w.w2, kMlpHidden, kMlpHidden, kMlpHidden, kUK, kMlpHidden) ||
+        !make_map(&t3, w.w3, kMlpHidden, kMlpOut, kMlpHidden, kUK, kMlpOut))
+        return fail("fused forward: tensor map encoding failed");
+    FusedParams p{};
+    p.M = n;
+    p.dM = d_count;
+    p.b1 = w.b1;
+    p.b2 = w.b2;
+    p.b3 = w.b3;
+    p.h1 = h1;
+    p.h2 = h2;
+    p.logits = logits;
+    p.err = rt.d_err;
+    const int grid = (int)std::min<long>((n + kUM - 1) / kUM, rt.sms);
+    launch_dep(dep, k_mlp_fused, grid, kUThreads, kFSmemBytes, st, tx, t1, t2, t3, p);
 }
 
 }  // namespace frrt

@@ -131,3 +131,29 @@ def test_gemm_split_over_k(T, M, N, K):
     # too small a workspace: the unsplit product, within the same bound
     small = gemm(A, B, trans_a=True, trans_b=True, split_ws=ws[:M * N])
     check(small, Am @ Bm, Am.abs() @ Bm.abs(), False)
+
+
+def test_fused_forward_equals_the_layer_gemms(T, gpu):
+    """The network's one-kernel forward pass (activations kept in shared
+    memory between the layers) against three single GEMM launches with the
+    same epilogues on the same bf16 operands: bit-identical logits."""
+    from fastrrt_b200 import proposal as P
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(9)
+    ws = M.random_weights(rng)
+    for w in ws[1::2]:
+        w[:] = rng.standard_normal(w.shape).astype(np.float32) * 0.1
+    net = P.ProposalNet(seed=1, max_batch=512)
+    net.set_weights(ws)
+    for n in (1, 129, 300, 512):
+        X = (rng.random((n, 1030)) < 0.3).astype(np.float32)
+        X[:, 1024:] = rng.standard_normal((n, 6))
+        got = T.from_numpy(net.forward(X))
+        Xp = np.zeros((n, 1040), np.float32)
+        Xp[:, :1030] = X
+        xb = T.from_numpy(Xp).to(T.bfloat16).cuda()
+        w1, b1, w2, b2, w3, b3 = [T.from_numpy(np.ascontiguousarray(w)).cuda() for w in ws]
+        h1 = P.gemm(xb, w1.to(T.bfloat16), bias=b1, relu=True, out=T.empty((n, 256), dtype=T.bfloat16, device="cuda"))
+        h2 = P.gemm(h1, w2.to(T.bfloat16), bias=b2, relu=True, out=T.empty((n, 256), dtype=T.bfloat16, device="cuda"))
+        want = P.gemm(h2, w3.to(T.bfloat16), bias=b3).cpu()
+        assert T.equal(got, want), (n, float((got - want).abs().max()))
