@@ -83,7 +83,6 @@ struct Inst {
     float *cand_heading;
     float *cand_cost;
     float *cand_steer, *cand_len;  // per candidate: the draw it was integrated with
-    int32_t *prop_row;             // per candidate: row of the learned proposal, or -1
     float *prop_steer, *prop_len;  // per candidate: the proposal (prop_len < 0: uniform)
     float *exp_steer, *exp_len;    // per cell: the draw of the expansion that made the node
     int32_t *nodes;

@@ -201,7 +201,7 @@ void slot_parts(int W, int H, size_t parts[kParts])
         C / 8, 4 * C,                       // 25 gd request bits, 26 gd cell list
         8 * C, 8 * C,                       // 27 memo key, 28 memo result
         2 * (size_t)(W + 1) * (H + 1),      // 29 obstacle summed-area table
-        4 * C, 4 * C, 4 * C, 4 * C, 4 * C,  // 30 cand steer, 31 cand len, 32 prop row, 33/34 prop
+        4 * C, 4 * C, 0, 4 * C, 4 * C,      // 30 cand steer, 31 cand len, 32 (unused), 33/34 prop
         4 * C, 4 * C,                       // 35 exp steer, 36 exp len
     };
     for (int k = 0; k < kParts; k++)
@@ -265,7 +265,6 @@ bool Engine::layout_slot(int s, int W, int H)
     I.sat = (const uint16_t *)ptr[29];
     I.cand_steer = (float *)ptr[30];
     I.cand_len = (float *)ptr[31];
-    I.prop_row = (int32_t *)ptr[32];
     I.prop_steer = (float *)ptr[33];
     I.prop_len = (float *)ptr[34];
     I.exp_steer = (float *)ptr[35];
@@ -473,10 +472,6 @@ Engine::~Engine()
     cudaFree(d_class_costs_);
     cudaFree(d_bad_);
     cudaFree(d_clock_);
-    cudaFree(pb_.cells);
-    cudaFree(pb_.slot_of);
-    cudaFree(pb_.idx);
-    cudaFree(pb_.count);
     cudaFree(pb_.X);
     cudaFree(pb_.logits);
     cudaFree(d_log_cells_);
@@ -1219,19 +1214,11 @@ bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
         return false;
     }
     if (w && cap > 0 && cap != pb_.cap) {
-        cudaFree(pb_.cells);
-        cudaFree(pb_.slot_of);
-        cudaFree(pb_.idx);
-        cudaFree(pb_.count);
         cudaFree(pb_.X);
         cudaFree(pb_.logits);
         pb_ = ProposalBufs{};
         const size_t c = (size_t)cap;
-        if (!check(cudaMalloc(&pb_.cells, 4 * c), "proposal buffers") ||
-            !check(cudaMalloc(&pb_.slot_of, 4 * c), "proposal buffers") ||
-            !check(cudaMalloc(&pb_.idx, 4 * c), "proposal buffers") ||
-            !check(cudaMalloc(&pb_.count, sizeof(int)), "proposal buffers") ||
-            !check(cudaMalloc(&pb_.X, 2 * c * kMlpInPad), "proposal buffers") ||
+        if (!check(cudaMalloc(&pb_.X, 2 * c * kMlpInPad), "proposal buffers") ||
             !check(cudaMalloc(&pb_.logits, 4 * c * kMlpOut), "proposal buffers"))
             return false;
         pb_.cap = cap;
@@ -1240,7 +1227,9 @@ bool Engine::set_proposal(const MlpWeights *w, float mix, int cap)
     if (use_proposal_) {
         pb_.w = *w;
         pb_.mix = mix;
+        pb_.count = h_sched_.cand_exact + n_slots_;  // the iteration's candidate count
     }
+    h_sched_.prop_cap = use_proposal_ ? pb_.cap : 0;
     for (auto &I : h_inst_)
         I.proposal = use_proposal_ ? 1 : 0;
     dirty_ = true;

@@ -40,18 +40,7 @@ namespace frrt {
 
 namespace {
 
-__device__ __forceinline__ int find_slot(const int *prefix, int n, int chunk)
-{
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= chunk)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
+
 
 __device__ __forceinline__ bool live(const State &S) { return S.active && !S.done; }
 
@@ -1113,7 +1102,7 @@ __global__ void __launch_bounds__(256) k_expand(const Inst *insts, State *states
         const int pos = I.cand[idx];
         const int z = pos / I.W, x = pos - z * I.W;
         float steer, len;
-        if (I.proposal && I.prop_row[idx] >= 0 && I.prop_len[idx] >= 0.0f) {
+        if (I.proposal && e < sc->prop_cap && I.prop_len[idx] >= 0.0f) {
             steer = I.prop_steer[idx];
             len = I.prop_len[idx];
         } else {
@@ -1423,51 +1412,18 @@ const char *const kIterKernelNames[kIterKernels] = {
 // learned expansion proposal inside an iteration
 // ---------------------------------------------------------------------------
 
-// lists the candidates of slots that use the proposal (up to pb.cap rows)
-__global__ void __launch_bounds__(256) k_prop_list(const Inst *insts, const State *states,
-                                                   const Sched *sc, ProposalBufs pb)
-{
-    griddep_wait();  // the previous kernel of the iteration has finished
-    const int n = sc->n_slots;
-    const int total = sc->cand_start[n];
-    const int lane = threadIdx.x & 31;
-    for (int c = blockIdx.x; c < total; c += gridDim.x) {
-        const int slot = find_slot(sc->cand_start, n, c);
-        const Inst &I = insts[slot];
-        const State &S = states[slot];
-        const int idx = (c - sc->cand_start[slot]) * kCandChunk + threadIdx.x;
-        const bool is = idx < S.n_cand && I.proposal;
-        const unsigned m = __ballot_sync(kFull, is);
-        if (!m)
-            continue;
-        int b0 = 0;
-        if (lane == 0)
-            b0 = atomicAdd(pb.count, __popc(m));  // one atomic per warp
-        b0 = __shfl_sync(kFull, b0, 0);
-        if (!is)
-            continue;
-        int row = b0 + __popc(m & ((1u << lane) - 1u));
-        if (row >= pb.cap) {
-            row = -1;
-        } else {
-            pb.cells[row] = I.cand[idx];
-            pb.slot_of[row] = slot;
-            pb.idx[row] = idx;
-        }
-        I.prop_row[idx] = row;
-    }
-}
-
 // One warp per listed candidate: with probability mix (the third Philox word
 // of the candidate's draw) the (steering, length) bin is sampled from the
 // softmax of the network's logits (fourth word, inverse CDF) and the value
 // uniformly inside the bin (first two words); otherwise prop_len = -1 and
 // the expansion draws uniformly as without the network.
-__device__ void prop_sample_row(const Inst *insts, const State *states, const ProposalBufs &pb, int r,
-                                int lane)
+__device__ void prop_sample_row(const Inst *insts, const State *states, const Sched *sc, const ProposalBufs &pb,
+                                int r, int lane)
 {
-    const int slot = pb.slot_of[r], idx = pb.idx[r], pos = pb.cells[r];
+    const int slot = find_slot(sc->cand_exact, sc->n_slots, r);
+    const int idx = r - sc->cand_exact[slot];
     const Inst &I = insts[slot];
+    const int pos = I.cand[idx];
     const State &S = states[slot];
     uint32_t w[4];
     philox4x32((uint32_t)pos, S.iter, kRngTag, 0u, (uint32_t)I.seed, (uint32_t)(I.seed >> 32), w);
@@ -1532,26 +1488,29 @@ __device__ void prop_sample_row(const Inst *insts, const State *states, const Pr
 }
 
 // rows grid-strided over a machine-sized grid (the row count is on the device)
-__global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const State *states,
+__global__ void __launch_bounds__(256) k_prop_sample(const Inst *insts, const State *states, const Sched *sc,
                                                      ProposalBufs pb)
 {
     griddep_wait();  // the previous kernel of the iteration has finished
     const int lane = threadIdx.x & 31;
-    const int rows = min(*pb.count, pb.cap);
+    const int rows = min(sc->cand_exact[sc->n_slots], pb.cap);
     const int warps = (int)((gridDim.x * (long)blockDim.x) >> 5);
     for (int r = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); r < rows; r += warps)
-        prop_sample_row(insts, states, pb, r, lane);
+        prop_sample_row(insts, states, sc, pb, r, lane);
 }
 
+// the proposal step: every candidate of the iteration has its row (the exact
+// candidate prefix of its slot + its index), so features, the network and
+// the sampling read their rows' candidates directly; *count is the number
+// of candidates (the last entry of the exact prefix, on the device)
 void launch_proposal(const Inst *d_inst, State *d_state, const Sched *d_sched, const ProposalBufs &pb,
                      const Launch &L, cudaStream_t st, bool dep)
 {
-    cudaMemsetAsync(pb.count, 0, sizeof(int), st);
-    launch_dep(dep, k_prop_list, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched, pb);
-    launch_features(d_inst, pb.cells, pb.slot_of, pb.cap, pb.X, st, pb.count, dep);
+    (void)L;
+    launch_features_sched(d_inst, d_sched, pb.cap, pb.X, st, pb.count, dep);
     launch_mlp_forward(pb.w, pb.X, pb.cap, pb.count, nullptr, nullptr, pb.logits, st, dep);
     launch_dep(dep, k_prop_sample, std::min((pb.cap * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st, d_inst,
-               d_state, pb);
+               d_state, d_sched, pb);
 }
 
 void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_slots,

@@ -33,7 +33,24 @@ struct Sched {
     int *goal_start;          // [n_slots + 1] prefix of (node, window chunk) units per slot
     int *cand_exact;          // [n_slots + 1] prefix of candidates per slot
     unsigned *grab;           // [4] dynamic work counters
+    int prop_cap;             // proposal rows per iteration (0: no network attached); the
+                              // candidate idx of slot s is row cand_exact[s] + idx
 };
+
+// the slot whose prefix range [prefix[s], prefix[s + 1]) holds `chunk`
+// (the last of equal entries: slots with nothing are skipped)
+__device__ __forceinline__ int find_slot(const int *prefix, int n, int chunk)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= chunk)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
 
 struct Launch {
     int sms;                  // multiprocessors

@@ -125,18 +125,27 @@ __global__ void k_gather_rows(const __nv_bfloat16 *X, const int32_t *labels, con
 }
 
 // one warp per candidate; lanes over the 1024 patch samples
-__global__ void k_features(const Inst *insts, const int32_t *cells, const int32_t *slot_of, int n,
-                           __nv_bfloat16 *X, const int *d_count)
+// rows come from cells[k] / slot_of[k], or, with sc, from the planner's
+// exact candidate prefix (row = cand_exact[slot] + candidate index)
+__global__ void k_features(const Inst *insts, const int32_t *cells, const int32_t *slot_of, const Sched *sc,
+                           int n, __nv_bfloat16 *X, const int *d_count)
 {
-    griddep_wait();  // the candidate list is complete
+    griddep_wait();  // the candidates are listed
     const int lane = threadIdx.x & 31;
     if (d_count && *d_count < n)
         n = *d_count;
     // rows grid-strided over a machine-sized grid (the count is on the device)
     const int warps = (int)((gridDim.x * (long)blockDim.x) >> 5);
     for (int k = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); k < n; k += warps) {
-        const Inst &I = insts[slot_of[k]];
-        const int pos = cells[k];
+        int slot, pos;
+        if (sc) {
+            slot = find_slot(sc->cand_exact, sc->n_slots, k);
+            pos = insts[slot].cand[k - sc->cand_exact[slot]];
+        } else {
+            slot = slot_of[k];
+            pos = cells[k];
+        }
+        const Inst &I = insts[slot];
         const int z = pos / I.W, x = pos - z * I.W;
         const float h = I.heading[pos];
         float sh, ch;
@@ -226,7 +235,16 @@ void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *sl
     if (n <= 0)
         return;
     launch_dep(dep, k_features, std::min((n * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st, d_inst, cells,
-               slot_of, n, X, d_count);
+               slot_of, (const Sched *)nullptr, n, X, d_count);
+}
+
+void launch_features_sched(const Inst *d_inst, const Sched *d_sched, int n, __nv_bfloat16 *X, cudaStream_t st,
+                           const int *d_count, bool dep)
+{
+    if (n <= 0)
+        return;
+    launch_dep(dep, k_features, std::min((n * 32 + 255) / 256, kMlpGridBlocks), 256, 0, st, d_inst,
+               (const int32_t *)nullptr, (const int32_t *)nullptr, d_sched, n, X, d_count);
 }
 
 void launch_mlp_forward(const MlpWeights &w, const __nv_bfloat16 *X, int n, const int *d_count,

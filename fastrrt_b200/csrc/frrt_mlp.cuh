@@ -105,8 +105,7 @@ void launch_mlp_fused(const MlpWeights &w, const __nv_bfloat16 *X, int n, const 
 struct ProposalBufs {
     int cap;                   // candidates the network proposes for per iteration
     float mix;                 // probability of sampling from the network (else uniform)
-    int32_t *cells, *slot_of, *idx;
-    int *count;                // candidates listed this iteration (may exceed cap)
+    const int *count;          // candidates this iteration (device: the exact prefix's last entry)
     __nv_bfloat16 *X;
     float *logits;
     MlpWeights w;
@@ -119,6 +118,11 @@ struct ProposalBufs {
 // kMlpInPad (zero padded).  cells[k] / slots[k] name the parent.
 void launch_features(const Inst *d_inst, const int32_t *cells, const int32_t *slot_of, int n,
                      __nv_bfloat16 *X, cudaStream_t st, const int *d_count = nullptr, bool dep = false);
+struct Sched;
+// the same for the planner's proposal rows: row r is candidate
+// r - cand_exact[s] of the slot s whose exact candidate prefix holds r
+void launch_features_sched(const Inst *d_inst, const Sched *d_sched, int n, __nv_bfloat16 *X, cudaStream_t st,
+                           const int *d_count, bool dep);
 
 // The (steering, length) bin of a draw, the training label
 __host__ __device__ inline int proposal_bin(float steer, float len, float max_steer, float max_path)
