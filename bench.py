@@ -16,7 +16,7 @@ or its timeout, then extracted and validated on the device.  Only validated
 plans count.  The headline operating point is the autotuner's
 (fastrrt_b200/tuned.json): the fastest slot count, harvest interval and
 expansion proposal (the learned network or uniform draws) whose success
-rate meets the reference planner's minus one point.
+rate is at least 96.9 %.
 
   value   : validated plans/s with the frames already in HBM (device clock,
             CUDA events around each step, max over ranks)
@@ -25,11 +25,16 @@ rate meets the reference planner's minus one point.
             inside the timed region)
   serving : Poisson arrivals at the C3 rates; p50/p95/p99 latency from
             arrival to finish
+  serving_mixed_sizes / batched_mixed_sizes : the C3 and C2 workloads
+            (60/30/10 % 256/128/512 frames under a 40 GB budget; 512
+            instances of 128/256/512 frames per batch)
+  roofline: the dominant kernel's footprint-probe rate against one probe per
+            lane per cycle
   cpu_baseline / --impl reference : the CPU restatement of the same planner
             (oracle/, all host cores) on a bounded sample of the workload
 
 Each step plans frames never planned before; the per-step working set (S
-slots x ~6.6 MB of node grid and scratch) exceeds L2.  With --gpus N > 1 and
+slots x ~8 MB of node grid and scratch) exceeds L2.  With --gpus N > 1 and
 no torchrun environment the script starts N ranks itself (one process per
 GPU); every rank serves its own requests (weak scaling, no collective on the
 data path) and the time is the maximum over ranks.
