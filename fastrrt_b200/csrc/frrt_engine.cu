@@ -646,7 +646,6 @@ bool Engine::commit()
     h_sched_.sweep_start = d_sched_arrays_;
     h_sched_.cand_start = d_sched_arrays_ + (n_slots_ + 1);
     h_sched_.node_start = d_sched_arrays_ + 2 * (n_slots_ + 1);
-    h_sched_.gd_start = d_sched_arrays_ + 3 * (n_slots_ + 1);
     h_sched_.goal_start = d_sched_arrays_ + 4 * (n_slots_ + 1);
     h_sched_.cand_exact = d_sched_arrays_ + 5 * (n_slots_ + 1);
     h_sched_.grab = d_grab_;

@@ -605,23 +605,29 @@ __device__ void plan_prefix(const Inst *insts, State *states, int n, int which, 
         out[n] = fits ? (int)run : 0;
 }
 
-// prefix of per-slot work (one block) for one kernel of the iteration, and
-// the reset of that kernel's work counter; which = 0 (candidates) writes the
-// chunk prefix and the exact candidate prefix
+// prefix of per-slot work (one block) for kernels of the iteration, and the
+// reset of their work counters; which = 0 (candidates) writes the chunk
+// prefix and the exact candidate prefix, which = 1 (node chunks) also the
+// prefix of the goal search's (node, window chunk) units, which counts the
+// same listed nodes (k_gd_eval scans its own listed cells)
 __global__ void __launch_bounds__(1024) k_plan(const Inst *insts, State *states, Sched *sc,
                                               int which)
 {
     griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
-    int *out = which == 0   ? sc->cand_start
-               : which == 1 ? sc->node_start
-               : which == 2 ? sc->gd_start
-                            : sc->goal_start;
+    int *out = which == 0 ? sc->cand_start : sc->node_start;
     plan_prefix(insts, states, n, which, out);
     if (which == 0)
         plan_prefix(insts, states, n, 4, sc->cand_exact);
-    if (threadIdx.x == 0)
+    if (which == 1)
+        plan_prefix(insts, states, n, 3, sc->goal_start);
+    if (threadIdx.x == 0) {
         sc->grab[which] = 0;
+        if (which == 1) {  // the direct-connection evaluation and the goal search follow
+            sc->grab[2] = 0;
+            sc->grab[3] = 0;
+        }
+    }
 }
 
 
@@ -1033,7 +1039,12 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
 {
     griddep_wait();  // the previous kernel of the iteration has finished
     const int n = sc->n_slots;
-    const int total = sc->gd_start[n];
+    // every block scans the slots' listed-cell counts into its own prefix
+    // (n + 1 ints of dynamic shared memory) instead of a separate launch
+    extern __shared__ int gd_start[];
+    plan_prefix(insts, states, n, 2, gd_start);
+    __syncthreads();
+    const int total = gd_start[n];
     const int lane = threadIdx.x & 31;
     const int batch = grab_batch(total);
     for (int e0 = 0, e1 = 0, e = 0, slot = 0;; e++) {
@@ -1045,12 +1056,12 @@ __global__ void __launch_bounds__(256, kEvalBlocks) k_gd_eval(const Inst *insts,
                 break;
             e = e0;
             e1 = min(e0 + batch, total);
-            slot = find_slot(sc->gd_start, n, e);
+            slot = find_slot(gd_start, n, e);
         }
-        while (e >= sc->gd_start[slot + 1])
+        while (e >= gd_start[slot + 1])
             slot++;
         const Inst &I = insts[slot];
-        const int pos = I.gd_list[e - sc->gd_start[slot]];
+        const int pos = I.gd_list[e - gd_start[slot]];
         const Foot f = foot_of(I, I.blocked, I.clear);
         const int z = pos / I.W;
         const int x = pos - z * I.W;
@@ -1405,8 +1416,8 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
 
 const char *const kIterKernelNames[kIterKernels] = {
     "k_scan", "k_plan(cand)", "k_propose(mlp)", "k_expand", "k_apply", "k_post", "k_erase",
-    "k_setnodes", "k_accept", "k_plan(nodes)", "k_plan(windows)", "k_gd_demand", "k_plan(cells)",
-    "k_gd_eval", "k_goal", "k_select", "k_finish"};
+    "k_setnodes", "k_accept", "k_plan(nodes, windows)", "k_gd_demand", "k_gd_eval", "k_goal", "k_select",
+    "k_finish"};
 
 // ---------------------------------------------------------------------------
 // learned expansion proposal inside an iteration
@@ -1547,15 +1558,12 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     mark();
     launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 1);
     mark();
-    launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 3);
-    mark();
     // one warp per (node, window chunk): its grid follows the machine, not
     // the frame's sweep chunks (16 for one 256 x 256 slot)
     launch_dep(dep, k_gd_demand, L.sms * 8, 256, 0, st, d_inst, d_state, d_sched);
     mark();
-    launch_dep(dep, k_plan, 1, 1024, 0, st, d_inst, d_state, d_sched, 2);
-    mark();
-    launch_dep(dep, k_gd_eval, L.sms * kEvalBlocks, 256, 0, st, d_inst, d_state, d_sched);
+    launch_dep(dep, k_gd_eval, L.sms * kEvalBlocks, 256, sizeof(int) * (n_slots + 1), st, d_inst, d_state,
+               d_sched);
     mark();
     launch_dep(dep, k_goal, L.sms * kGoalBlocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();

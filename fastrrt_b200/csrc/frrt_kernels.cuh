@@ -29,7 +29,6 @@ struct Sched {
     int *sweep_start;         // [n_slots + 1] prefix of sweep chunks per slot
     int *cand_start;          // [n_slots + 1] prefix of candidate chunks per slot
     int *node_start;          // [n_slots + 1] prefix of node chunks per slot
-    int *gd_start;            // [n_slots + 1] prefix of listed direct-connection cells per slot
     int *goal_start;          // [n_slots + 1] prefix of (node, window chunk) units per slot
     int *cand_exact;          // [n_slots + 1] prefix of candidates per slot
     unsigned *grab;           // [4] dynamic work counters
@@ -108,7 +107,7 @@ void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, 
 // one planning iteration (loop()) over all active slots; with `ev` (an array
 // of kIterKernels + 1 events) an event is recorded before each kernel and
 // after the last one
-constexpr int kIterKernels = 17;
+constexpr int kIterKernels = 15;
 extern const char *const kIterKernelNames[kIterKernels];
 struct ProposalBufs;
 // with `pb`, candidates of slots that use the learned proposal get their
