@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--check-every", type=int, default=None,
                     help="graph launches between harvests (default: autotuned, else 2)")
     ap.add_argument("--rates", default="200,1000,5000", help="Poisson arrival rates (req/s)")
-    ap.add_argument("--rate-requests", type=int, default=600)
+    ap.add_argument("--rate-requests", type=int, default=2000)
     ap.add_argument("--mix", type=float, default=None,
                     help="learned-proposal sampling probability (default: the autotuned one; "
                          "< 0: uniform draws only)")
@@ -520,7 +520,7 @@ def c3_serving(args, rank, world, tuned, attach_net):
         out_rates = {}
         for rate in rates:
             out = planner.serve(reqs, arrival_ms=arrivals[rate], timeout_ms=TIMEOUT_MS,
-                                check_every=args.check_every)
+                                check_every=args.serving_check_every)
             v = out["valid"] > 0
             lat = out["latency_ms"][v]
             out_rates[f"{rate:g}_req_s"] = {
@@ -574,6 +574,8 @@ def run_mine(args, rank, world, local):
         args.slots = tuned["slots"]
     if tuned and args.check_every is None:
         args.check_every = tuned["check_every"]
+    # the Poisson (latency) legs harvest at the interval tuned for latency
+    args.serving_check_every = (tuned or {}).get("serving_check_every") or args.check_every
     if args.mix is None:
         args.mix = tuned.get("mix") if tuned else 0.8
         if args.mix is None:
@@ -607,8 +609,8 @@ def run_mine(args, rank, world, local):
         return reqs
 
     def serve(reqs, arrival=None):
-        return planner.serve(reqs, arrival_ms=arrival, timeout_ms=TIMEOUT_MS,
-                             check_every=args.check_every)
+        ce = args.serving_check_every if arrival is not None else args.check_every
+        return planner.serve(reqs, arrival_ms=arrival, timeout_ms=TIMEOUT_MS, check_every=ce)
 
     def timed_steps(reqs_of_step, clocks=None):
         """the timed steps: (device ms summed, validated plans, service ms, loops, lengths)"""
@@ -735,7 +737,8 @@ def run_mine(args, rank, world, local):
                                    f"{args.slots} slots, {TIMEOUT_MS} ms timeout per request, "
                                    f"expansion proposal: {proposal}",
                        "requests_per_step_per_gpu": R, "slots_per_gpu": args.slots,
-                       "check_every": args.check_every, "proposal": proposal,
+                       "check_every": args.check_every,
+                       "serving_check_every": args.serving_check_every, "proposal": proposal,
                        "launch_shape": ({k: tuned[k] for k in ("sweep_blocks_per_sm", "work_blocks_per_sm")}
                                         if tuned else "default"),
                        "frame": f"{SIZE}x{SIZE} @ {M_PER_PX} m/px",

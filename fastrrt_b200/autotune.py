@@ -5,10 +5,13 @@ launches between checks) and expansion proposal (uniform draws, or the
 learned network sampled with probability `mix`), and keeps the fastest
 combination whose success rate is at least `--min-success` (97.9 %, the
 planner's success rate over 1000 C0 seeds with a 50-loop cap, minus one
-point; the reference's own planner solves 97.3 % of them); then
-the launch shape (blocks per SM of the sweep and persistent kernels) of the
-batched workload (512 instances of mixed 128 / 256 / 512 frames).  The best
-and every trial go to a JSON file that bench.py reads.
+point; the reference's own planner solves 97.3 % of them); then the
+harvest interval with the lowest p99 latency of Poisson arrivals at 1000
+req/s through that operating point (the interval of the served benchmark's
+Poisson legs); then the launch shape (blocks per SM of the sweep and
+persistent kernels) of the batched workload (512 instances of mixed 128 /
+256 / 512 frames).  The best and every trial go to a JSON file that
+bench.py reads.
 
     python -m fastrrt_b200.autotune [--requests N] [--min-success S] [--out PATH]
 """
@@ -22,8 +25,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "tuned.json")
-GRID = {"slots": (256, 384, 512, 640, 768, 1024), "check_every": (1, 2),
+GRID = {"slots": (256, 384, 512, 640, 768, 1024), "check_every": (1, 2, 3, 4),
         "mix": (None, 0.8, 1.0)}
+SERVING = {"rate": 1000.0, "requests": 2000, "check_every": (1, 2, 3, 4)}
 LAUNCH = {"sweep_blocks_per_sm": 16, "work_blocks_per_sm": 2}
 C2_GRID = {"sweep_blocks_per_sm": (4, 8, 16), "work_blocks_per_sm": (1, 2, 4)}
 MIN_SUCCESS = 0.969
@@ -92,6 +96,27 @@ def main():
     best = pick(trials, a.min_success)
     if best is None:  # nothing meets the bar: the most successful trial
         best = max(trials, key=lambda t: (t["success_rate"], t["plans_per_s"]))
+    # the harvest interval for latency: Poisson arrivals at 1000 req/s through
+    # the chosen slots and proposal, the interval with the lowest p99 latency
+    serving_trials = []
+    planner = F.BatchPlanner(best["slots"], 256, 256)
+    planner.set_launch(LAUNCH["sweep_blocks_per_sm"], LAUNCH["work_blocks_per_sm"])
+    planner.set_proposal(net if best["mix"] is not None else None, mix=best["mix"] or 0.0)
+    rng = np.random.default_rng(99)
+    arrival = np.cumsum(rng.exponential(1e3 / SERVING["rate"], SERVING["requests"]))
+    sreqs = reqs[:SERVING["requests"]]
+    for ce in SERVING["check_every"]:
+        planner.serve(sreqs[:256], timeout_ms=100, check_every=ce)
+        out = planner.serve(sreqs, arrival_ms=arrival, timeout_ms=100, check_every=ce)
+        v = out["valid"] > 0
+        serving_trials.append({"check_every": ce, "rate": SERVING["rate"],
+                               "p50_ms": float(np.percentile(out["latency_ms"][v], 50)),
+                               "p99_ms": float(np.percentile(out["latency_ms"][v], 99)),
+                               "success_rate": float(v.mean())})
+        print(json.dumps(serving_trials[-1]), flush=True)
+    planner.set_proposal(None)
+    del planner
+    best["serving_check_every"] = min(serving_trials, key=lambda t: t["p99_ms"])["check_every"]
     # the batched workload (512 instances of 128 / 256 / 512 frames in one
     # batch): the launch shape with the most validated plans/s
     c2_trials = []
@@ -115,7 +140,8 @@ def main():
     del planner
     c2_best = max(c2_trials, key=lambda t: t["plans_per_s"])
     best["c2_launch"] = {k: c2_best[k] for k in ("sweep_blocks_per_sm", "work_blocks_per_sm")}
-    json.dump({"best": best, "min_success": a.min_success, "trials": trials, "c2_trials": c2_trials,
+    json.dump({"best": best, "min_success": a.min_success, "trials": trials, "serving_trials": serving_trials,
+               "c2_trials": c2_trials,
                "requests": a.requests, "when": time.strftime("%Y-%m-%d")}, open(a.out, "w"), indent=1)
     print("best", json.dumps(best))
 
