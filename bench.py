@@ -24,7 +24,8 @@ rate is at least 96.9 %.
             copies of the frames and device -> host copies of the results
             inside the timed region)
   serving : Poisson arrivals at the C3 rates; p50/p95/p99 latency from
-            arrival to finish
+            arrival until the validated path is on the host (and from
+            arrival to the device-clock finish)
   serving_mixed_sizes / batched_mixed_sizes : the C3 and C2 workloads
             (60/30/10 % 256/128/512 frames under a 40 GB budget; 512
             instances of 128/256/512 frames per batch)
@@ -522,7 +523,7 @@ def c3_serving(args, rank, world, tuned, attach_net):
             out = planner.serve(reqs, arrival_ms=arrivals[rate], timeout_ms=TIMEOUT_MS,
                                 check_every=args.serving_check_every)
             v = out["valid"] > 0
-            lat = out["latency_ms"][v]
+            lat = out["result_ms"][v]     # arrival -> validated path on the host
             out_rates[f"{rate:g}_req_s"] = {
                 "offered": rate, "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
                 "success_rate": float(v.mean()), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
@@ -665,12 +666,14 @@ def run_mine(args, rank, world, local):
             arrival = np.cumsum(rng.exponential(1e3 / rate, n_rate))
             out = serve(rate_reqs, arrival)
             v = out["valid"] > 0
-            lat = out["latency_ms"][v]
+            lat = out["result_ms"][v]     # arrival -> validated path on the host
+            fin = out["latency_ms"][v]    # arrival -> finish on the device clock
             res[f"{rate:g}_req_s"] = {
                 "offered": rate, "requests": n_rate,
                 "achieved_plans_per_s": float(v.sum()) / (out["wall_ms"] / 1e3),
                 "success_rate": float(v.mean()),
-                "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99)}
+                "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99),
+                "finish_p50_ms": pct(fin, 50), "finish_p99_ms": pct(fin, 99)}
         return res
 
     serving = poisson()

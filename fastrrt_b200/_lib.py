@@ -188,7 +188,7 @@ def lib():
         "fastrrt_batch_log_paths": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
         "fastrrt_batch_log_nodes": (C.c_int, [vp, vp, vp, C.c_int, C.c_int]),
         "fastrrt_batch_serve": (C.c_int, [vp, C.c_int, P(Request), vp, C.c_int, C.c_int, i32p, f32p,
-                                          f32p, f32p, i32p, P(C.c_double), P(C.c_float)]),
+                                          f32p, f32p, i32p, P(C.c_double), P(C.c_float), f32p]),
     }
     for name in EXPORTS:
         fn = getattr(L, name)

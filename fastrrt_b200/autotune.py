@@ -49,11 +49,39 @@ def pick(trials, min_success):
     return max(ok, key=lambda t: t["plans_per_s"]) if ok else None
 
 
+def serving_sweep(F, net, best, reqs):
+    """the harvest interval for latency: Poisson arrivals at 1000 req/s
+    through the chosen slots and proposal, p99 latency until the validated
+    path is on the host for each interval"""
+    serving_trials = []
+    planner = F.BatchPlanner(best["slots"], 256, 256)
+    planner.set_launch(LAUNCH["sweep_blocks_per_sm"], LAUNCH["work_blocks_per_sm"])
+    planner.set_proposal(net if best["mix"] is not None else None, mix=best["mix"] or 0.0)
+    rng = np.random.default_rng(99)
+    arrival = np.cumsum(rng.exponential(1e3 / SERVING["rate"], SERVING["requests"]))
+    sreqs = reqs[:SERVING["requests"]]
+    for ce in SERVING["check_every"]:
+        planner.serve(sreqs[:256], timeout_ms=100, check_every=ce)
+        out = planner.serve(sreqs, arrival_ms=arrival, timeout_ms=100, check_every=ce)
+        v = out["valid"] > 0
+        serving_trials.append({"check_every": ce, "rate": SERVING["rate"],
+                               "p50_ms": float(np.percentile(out["result_ms"][v], 50)),
+                               "p99_ms": float(np.percentile(out["result_ms"][v], 99)),
+                               "finish_p99_ms": float(np.percentile(out["latency_ms"][v], 99)),
+                               "success_rate": float(v.mean())})
+        print(json.dumps(serving_trials[-1]), flush=True)
+    planner.set_proposal(None)
+    del planner
+    return serving_trials
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=8192)
     ap.add_argument("--min-success", type=float, default=MIN_SUCCESS)
     ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--serving-only", action="store_true",
+                    help="keep the recorded operating point; measure only the latency harvest interval")
     a = ap.parse_args()
     import torch
 
@@ -74,6 +102,15 @@ def main():
                                    dev[k].data_ptr()) for k in range(a.requests)]
     net = P.ProposalNet(seed=0, max_batch=512)
     have_net = TP.load(net)
+    if a.serving_only:
+        with open(a.out) as f:
+            record = json.load(f)
+        best = record["best"]
+        record["serving_trials"] = serving_sweep(F, net, best, reqs)
+        best["serving_check_every"] = min(record["serving_trials"], key=lambda t: t["p99_ms"])["check_every"]
+        json.dump(record, open(a.out, "w"), indent=1)
+        print("best", json.dumps(best))
+        return
     trials = []
     for slots in GRID["slots"]:
         planner = F.BatchPlanner(slots, 256, 256)
@@ -96,26 +133,7 @@ def main():
     best = pick(trials, a.min_success)
     if best is None:  # nothing meets the bar: the most successful trial
         best = max(trials, key=lambda t: (t["success_rate"], t["plans_per_s"]))
-    # the harvest interval for latency: Poisson arrivals at 1000 req/s through
-    # the chosen slots and proposal, the interval with the lowest p99 latency
-    serving_trials = []
-    planner = F.BatchPlanner(best["slots"], 256, 256)
-    planner.set_launch(LAUNCH["sweep_blocks_per_sm"], LAUNCH["work_blocks_per_sm"])
-    planner.set_proposal(net if best["mix"] is not None else None, mix=best["mix"] or 0.0)
-    rng = np.random.default_rng(99)
-    arrival = np.cumsum(rng.exponential(1e3 / SERVING["rate"], SERVING["requests"]))
-    sreqs = reqs[:SERVING["requests"]]
-    for ce in SERVING["check_every"]:
-        planner.serve(sreqs[:256], timeout_ms=100, check_every=ce)
-        out = planner.serve(sreqs, arrival_ms=arrival, timeout_ms=100, check_every=ce)
-        v = out["valid"] > 0
-        serving_trials.append({"check_every": ce, "rate": SERVING["rate"],
-                               "p50_ms": float(np.percentile(out["latency_ms"][v], 50)),
-                               "p99_ms": float(np.percentile(out["latency_ms"][v], 99)),
-                               "success_rate": float(v.mean())})
-        print(json.dumps(serving_trials[-1]), flush=True)
-    planner.set_proposal(None)
-    del planner
+    serving_trials = serving_sweep(F, net, best, reqs)
     best["serving_check_every"] = min(serving_trials, key=lambda t: t["p99_ms"])["check_every"]
     # the batched workload (512 instances of 128 / 256 / 512 frames in one
     # batch): the launch shape with the most validated plans/s

@@ -176,13 +176,15 @@ class BatchPlanner:
     def serve(self, requests, arrival_ms=None, timeout_ms=100, check_every=2):
         """Continuous batching over `requests` (admitted as they arrive and
         slots free up); returns a dict of per-request arrays (valid, length,
-        latency_ms from arrival, service_ms from admission, loops) and the
-        wall and device (CUDA event) time of the call in ms."""
+        latency_ms from arrival to the device-clock finish, service_ms from
+        admission to finish, result_ms from arrival until the validated path
+        is on the host, loops) and the wall and device (CUDA event) time of
+        the call in ms."""
         n = len(requests)
         arr = (_lib.Request * n)(*requests) if n else None
         out = {"valid": np.zeros(n, np.int32), "length": np.zeros(n, np.float32),
                "latency_ms": np.zeros(n, np.float32), "service_ms": np.zeros(n, np.float32),
-               "loops": np.zeros(n, np.int32)}
+               "loops": np.zeros(n, np.int32), "result_ms": np.zeros(n, np.float32)}
         arrival = None
         if arrival_ms is not None:
             arrival = np.ascontiguousarray(arrival_ms, np.float64)
@@ -191,7 +193,7 @@ class BatchPlanner:
         _lib.check(_lib.lib().fastrrt_batch_serve(
             self._h, n, arr, None if arrival is None else arrival.ctypes.data, int(timeout_ms),
             int(check_every), out["valid"], out["length"], out["latency_ms"], out["service_ms"],
-            out["loops"], _lib.C.byref(wall), _lib.C.byref(dev)), "batch_serve")
+            out["loops"], _lib.C.byref(wall), _lib.C.byref(dev), out["result_ms"]), "batch_serve")
         out["wall_ms"] = wall.value
         out["device_ms"] = dev.value
         return out

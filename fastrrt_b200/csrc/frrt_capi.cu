@@ -1224,7 +1224,7 @@ int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_
 int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const double *arrival_ms,
                         int timeout_ms, int check_every, int32_t *valid, float *length,
                         float *latency_ms, float *service_ms, int32_t *loops, double *wall_ms,
-                        float *device_ms)
+                        float *device_ms, float *result_ms)
 {
     auto *b = static_cast<Batch *>(batch);
     if (!b || n < 0 || (n > 0 && !reqs)) {
@@ -1320,10 +1320,14 @@ int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const d
             continue;
         if (!e.extract_and_validate(list, 1024, false))
             return -1;
+        // the paths and verdicts of these requests are on the host now
+        const double ready = now_ms() - t0;
         for (size_t k = 0; k < list.size(); k++) {
             const int s = list[k];
             const int r = owner[s];
             const State &S = e.state(s);
+            if (result_ms)
+                result_ms[r] = (float)(ready - (arrival_ms ? arrival_ms[r] : 0.0));
             const int v = e.valid()[k] && S.goal_reached;
             good += v;
             const double fin = finish_ms(S.finish_ns);

@@ -328,14 +328,16 @@ int fastrrt_batch_plan(void *batch, int n, const fastrrt_request *reqs, int max_
  * as soon as it finishes: goal reached, loop cap, or timeout_ms after it
  * started planning (device clock; a request's own timeout_ms wins).  Per
  * request (any output may be NULL): valid, coarse path length, latency from
- * arrival and from admission to finish (ms, host clock), loops run.
- * *wall_ms = the whole call on the host clock, *device_ms = the same span
- * between CUDA events on the planner's stream.  Returns the number of
- * validated plans. */
+ * arrival and from admission to finish (ms: the device clock's finish in
+ * host time), loops run, and result_ms, the latency from arrival to the
+ * moment its validated path was on the host (the harvest of its slot, every
+ * check_every launches).  *wall_ms = the whole call on the host clock,
+ * *device_ms = the same span between CUDA events on the planner's stream.
+ * Returns the number of validated plans. */
 int fastrrt_batch_serve(void *batch, int n, const fastrrt_request *reqs, const double *arrival_ms,
                         int timeout_ms, int check_every, int32_t *valid, float *length,
                         float *latency_ms, float *service_ms, int32_t *loops, double *wall_ms,
-                        float *device_ms);
+                        float *device_ms, float *result_ms);
 /* launch shape of the iteration: blocks per SM of the sweep kernels (1..64,
  * default 8) and of the persistent expansion kernel (1..8, default 2); the
  * autotuner (fastrrt_b200/autotune.py) picks them */

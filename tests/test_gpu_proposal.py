@@ -75,3 +75,25 @@ def test_trained_proposal_raises_success(gpu, torch_gpu):
     sl = float((r["learned"]["valid"] > 0).mean())
     print(f"held-out success: uniform {su:.3f}, learned {sl:.3f}")
     assert sl > su
+
+
+def test_learned_plans_same_alone_and_in_a_batch(gpu):
+    """With the shipped network attached (mix 1.0) a request's plan does not
+    depend on the other requests of its batch: its candidates' rows,
+    features, logits and draws are its own."""
+    from fastrrt_b200 import proposal as P
+    from fastrrt_b200 import train_proposal as TP
+    net = P.ProposalNet(seed=0, max_batch=512)
+    assert TP.load(net)
+    reqs = requests(gpu, range(5000, 5012))
+    B = gpu.BatchPlanner(12, 512, 512)
+    B.set_proposal(net, mix=1.0)
+    vb, lb, _, _ = B.plan(reqs, 60, 4)
+    _, _, loops_b = B.status()
+    A = gpu.BatchPlanner(1, 512, 512)
+    A.set_proposal(net, mix=1.0)
+    for k in range(len(reqs)):
+        va, la, _, _ = A.plan([reqs[k]], 60, 4)
+        _, _, loops_a = A.status()
+        assert (int(va[0]), float(la[0]), int(loops_a[0])) == (int(vb[k]), float(lb[k]), int(loops_b[k])), k
+        assert np.array_equal(A.path(0), B.path(k)), k
