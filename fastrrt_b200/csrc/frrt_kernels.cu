@@ -1610,17 +1610,25 @@ void launch_goal_check(const Inst *d_inst, State *d_state, const int *d_slots, i
 // findBestNode pass 1 (graph_best_node.cu:15-75): key = cost * 2^32 +
 // (2^32 - 1 - cell), so the minimum is the lowest cost and, among equal
 // costs, the highest cell index (the last writer of the sequential pass 2)
+// Only the NODE cells within dist_tol of the goal qualify, so one block per
+// slot scans the goal's window (the cells within dist_tol on each axis); the
+// minimum key does not depend on the order of the scan.
 __global__ void k_best_node(const Inst *insts, const int *slots, long long *keys)
 {
     const int k = blockIdx.y;
     const Inst &I = insts[slots[k]];
-    const long cells = (long)I.W * I.H;
     const Foot f = foot_of(I, I.blocked, I.clear);
-    for (long pos = blockIdx.x * (long)blockDim.x + threadIdx.x; pos < cells;
-         pos += (long)gridDim.x * blockDim.x) {
+    int zlo, xlo;
+    const int nz = window_count(I.goal_z, I.dist_tol, zlo);
+    const int nx = window_count(I.goal_x, I.dist_tol, xlo);
+    const int wtotal = nx > 0 ? nz * nx : 0;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < wtotal; w += gridDim.x * blockDim.x) {
+        const int z = zlo + w / nx, x = xlo + w % nx;
+        if (z < 0 || z >= I.H || x < 0 || x >= I.W)
+            continue;
+        const long pos = (long)z * I.W + x;
         if (I.type[pos] != T_NODE)
             continue;
-        const int z = (int)(pos / I.W), x = (int)(pos - (long)z * I.W);
         const int dx = I.goal_x - x, dz = I.goal_z - z;
         const float dist = sqrtf(dx * dx + dz * dz);
         if (dist > I.dist_tol)
@@ -1703,7 +1711,8 @@ void launch_extract_paths(const Inst *d_inst, State *d_state, const int *d_slots
     if (n <= 0)
         return;
     k_fill_keys<<<(n + 255) / 256, 256, 0, st>>>(d_keys, n);
-    k_best_node<<<dim3((max_cells + 255) / 256, n), 256, 0, st>>>(d_inst, d_slots, d_keys);
+    (void)max_cells;
+    k_best_node<<<dim3(1, n), 256, 0, st>>>(d_inst, d_slots, d_keys);
     k_walk<<<(n + 63) / 64, 64, 0, st>>>(d_inst, d_slots, n, d_keys, d_paths, d_path_n, cap);
 }
 
