@@ -6,15 +6,17 @@
 //
 //   k_scan        gate + candidate list             (graph_expansion.cu:148-183,
 //                                                    graph_expansion_search_zones.cu:161-194)
-//   k_plan        per-slot work prefix (1 block)
+//   k_plan        per-slot candidate prefixes (1 block)
+//   [proposal]    features, network, sampling (learned proposal only)
 //   k_expand      integrate + footprint + claim     (expand_node, graph_expansion.cu:103-145)
 //   k_apply       claim winners change the grid
 //   k_post        NODE count + region density       (graph_expansion_search_zones.cu:42-66)
 //   k_erase       colliding subtree erase           (graph_collision.cu:32-83)
-//   k_setnodes    COLLISION -> NODE                 (graph_collision.cu:84-104)
-//   k_accept      TEMP count, all count, TEMP->NODE, node list
-//                                                   (graph_list.cu:7-60, graph_expansion.cu:36-65)
-//   k_plan        node work prefix
+//   k_accept      COLLISION -> NODE (graph_collision.cu:84-104), TEMP count, all
+//                 count, TEMP->NODE, node list      (graph_list.cu:7-60, graph_expansion.cu:36-65)
+//   k_plan        node and goal-window work prefixes
+//   k_gd_demand   window cells whose goal direct connection is unknown
+//   k_gd_eval     their direct connections (graph_direct_goal_connection.cu:16-167)
 //   k_goal        goal check + best node->cell goal connection
 //                                                   (graph_best_node.cu:181-222,
 //                                                    graph_check_goal_reached.cu:17-139)
@@ -816,34 +818,24 @@ __global__ void __launch_bounds__(256) k_erase(const Inst *insts, State *states,
 
 // COLLISION -> NODE, child count reset, parent child count + 1
 // (graph_collision.cu:84-104)
-__global__ void __launch_bounds__(256) k_setnodes(const Inst *insts, State *states, const Sched *sc)
+// COLLISION -> NODE of a thread's 16 cells with the child-count updates
+// (graph_collision.cu:90-110), run by k_accept before it reads them; the
+// collision pass needs k_erase's walks over the whole grid done, which the
+// kernel boundary before k_accept provides
+__device__ __forceinline__ void set_collision_nodes(const Inst &I, int base, int cells)
 {
-    griddep_wait();  // the previous kernel of the iteration has finished
-    const int n = sc->n_slots;
-    const int total = sc->sweep_total;
-    for (int c = blockIdx.x; c < total; c += gridDim.x) {
-        const int slot = find_slot(sc->sweep_start, n, c);
-        const State &S = states[slot];
-        if (!live(S) || !S.collision || S.node_count <= 2)
+    int8_t t[16];
+    load16(I.type + base, t);
+    for (int k = 0; k < 16; k++) {
+        const int pos = base + k;
+        if (pos >= cells || t[k] != T_COLLISION)
             continue;
-        const Inst &I = insts[slot];
-        const int cells = I.W * I.H;
-        const int base = (c - sc->sweep_start[slot]) * kSweepCells + threadIdx.x * 16;
-        if (base >= cells)
-            continue;
-        int8_t t[16];
-        load16(I.type + base, t);
-        for (int k = 0; k < 16; k++) {
-            const int pos = base + k;
-            if (pos >= cells || t[k] != T_COLLISION)
-                continue;
-            I.type[pos] = T_NODE;
-            I.child[pos] = 0;
-            const int32_t p = I.parent[pos];
-            const int px = unpack_x(p), pz = unpack_z(p);
-            if (px >= 0 && px < I.W && pz >= 0 && pz < I.H)
-                atomicAdd(&I.child[pz * I.W + px], 1);
-        }
+        I.type[pos] = T_NODE;
+        I.child[pos] = 0;
+        const int32_t p = I.parent[pos];
+        const int px = unpack_x(p), pz = unpack_z(p);
+        if (px >= 0 && px < I.W && pz >= 0 && pz < I.H)
+            atomicAdd(&I.child[pz * I.W + px], 1);
     }
 }
 
@@ -879,6 +871,8 @@ __global__ void __launch_bounds__(256) k_accept(const Inst *insts, State *states
         int temps = 0, all = 0, cnt = 0, kept = 0;
         int32_t mine[16];
         int32_t mine_kept[16];
+        if (base < cells && S.collision && S.node_count > 2)
+            set_collision_nodes(I, base, cells);  // this thread's own 16 cells, before it reads them
         if (base < cells) {
             int4 v = *reinterpret_cast<const int4 *>(I.type + base);
             int8_t *t = reinterpret_cast<int8_t *>(&v);
@@ -1416,7 +1410,7 @@ __global__ void k_finish(const Inst *insts, State *states, int n)
 
 const char *const kIterKernelNames[kIterKernels] = {
     "k_scan", "k_plan(cand)", "k_propose(mlp)", "k_expand", "k_apply", "k_post", "k_erase",
-    "k_setnodes", "k_accept", "k_plan(nodes, windows)", "k_gd_demand", "k_gd_eval", "k_goal", "k_select",
+    "k_accept", "k_plan(nodes, windows)", "k_gd_demand", "k_gd_eval", "k_goal", "k_select",
     "k_finish"};
 
 // ---------------------------------------------------------------------------
@@ -1551,8 +1545,6 @@ void launch_iteration(const Inst *d_inst, State *d_state, Sched *d_sched, int n_
     launch_dep(dep, k_post, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
     launch_dep(dep, k_erase, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
-    mark();
-    launch_dep(dep, k_setnodes, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();
     launch_dep(dep, k_accept, L.sweep_blocks, 256, 0, st, d_inst, d_state, d_sched);
     mark();

@@ -107,7 +107,7 @@ void launch_search_init(const Inst *d_inst, State *d_state, const int *d_slots, 
 // one planning iteration (loop()) over all active slots; with `ev` (an array
 // of kIterKernels + 1 events) an event is recorded before each kernel and
 // after the last one
-constexpr int kIterKernels = 15;
+constexpr int kIterKernels = 14;
 extern const char *const kIterKernelNames[kIterKernels];
 struct ProposalBufs;
 // with `pb`, candidates of slots that use the learned proposal get their
