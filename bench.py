@@ -554,11 +554,16 @@ def issue_peak(peaks):
     return sms * 32 * mhz * 1e6, sms, mhz
 
 
-# DRAM bytes per launch of the dominant search kernels, from one ncu capture
-# each (profiles/search_kernels_served_256x256.txt: dram__bytes_read.sum +
-# dram__bytes_write.sum of a steady-state launch, scaled to the bench's
-# launch by the listed units)
-NCU_DRAM_BYTES_PER_UNIT = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one captured
+# launch of the dominant search kernel (profiles/k_gd_eval_served_first_iterations.txt:
+# a launch of the first iterations of 256 fresh 256x256 requests, 17.16 MB
+# read + 0.06 MB written).  The masks and summed-area tables it probes stay
+# in L2, so its DRAM bytes follow the frames it touches, not its probes: the
+# figure is reported as captured, not scaled by probe count.
+NCU_DRAM_BYTES_PER_LAUNCH = {
+    "k_gd_eval": {"bytes": 17.22e6, "captured": "one launch of the first iterations of "
+                  "256 fresh 256x256 C0 requests, 256 slots (ncu --set full)"},
+}
 
 
 def run_mine(args, rank, world, local):
@@ -763,7 +768,11 @@ def run_mine(args, rank, world, local):
             "gpu_launches": int(sum(v[1] for v in ktimes.values()) * args.steps),
             "roofline": {"bound": "issue", "kernel": name, "achieved": achieved / 1e9, "peak": peak / 1e9,
                          "unit": "Gprobe/s", "frac": achieved / peak if peak else None,
-                         "traffic": NCU_DRAM_BYTES_PER_UNIT.get(name),
+                         "traffic": (NCU_DRAM_BYTES_PER_LAUNCH[name]["bytes"]
+                                     if name in NCU_DRAM_BYTES_PER_LAUNCH else None),
+                         "traffic_captured": (NCU_DRAM_BYTES_PER_LAUNCH[name]["captured"]
+                                              if name in NCU_DRAM_BYTES_PER_LAUNCH else None),
+                         "probes_per_launch": alg / max(kn, 1),
                          "algorithmic": "reference footprint probes (class lookups of "
                                         "__computeFeasibleForAngle) the kernel's work stands for, "
                                         f"against one per lane per cycle ({sms} SMs x 32 lanes x "
