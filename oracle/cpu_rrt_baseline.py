@@ -1,8 +1,9 @@
 """Times the reference's own CPU planner on C0 frames: tests/cpu_tests/cpu_rrt.py
 (RRT.loop_rrt(kinematic=True) with the MIN_DIST_CPU footprint check, on the
 NodeGrid of node_grid.py).  TEST INFRASTRUCTURE and a reported baseline only:
-it imports the reference tree, so it runs where that tree is, never on the
-GPU box; the record it writes is committed beside it.
+it imports the reference tree, so it runs only on a machine that has that
+tree, never where the bench runs; the record it writes is committed beside
+it.
 
 cpu_rrt.py imports model.waypoint.Waypoint, which is not in the reference
 tree; a stand-in with the members the planner uses (x, z, heading and
