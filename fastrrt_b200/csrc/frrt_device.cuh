@@ -343,6 +343,14 @@ struct KinTask {
 
 };
 
+// The reference's curvature, (float)(num / pow(s2, 1.5)).  Only samples
+// within 1e-6 of the limit reach it, so it stays out of line: the curve
+// loops keep their code small (their warps stall on instruction fetch).
+static __device__ __noinline__ float curv_pow(double num, double s2)
+{
+    return num / pow(s2, 1.5);
+}
+
 // The constants of one checkDirectConnectionToGoal curve
 // (graph_direct_goal_connection.cu:16-167, isDistanceToGoalProcessed =
 // false) and the reference's per-sample arithmetic; curve_warp walks it.
@@ -435,8 +443,7 @@ struct HermTask {
             return true;
         if (n2 < lo2 * s6)
             return false;
-        const float k = num / pow(s2, 1.5);
-        return k > max_curvature;
+        return curv_pow(num, s2) > max_curvature;
     }
     // t = i / (numPoints - 1), correctly rounded, without a division per
     // sample: with y = RN(1/b), q = RN(a y) and the exact remainder
@@ -464,6 +471,25 @@ __device__ inline bool footprint_warp(const Foot &f, int x, int z, float angle, 
         return true;
     }
     return probe_warp(f, x, z, angle, lane, cnt);
+}
+// footprint_warp out of line, for loops where the full test is rare (the
+// goal curves: most samples are decided by the clear bit or the summed-area
+// box): a smaller loop body fetches fewer instructions; the call costs
+// registers, so the expansion and goal-search loops keep it inline.
+static __device__ __noinline__ unsigned long long footprint_warp_out(Foot f, int x, int z, float angle, int lane)
+{
+    unsigned cnt = 0;
+    const bool ok = footprint_warp(f, x, z, angle, lane, cnt);
+    return ((unsigned long long)(ok ? 1u : 0u) << 32) | cnt;
+}
+template <bool kOut>
+__device__ __forceinline__ bool footprint_call(const Foot &f, int x, int z, float angle, int lane, unsigned &cnt)
+{
+    if (!kOut)
+        return footprint_warp(f, x, z, angle, lane, cnt);
+    const unsigned long long r = footprint_warp_out(f, x, z, angle, lane);
+    cnt = (unsigned)r;
+    return (r >> 32) != 0;
 }
 
 // Result of one kinematic candidate (check_kinematic_new_path).
@@ -653,6 +679,8 @@ __device__ inline KinResult kin_warp(const Inst &I, const Foot &f, int sx, int s
 // callers treat any negative value as none, as the reference's do).
 // `dist_channel` (isDistanceToGoalProcessed) takes the curve's distance from
 // the frame's distance channel at the start cell instead of computing it.
+// `kOut` calls the full footprint test out of line (footprint_warp_out).
+template <bool kOut = false>
 __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv, int x, int z,
                                    float local_heading, int gx, int gz, float goal_heading, int safe,
                                    float start_cost, int coarse, int lane, unsigned long long &probes,
@@ -712,7 +740,7 @@ __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv,
                 const int leader = __ffs(hm) - 1;
                 hm &= hm - 1;
                 unsigned cnt = 0;
-                if (!footprint_warp(f, __shfl_sync(kFull, cx, leader), __shfl_sync(kFull, cz, leader),
+                if (!footprint_call<kOut>(f, __shfl_sync(kFull, cx, leader), __shfl_sync(kFull, cz, leader),
                                     __shfl_sync(kFull, ang, leader), lane, cnt))
                     return -1.0f;
             }
@@ -776,7 +804,7 @@ __device__ inline float curve_warp(const Inst &I, const Foot &f, float max_curv,
             const int leader = __ffs(hm) - 1;
             hm &= hm - 1;
             unsigned cnt = 0;
-            const bool ok = footprint_warp(f, __shfl_sync(kFull, cx, leader), __shfl_sync(kFull, cz, leader),
+            const bool ok = footprint_call<kOut>(f, __shfl_sync(kFull, cx, leader), __shfl_sync(kFull, cz, leader),
                                            __shfl_sync(kFull, ang, leader), lane, cnt);
             if (!ok) {
                 ff = leader;
