@@ -7,7 +7,9 @@ A curve is an (n, 2+) array of cells (x, z, ...).  The reference computes in
 float64 Python; so does this restatement.  Its window arithmetic indexes the
 curve with negative positions on short curves (Python wraps them); the
 restatement does the same and returns NaN where the reference would raise an
-IndexError (positions below -n).
+IndexError (positions below -n).  Pinned against the reference's own
+CurveAssessment by tests/golden/curve_quality.npz (generated by
+tests/golden/make_curve_quality.py, which imports the reference module).
 """
 import math
 

@@ -30,7 +30,8 @@ LR = 5.4 / 2
 
 
 def main(reference=None):
-    build_oracle.build_ref(reference or build_oracle.reference_root())
+    reference = reference or build_oracle.reference_root()
+    build_oracle.build_ref(reference)
     if O.ref_lib() is None:
         raise SystemExit("oracle/_ref not built")
     cls, _, _ = synth.c0_request(3)

@@ -1,10 +1,14 @@
 """The oracle (host arithmetic) against golden vectors produced by the
-reference's own host-compiled functions (tests/golden/make_golden.py)."""
+reference's own host-compiled functions (tests/golden/make_golden.py) and
+its own Python curve-quality code (tests/golden/make_curve_quality.py)."""
+import math
 import os
 
 import numpy as np
+import pytest
 
 from fastrrt_b200 import synth
+from oracle import curve_quality as Q
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -60,3 +64,31 @@ def test_graph_dump_fixtures_stay_dag_after_solve(orc):
                 g.set_collision(x, z, px, pz, h, c)
         g.solve_collisions()
         assert g.consistent(), name
+
+
+def test_curve_quality_golden():
+    """length, jerk and tangential discontinuity of the curve-quality
+    restatement against the reference's CurveAssessment on 101 curves,
+    including the short ones where its window arithmetic raises"""
+    d = load("curve_quality.npz")
+    offs = np.concatenate([[0], np.cumsum(d["lengths"])])
+    raised = 0
+    for k in range(len(d["lengths"])):
+        cells = d["cells"][offs[k]:offs[k + 1]]
+        curve = [(float(p[0]), float(p[1])) for p in cells]
+        assert Q.curve_length(curve) == pytest.approx(d["total_length"][k], rel=1e-12, abs=0)
+        if math.isnan(d["jerk"][k]):
+            raised += 1
+            with pytest.raises(IndexError):
+                Q.jerk(curve)
+        else:
+            # the reference sums |j| one term after another, numpy pairwise
+            assert Q.jerk(curve) == pytest.approx(d["jerk"][k], rel=1e-9, abs=1e-12)
+        if d["tan"][k] < 0:
+            with pytest.raises(IndexError):
+                Q.tangential_discontinuity(curve, float(d["start_heading"][k]))
+        else:
+            assert Q.tangential_discontinuity(curve, float(d["start_heading"][k])) == bool(d["tan"][k])
+    # the fixture holds both answers and the raising cases
+    assert raised >= 1
+    assert 0 < (d["tan"] == 1).sum() < (d["tan"] >= 0).sum()
