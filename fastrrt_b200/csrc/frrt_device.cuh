@@ -448,8 +448,8 @@ struct HermTask {
     // t = i / (numPoints - 1), correctly rounded, without a division per
     // sample: with y = RN(1/b), q = RN(a y) and the exact remainder
     // r = a - q b, RN(q + r y) is RN(a/b) (Markstein 1990); checked
-    // exhaustively for 0 <= a <= b <= 16384 against IEEE division, which
-    // covers every frame up to 4096 x 4096
+    // exhaustively for 0 <= a <= b <= 16384 against IEEE division
+    // (tests/sample_t_check.c), which covers every frame up to 4096 x 4096
     __device__ __forceinline__ double sample_t(int k) const
     {
         const double span = (double)(numPoints - 1);
