@@ -53,3 +53,22 @@ def test_errors_without_gpu_are_loud():
     import numpy as np
     with pytest.raises(F.FastRRTError):
         F.SearchFrame(class_ids=np.zeros((8, 8), np.uint8), class_costs=np.zeros(1, np.float32))
+
+
+def test_slot_storage_sizes():
+    """per-request storage of the budget arena (fastrrt_slot_bytes, host
+    arithmetic): 256-byte aligned, growing with the frame, about 122 bytes
+    per cell (node grid 22 B, goal connections, memo, scratch, frame copy,
+    masks and summed-area table), and the sizes the serving benchmark
+    reports for 128 / 256 / 512 frames"""
+    from fastrrt_b200 import batch
+    sizes = {s: batch.slot_bytes(s, s) for s in (64, 100, 128, 256, 512, 1000)}
+    assert (sizes[128], sizes[256], sizes[512]) == (2002944, 7974912, 31862784)
+    assert all(v % 256 == 0 for v in sizes.values())
+    keys = sorted(sizes)
+    assert all(sizes[a] < sizes[b] for a, b in zip(keys, keys[1:]))
+    for s in (256, 512, 1000):
+        assert 110 < sizes[s] / (s * s) < 130
+    # a wide frame and a tall one of the same cells take the same storage
+    # up to row padding of the bit masks
+    assert abs(batch.slot_bytes(512, 128) - batch.slot_bytes(128, 512)) < 0.01 * batch.slot_bytes(512, 128)
