@@ -10,6 +10,8 @@ with and without the fused multiply-add a compiler may form):
 - rows_clear_warp: every probed cell lies inside the x interval that the
   row-interval test computes for its row, so clear intervals mean a clear
   footprint;
+- the clear mask: every probe at any heading lies within Chebyshev radius
+  floor(sqrt(mdx^2 + mdz^2)) + 2, so a clear cell needs no probe;
 - HermTask::ref_over: outside the 1e-6 band around the curvature limit the
   comparison of num^2 with limit^2 s2^3 gives the reference's
   (float)(num / pow(s2, 1.5)) > limit.
@@ -136,3 +138,18 @@ def test_curvature_band_decides_as_the_reference():
     assert not (over & under).any()
     assert np.array_equal(ref[over], np.ones(over.sum(), bool))
     assert np.array_equal(ref[under], np.zeros(under.sum(), bool))
+
+
+def test_clear_radius_bounds_every_probe():
+    """the clear mask marks cells with no obstacle within Chebyshev radius
+    floor(sqrt(mdx^2 + mdz^2)) + 2: every probe of the footprint at any
+    heading lies within it, so a clear cell is feasible at every heading"""
+    for mdx, mdz in SIZES:
+        rc = int(math.floor(math.sqrt(mdx * mdx + mdz * mdz))) + 2
+        for a in angles(300, 31 + mdz):
+            c = f32(math.cos(a))
+            s = f32(math.sin(a))
+            for fused in (False, True):
+                for x, z in ((100, 100), (0, 0)):
+                    xl, zl = probe_cells(x, z, c, s, mdx, mdz, fused)
+                    assert max(np.abs(xl - x).max(), np.abs(zl - z).max()) <= rc, (mdx, mdz, a)
