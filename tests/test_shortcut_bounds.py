@@ -153,3 +153,22 @@ def test_clear_radius_bounds_every_probe():
                 for x, z in ((100, 100), (0, 0)):
                     xl, zl = probe_cells(x, z, c, s, mdx, mdz, fused)
                     assert max(np.abs(xl - x).max(), np.abs(zl - z).max()) <= rc, (mdx, mdz, a)
+
+
+def test_summed_area_boxes_stay_below_the_count_modulus():
+    """the summed-area table holds obstacle counts mod 2^16, so a box count
+    is exact only for boxes of fewer than 65536 cells; the box test is used
+    only when mdx + mdz <= 120, where the largest box at any heading
+    ((2 ex + 1) x (2 ez + 1), ex and ez at most ceil(sqrt(mdx^2 + mdz^2) +
+    1e-3)) stays below that"""
+    worst = 0
+    for mdx in range(0, 121):
+        for mdz in range(0, 121 - mdx):
+            e = math.ceil(math.sqrt(mdx * mdx + mdz * mdz) + 1e-3)
+            worst = max(worst, (2 * e + 1) ** 2)
+    assert worst < 65536
+    # and the bound on e holds at every heading
+    for mdx, mdz in SIZES:
+        for a in angles(200, 3):
+            e = mdx * abs(math.cos(a)) + mdz * abs(math.sin(a))
+            assert e <= math.sqrt(mdx * mdx + mdz * mdz) + 1e-9
