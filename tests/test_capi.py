@@ -72,3 +72,27 @@ def test_slot_storage_sizes():
     # a wide frame and a tall one of the same cells take the same storage
     # up to row padding of the bit masks
     assert abs(batch.slot_bytes(512, 128) - batch.slot_bytes(128, 512)) < 0.01 * batch.slot_bytes(512, 128)
+
+
+def declared_arity():
+    """parameter count of every function the header declares"""
+    text = open(os.path.join(ROOT, "include", "fastrrt_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    out = {}
+    for name, params in re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(([^;{()]*)\)\s*;", text):
+        p = " ".join(params.split())
+        out[name] = 0 if p in ("", "void") else p.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_the_header():
+    """the ctypes layer declares as many arguments as the header for every
+    entry point (a mismatch would pass garbage through the ABI)"""
+    from fastrrt_b200 import _lib
+    L = _lib.lib()
+    arity = declared_arity()
+    assert set(arity) == set(_lib.EXPORTS)
+    wrong = {n: (arity[n], len(getattr(L, n).argtypes)) for n in arity
+             if len(getattr(L, n).argtypes) != arity[n]}
+    assert not wrong, wrong
