@@ -96,3 +96,28 @@ def test_binding_argument_counts_match_the_header():
     wrong = {n: (arity[n], len(getattr(L, n).argtypes)) for n in arity
              if len(getattr(L, n).argtypes) != arity[n]}
     assert not wrong, wrong
+
+
+def test_request_struct_layout_matches_the_header(tmp_path):
+    """ctypes' Request against the C compiler's layout of fastrrt_request
+    (offset of every field and the size), from a tiny program built against
+    include/fastrrt_b200.h"""
+    import shutil
+    import subprocess
+
+    from fastrrt_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = [f[0] for f in _lib.Request._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "fastrrt_b200.h"\nint main(void) {\n'
+                   + "".join(f'    printf("{n} %zu\\n", offsetof(fastrrt_request, {n}));\n' for n in names)
+                   + '    printf("sizeof %zu\\n", sizeof(fastrrt_request));\n    return 0;\n}\n')
+    exe = str(tmp_path / "layout")
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", exe], check=True)
+    got = dict(line.split() for line in subprocess.run([exe], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for n in names:
+        assert int(got[n]) == getattr(_lib.Request, n).offset, n
+    assert int(got["sizeof"]) == __import__("ctypes").sizeof(_lib.Request)
