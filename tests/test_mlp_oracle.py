@@ -34,3 +34,28 @@ def test_backward_matches_finite_differences():
             wm[t][ix] -= eps
             num = (M.loss_only(wp, X, labels) - M.loss_only(wm, X, labels)) / (2 * eps)
             assert abs(num - gs[t][ix]) < 1e-6 + 1e-4 * abs(num), (t, ix, num, gs[t][ix])
+
+
+def test_shipped_weights_fit_the_network():
+    """fastrrt_b200/proposal_weights.npz: the network's shapes (1040 -> 256
+    -> 256 -> 128), finite values, the training record it was made from, and
+    finite logits through the oracle's bf16 forward pass"""
+    import os
+
+    from fastrrt_b200 import proposal as P
+    path = os.path.join(os.path.dirname(P.__file__), "proposal_weights.npz")
+    d = np.load(path)
+    ws = [d[k] for k in ["w1", "b1", "w2", "b2", "w3", "b3"]]
+    assert [w.shape for w in ws] == [tuple(s) for s in P.SHAPES]
+    assert all(np.isfinite(w).all() for w in ws)
+    # the padded input columns past the 1030 features never see a nonzero
+    # input, whatever their weights
+    assert P.N_IN == 1030 and P.N_IN_PAD == ws[0].shape[1]
+    assert int(d["rows"]) > 100000 and int(d["solved"]) <= int(d["plans"])
+    assert str(d["source"]) == "paths"
+    rng = np.random.default_rng(3)
+    X = rng.random((64, P.N_IN)).astype(np.float32)
+    X[:, :1024] = rng.random((64, 1024)) < 0.2
+    _, _, _, logits = M.forward(ws, X)
+    assert logits.shape == (64, P.N_OUT) and np.isfinite(logits).all()
+    assert logits.std(axis=1).min() > 0
