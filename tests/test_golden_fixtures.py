@@ -92,3 +92,25 @@ def test_curve_quality_golden():
     # the fixture holds both answers and the raising cases
     assert raised >= 1
     assert 0 < (d["tan"] == 1).sum() < (d["tan"] >= 0).sum()
+
+
+def test_interpolation_golden(orc):
+    """the oracle's Hermite interpolation of planned paths against the
+    reference's own interpolate() (src/interpolation.cpp built with g++,
+    tests/golden/make_interpolation.py): the same cells and headings on 63
+    control-point paths, including sharp turns, paths that leave the frame,
+    repeated points and two-point paths"""
+    d = load("interpolation.npz")
+    W, H = int(d["width"]), int(d["height"])
+    pi = np.concatenate([[0], np.cumsum(d["n_in"])])
+    po = np.concatenate([[0], np.cumsum(d["n_out"])])
+    total = 0
+    for k in range(len(d["n_in"])):
+        path = d["paths"][pi[k]:pi[k + 1]]
+        want = d["out"][po[k]:po[k + 1]]
+        got = orc.interpolate(path, W, H)
+        assert got.shape == want.shape, k
+        assert np.array_equal(got[:, :2], want[:, :2]), k
+        assert np.array_equal(got[:, 2].view(np.uint32), want[:, 2].view(np.uint32)), k
+        total += len(want)
+    assert total > 5000
